@@ -1,0 +1,284 @@
+/*
+ * specrel.h — C ABI of the B200 render engine for SpecRel's per-pixel render path.
+ *
+ * It replaces the wgpu backend `GpuRenderer` (src/gpu.rs:432-901) behind the same data split the
+ * reference already uses: static scene arrays uploaded once (`PackedSceneGpuData`,
+ * src/gpu.rs:232-315) and a 768-byte per-frame uniform block (`GpuUniforms`,
+ * src/gpu.rs:122-212). A Rust caller binds these functions with `extern "C"` (see
+ * INTEGRATION.md) and keeps `Scene4D::build`, `PackedSceneGpuData::from_scene` and
+ * `GpuUniforms::build` as they are.
+ *
+ * Conventions: every function returns an `sr_status` (no aborts); host buffers belong to the
+ * caller, device buffers to the context; one CUDA stream per context; a context is not
+ * thread-safe (the reference's `&mut self`).
+ */
+#ifndef SPECREL_H
+#define SPECREL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SR_MAX_FLASHES 16        /* renderer.rs:179 */
+#define SR_MAX_HAZE_ORIGINS 5    /* renderer.rs:224 */
+#define SR_GAMMA_LUT_SIZE 4096   /* renderer.rs:1102 */
+#define SR_BLOOM_LEVELS 6        /* bloom.rs:23 */
+#define SR_STACK_SIZE 64         /* bvh4d.rs:454, :537 */
+
+/* ---- Packed scene arrays, byte for byte the reference's layouts ---------------------------- */
+
+/* GpuNode (gpu.rs:44-51). Leaf when count > 0 (right_or_first = first hot record); else an
+ * internal node with children `left` and `right_or_first`. 4-vectors are (t, x, y, z). */
+typedef struct SrGpuNode {
+    float min[4];
+    float max[4];
+    uint32_t right_or_first;
+    uint32_t count;
+    uint32_t left;
+    uint32_t pad;
+} SrGpuNode;
+
+/* GpuGeom (gpu.rs:68-74): the 80-byte hot record of SimplexGeom4D (mesh4d.rs:153-159). */
+typedef struct SrGpuGeom {
+    float v0[4];
+    float n[4];
+    float b1[4];
+    float b2[4];
+    float b3[4];
+} SrGpuGeom;
+
+/* GpuAttr (gpu.rs:79-92): cold attributes, transposed (one row = one component, 4 vertices).
+ * misc = (uv_world_scale.u, uv_world_scale.v, bitcast<f32>(material_id), 0). */
+typedef struct SrGpuAttr {
+    float uv_u[4], uv_v[4];
+    float tb_x[4], tb_y[4], tb_z[4];
+    float tau[4];
+    float grad_u[4], grad_v[4];
+    float normal[4];
+    float four_vel[4];
+    float misc[4];
+    float decided_at[4];
+} SrGpuAttr;
+
+/* GpuMaterial (gpu.rs:96-100): base = (rgb, emission), checker = (rgb, grid_scale),
+ * params = (wireframe_width, bitcast<f32>(pattern), cavity_length, 0). */
+typedef struct SrGpuMaterial {
+    float base[4];
+    float checker[4];
+    float params[4];
+} SrGpuMaterial;
+
+/* GpuUniforms (gpu.rs:122-144), 768 bytes. */
+typedef struct SrGpuUniforms {
+    float cam_pos[4];
+    float e[4][4];
+    float light_pos[4];
+    float half_wh[2];
+    uint32_t size[2];
+    uint32_t mode;         /* 0 shaded, 1 isochrones, 2 tetrahedron inspector, 3 decision age */
+    uint32_t shadow_mode;  /* 0 off, 1 Lorentz-invariant (null), 2 camera slice */
+    uint32_t slice_mode;   /* 0 past light cone, 1 God's-eye slice, 2 frontier, 3 prophecy */
+    uint32_t num_nodes;
+    float frontier_origin[4];
+    float frontier_view_offset;
+    uint32_t num_flashes;
+    float frontier_tau;
+    float prophecy_delta;
+    uint32_t num_haze;
+    uint32_t num_stars;
+    uint32_t pad[2];
+    float haze_origin[SR_MAX_HAZE_ORIGINS][4];
+    float flash_at[SR_MAX_FLASHES][4];
+    float flash_col_width[SR_MAX_FLASHES][4];
+} SrGpuUniforms;
+
+/* PackedSceneGpuData (gpu.rs:232-244) plus two optional sidecars. */
+typedef struct SrSceneDesc {
+    const SrGpuNode* nodes;
+    uint32_t num_nodes;
+    uint32_t num_prims;
+    const SrGpuGeom* geoms;           /* num_prims, leaf order */
+    const SrGpuAttr* attrs;           /* num_prims, leaf order */
+    const SrGpuMaterial* materials;
+    uint32_t num_materials;
+    uint32_t num_stars;               /* star headers at the front of `stars` */
+    const float* stars;               /* pack_stars (gpu.rs:106-119), num_star_vec4 x vec4 */
+    uint64_t num_star_vec4;
+    float light_pos[4];               /* (unused, x, y, z) */
+    /* Optional: leaf slot -> original simplex index (Bvh4D::order, bvh4d.rs:72-73), so hit ids
+     * are reported in the caller's simplex order; NULL reports leaf slots. */
+    const uint32_t* leaf_to_orig;
+    /* Optional: FP64 anchor (t, x, y, z) that every f32 coordinate of the scene is relative to;
+     * NULL means the origin. Used by the FP64 camera path (sr_render_ex with `cam64`). */
+    const double* anchor;
+} SrSceneDesc;
+
+typedef struct SrRange { uint64_t start, end; } SrRange;
+
+/* ---- Status ------------------------------------------------------------------------------- */
+typedef int32_t sr_status;
+#define SR_OK 0
+#define SR_ERR_INVALID_ARGUMENT 1
+#define SR_ERR_CUDA 2
+#define SR_ERR_OUT_OF_MEMORY 3
+#define SR_ERR_NO_DEVICE 4
+#define SR_ERR_NO_SCENE 5
+#define SR_ERR_BAD_SCENE 6
+#define SR_ERR_TRAVERSAL_LIMIT 7
+#define SR_ERR_UNSUPPORTED 8
+
+typedef struct sr_ctx sr_ctx;
+
+/* GpuTimings (gpu.rs:408-420), milliseconds, plus per-phase device times recorded with CUDA
+ * events on the context's stream when SR_FLAG_TIMING is set. */
+typedef struct SrTimings {
+    float submit_ms;
+    float wait_ms;
+    float kernel_ms;    /* whole frame on the device */
+    float readback_ms;
+    float camera_ms;    /* FP64 camera / rebase kernel */
+    float trace_ms;     /* primary traversal (+ shading for the plain path) */
+    float shade_ms;     /* shading + shadow rays (fast path) */
+    float stars_ms;     /* star cone events, binning and gather */
+    float bloom_ms;     /* bloom pyramid + tone map + pack */
+    uint32_t shadow_rays;
+    uint32_t pad;
+    /* Traversal work, filled when SR_FLAG_COUNT_WORK is set (a slower counting variant of the
+     * kernels): internal-node visits (each tests two child boxes), leaf visits and tetrahedron
+     * tests, for primary rays and for shadow rays. */
+    uint64_t nodes_visited, leaves_visited, tets_tested;
+    uint64_t shadow_nodes_visited, shadow_leaves_visited, shadow_tets_tested;
+} SrTimings;
+
+/* Which implementation renders a frame. */
+#define SR_PATH_PLAIN 0   /* one thread per pixel, the reference's BVH2 traversal order */
+#define SR_PATH_FAST 1    /* persistent, warp-cooperative traversal over the B200 node layout */
+
+#define SR_FLAG_TIMING 1u          /* record per-phase CUDA events into SrTimings */
+#define SR_FLAG_DEVICE_OUTPUT 2u   /* output pointers are device pointers; return without syncing */
+#define SR_FLAG_STAR_BRUTE 4u      /* stars: O(N_stars) per pixel as the reference, no binning */
+#define SR_FLAG_COUNT_WORK 8u      /* count traversal work into SrTimings (slower; blocks) */
+
+/* Optional per-pixel outputs (host or device pointers, as the call's flags say). */
+typedef struct SrOutputs {
+    uint32_t* rgb;      /* W*H packed 0x00RRGGBB (required) */
+    uint32_t* hit_id;   /* W*H original simplex index of the primary hit, 0xFFFFFFFF on a miss */
+    float* lambda;      /* W*H affine parameter of the primary hit */
+    float* tau;         /* W*H interpolated proper time of the primary hit */
+    float* hdr;         /* W*H*4 pre-bloom radiance (r, g, b, 0) */
+} SrOutputs;
+
+/* The observer in FP64: event and tetrad are built on the GPU in double precision, rebased to the
+ * scene anchor, then rounded to the f32 uniforms the traversal uses. */
+typedef struct SrCameraF64 {
+    double event[4];      /* (t, x, y, z) in world coordinates */
+    double rapidity[3];   /* Tetrad::rest().boost_local(rapidity) (minkowski.rs:467-479) */
+    double yaw, pitch, roll;  /* then rotate_local (minkowski.rs:498-521) */
+} SrCameraF64;
+
+typedef struct SrRenderOpts {
+    uint32_t path;               /* SR_PATH_* */
+    uint32_t flags;              /* SR_FLAG_* */
+    const SrCameraF64* cam64;    /* optional FP64 camera (overrides cam_pos / e of the uniforms) */
+} SrRenderOpts;
+
+/* ---- Context ----------------------------------------------------------------------------- */
+
+/* GpuRenderer::new (gpu.rs:472-620), device half: picks CUDA device `device`, creates the stream,
+ * uploads the gamma LUT and glyph tables (gpu.rs:223-229). */
+sr_status sr_create(int device, sr_ctx** out, char* err, size_t errlen);
+void sr_destroy(sr_ctx* ctx);
+const char* sr_last_error(const sr_ctx* ctx);
+/* GpuRenderer::adapter_name (gpu.rs:734). */
+sr_status sr_adapter_name(const sr_ctx* ctx, char* buf, size_t len);
+/* Use a caller-owned cudaStream_t (NULL: the context's own stream). */
+sr_status sr_set_stream(sr_ctx* ctx, void* cuda_stream);
+sr_status sr_synchronize(sr_ctx* ctx);
+
+/* ---- Scenes ------------------------------------------------------------------------------ */
+
+/* GpuRenderer::upload_scene (gpu.rs:622-699): copies the packed arrays to the device, validates
+ * them (child links, leaf ranges, material ids) and builds the B200 node layout on the device. */
+sr_status sr_upload_scene(sr_ctx* ctx, uint32_t scene_idx, const SrSceneDesc* desc);
+/* The host-side checks sr_upload_scene runs before copying (no device needed): child links and
+ * leaf ranges in bounds, every node reached once from the root, material ids, leaf_to_orig and
+ * star segment ranges in bounds. `depth` (optional) receives the tree depth. The reference's
+ * upload (gpu.rs:622-699) trusts its own builder and has no counterpart. */
+sr_status sr_scene_validate(const SrSceneDesc* desc, uint32_t* depth, char* err, size_t errlen);
+/* GpuRenderer::update_scene (gpu.rs:704-731): writes only the dirty node and primitive ranges
+ * when they fit the arrays already on the device, else uploads afresh. `desc` holds the full
+ * new arrays; the ranges say which items changed since the last upload or update. */
+sr_status sr_update_scene(sr_ctx* ctx, uint32_t scene_idx, const SrSceneDesc* desc, const SrRange* node_ranges,
+                          uint32_t n_node_ranges, const SrRange* prim_ranges, uint32_t n_prim_ranges);
+
+typedef struct SrSceneStats {
+    uint32_t num_nodes, num_prims, num_stars, bvh_depth;
+    uint64_t device_bytes;
+    uint32_t fast_nodes;   /* nodes of the B200 layout */
+    uint32_t pad;
+} SrSceneStats;
+sr_status sr_scene_stats(const sr_ctx* ctx, uint32_t scene_idx, SrSceneStats* out);
+
+/* ---- Frames ------------------------------------------------------------------------------- */
+
+/* GpuRenderer::render (gpu.rs:798-900): renders scene `scene_idx` with uniforms `u` into the
+ * caller's host framebuffer (`fb_len` = width * height packed 0x00RRGGBB) and blocks until it
+ * is there. Uses the fast path. */
+sr_status sr_render(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, uint32_t* framebuffer,
+                    uint64_t fb_len, SrTimings* timings);
+
+/* The general form: explicit path, optional side outputs, optional FP64 camera, and (with
+ * SR_FLAG_DEVICE_OUTPUT) device-resident outputs with no synchronisation. */
+sr_status sr_render_ex(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, const SrRenderOpts* opts,
+                       const SrOutputs* out, SrTimings* timings);
+
+/* Many observers of one scene in one persistent launch (recorded once into a CUDA graph and
+ * replayed). Observer i renders with uniforms `u[i]` (and `cam64[i]` when cam64 is not NULL)
+ * into `rgb_out + offset_i`, offset_i = sum of width*height of observers before it. */
+sr_status sr_render_batch(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, const SrCameraF64* cam64,
+                          uint32_t n_observers, uint32_t* rgb_out, uint64_t rgb_len, uint32_t flags,
+                          SrTimings* timings);
+
+/* Launch parameters of the fast path; the autotuner (sr_autotune) picks them per scene. */
+typedef struct SrTuning {
+    uint32_t block_threads;   /* threads per block of the persistent traversal kernel */
+    uint32_t blocks_per_sm;   /* resident blocks per SM */
+    uint32_t stack_depth;     /* traversal stack entries in shared memory before spilling */
+    uint32_t smem_levels;     /* top BVH levels staged in shared memory */
+    uint32_t tile_w, tile_h;  /* pixel tile a warp takes at a time */
+} SrTuning;
+sr_status sr_get_tuning(const sr_ctx* ctx, uint32_t scene_idx, SrTuning* out);
+sr_status sr_set_tuning(sr_ctx* ctx, uint32_t scene_idx, const SrTuning* t);
+/* Times candidate SrTuning values on `n` frames and keeps the fastest for this scene. */
+sr_status sr_autotune(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, uint32_t n, SrTuning* best,
+                      float* best_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#ifdef __cplusplus
+static_assert(sizeof(SrGpuNode) == 48, "GpuNode is 48 bytes (gpu.rs:44-51)");
+static_assert(sizeof(SrGpuGeom) == 80, "GpuGeom is 80 bytes (gpu.rs:68-74)");
+static_assert(sizeof(SrGpuAttr) == 192, "GpuAttr is 192 bytes (gpu.rs:79-92)");
+static_assert(sizeof(SrGpuMaterial) == 48, "GpuMaterial is 48 bytes (gpu.rs:96-100)");
+static_assert(sizeof(SrGpuUniforms) == 768, "GpuUniforms is 768 bytes (gpu.rs:122-144)");
+static_assert(offsetof(SrGpuUniforms, light_pos) == 80, "Uniforms.light_pos");
+static_assert(offsetof(SrGpuUniforms, num_nodes) == 124, "Uniforms.num_nodes");
+static_assert(offsetof(SrGpuUniforms, frontier_origin) == 128, "Uniforms.frontier_origin");
+static_assert(offsetof(SrGpuUniforms, frontier_view_offset) == 144, "Uniforms.frontier_view_offset");
+static_assert(offsetof(SrGpuUniforms, num_flashes) == 148, "Uniforms.num_flashes");
+static_assert(offsetof(SrGpuUniforms, frontier_tau) == 152, "Uniforms.frontier_tau");
+static_assert(offsetof(SrGpuUniforms, num_haze) == 160, "Uniforms.num_haze");
+static_assert(offsetof(SrGpuUniforms, num_stars) == 164, "Uniforms.num_stars");
+static_assert(offsetof(SrGpuUniforms, haze_origin) == 176, "Uniforms.haze_origin");
+static_assert(offsetof(SrGpuUniforms, flash_at) == 256, "Uniforms.flash_at");
+static_assert(offsetof(SrGpuUniforms, flash_col_width) == 512, "Uniforms.flash_col_width");
+static_assert(offsetof(SrGpuAttr, misc) == 160, "Attr.misc");
+static_assert(offsetof(SrGpuAttr, decided_at) == 176, "Attr.decided_at");
+#endif
+
+#endif /* SPECREL_H */

@@ -1,0 +1,112 @@
+/*
+ * specrel_scene.h — host-side helpers on the caller's side of the boundary, in C++.
+ *
+ * In the reference these steps run in Rust before the GPU backend sees any data:
+ *   Scene4D::build / Bvh4D::build (scene.rs:164, bvh4d.rs:123-141) and the worldtube pipeline
+ *   (mesh4d.rs:312-371, :721-854, :912-1052); PackedSceneGpuData::from_scene (gpu.rs:247-289);
+ *   Camera4D / Tetrad setup (renderer.rs:45-65, minkowski.rs:424-596); GpuUniforms::build
+ *   (gpu.rs:147-211).
+ * This library restates them so the benchmarks and tests can produce the reference's packed
+ * arrays and uniform blocks for the seeded synthetic workloads without a Rust toolchain. A Rust
+ * caller keeps its own code and only binds include/specrel.h.
+ */
+#ifndef SPECREL_SCENE_H
+#define SPECREL_SCENE_H
+
+#include "specrel.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A seeded synthetic workload. config: 1 = 64 inertial unit cubes; 2 = 64 accelerated
+ * icospheres; 3 = configuration 1 translated by `translate` (FP64 anchor); 4 = configuration 1's
+ * scene (the batched-observer workload); 5 = configuration 1's scene plus `n_stars` point stars. */
+typedef struct SrSynthParams {
+    uint32_t config;
+    uint32_t n_bodies;
+    uint32_t steps;
+    uint32_t subdiv;
+    uint32_t n_stars;
+    uint32_t threads;     /* worker threads for extrusion and the BVH build (0: all cores) */
+    uint64_t seed;
+    double translate[4];  /* configuration 3's offset (t, x, y, z) */
+} SrSynthParams;
+
+typedef struct sr_scene sr_scene;
+
+typedef struct SrSynthInfo {
+    uint32_t bvh_depth;
+    int32_t rindler_ok;      /* the reference's f32 finite-difference check (mesh4d.rs:742-749) */
+    uint32_t clamped_accel;  /* bodies whose |a| was clamped to 0.8 / r */
+    uint32_t max_leaf;
+    double cam_pos[4];       /* the workload's observer event */
+    double cam_rapidity[3];  /* the workload's observer rapidity */
+    double anchor[4];        /* FP64 anchor of the f32 coordinates */
+    double build_seconds;
+} SrSynthInfo;
+
+/* Builds the workload (threads: params->threads). */
+sr_status sr_scene_synth(const SrSynthParams* params, sr_scene** out, char* err, size_t errlen);
+void sr_scene_free(sr_scene* s);
+/* Pointers into the scene's packed arrays (valid until sr_scene_free). */
+sr_status sr_scene_desc(const sr_scene* s, SrSceneDesc* out);
+sr_status sr_scene_info(const sr_scene* s, SrSynthInfo* out);
+
+/* One observer of the batched workload (configuration 4). */
+typedef struct SrObserverDraw {
+    uint32_t width, height, slice_mode, pad;
+    double pos[4];
+    double rapidity[3];
+} SrObserverDraw;
+sr_status sr_observers_synth(uint64_t seed, uint32_t n, SrObserverDraw* out);
+
+/* Camera4D (renderer.rs:45-65) with its f32 tetrad. */
+typedef struct SrCamera {
+    float position[4];
+    float e[4][4];
+    float proper_time;
+    float fov_y_rad;
+} SrCamera;
+/* Camera4D::new(position, fov_deg): rest tetrad, fov_deg.to_radians(). */
+sr_status sr_camera_new(const float position[4], float fov_deg, SrCamera* out);
+/* Tetrad::boost_local (minkowski.rs:467-479) and rotate_local (minkowski.rs:498-521). */
+sr_status sr_camera_boost_local(SrCamera* cam, const float d_rapidity[3]);
+sr_status sr_camera_rotate_local(SrCamera* cam, float yaw, float pitch, float roll);
+
+/* RenderConfig (renderer.rs:160-168). */
+typedef struct SrRenderConfig {
+    uint32_t width, height, mode, shadow_mode, slice_mode;
+    float prophecy_delta;
+} SrRenderConfig;
+
+/* FlashEvent (renderer.rs:185-190) and FrameDynamics (renderer.rs:205-218). */
+typedef struct SrFlash {
+    float at[4];
+    float width, intensity;
+    float color[3];
+} SrFlash;
+typedef struct SrFrameDynamics {
+    int32_t has_frontier;
+    uint32_t n_flashes;
+    float frontier_origin[4];
+    float frontier_tau;
+    float frontier_lag;
+    const SrFlash* flashes;
+    const float* remote_origins;  /* n_remote x 4 */
+    uint32_t n_remote;
+    uint32_t pad;
+} SrFrameDynamics;
+
+/* GpuUniforms::build (gpu.rs:147-211). `dyn` may be NULL (FrameDynamics::default()). */
+sr_status sr_uniforms_build(const SrCamera* cam, const SrRenderConfig* cfg, const SrFrameDynamics* dyn,
+                            uint32_t num_nodes, const float light_pos[4], uint32_t num_stars, SrGpuUniforms* out);
+
+/* build_tables_data (gpu.rs:223-229): 4096 gamma-LUT entries then 14 glyphs x 7 rows. */
+sr_status sr_tables_build(uint32_t* out4194);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPECREL_SCENE_H */

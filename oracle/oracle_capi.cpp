@@ -1,0 +1,358 @@
+// TEST INFRASTRUCTURE ONLY — C ABI of the CPU oracle, loaded by the parity tests (ctypes) and by
+// bench.py's CPU-baseline leg. Never linked into the shipped library.
+#include <cstring>
+#include <memory>
+
+#include "oracle_scenes.hpp"
+
+using namespace orc;
+
+extern "C" {
+
+struct OrcSynthParams {
+    uint32_t config;
+    uint32_t n_bodies;
+    uint32_t steps;
+    uint32_t subdiv;
+    uint32_t n_stars;
+    uint32_t pad;
+    uint64_t seed;
+    double translate[4];
+};
+
+struct OrcSceneInfo {
+    uint64_t n_prims, n_nodes, n_stars, n_star_vec4, n_materials;
+    uint32_t depth;
+    int32_t rindler_ok, superluminal;
+    uint32_t clamped_accel;
+    double cam_pos[4];
+    double cam_rapidity[3];
+    double bounds_min[4], bounds_max[4];
+};
+
+struct OrcCamera {
+    double pos[4];
+    double rapidity[3];
+    double yaw, pitch, roll;
+    double fov_deg;
+    double proper_time;
+    int32_t use_tetrad;
+    int32_t pad;
+    double tetrad[16];  // e0..e3, each (t, x, y, z); used when use_tetrad != 0
+};
+
+struct OrcConfig {
+    uint32_t width, height, mode, shadow_mode, slice_mode;
+    float prophecy_delta;
+    uint32_t full_height, row_stride, row_offset;  // row sampling (0 = render the whole frame)
+};
+
+struct OrcFlash {
+    double at[4];
+    double width, intensity;
+    double color[3];
+};
+
+struct OrcDynamics {
+    int32_t has_frontier;
+    uint32_t n_flashes;
+    double frontier_origin[4];
+    double frontier_tau;
+    double frontier_lag;
+    const OrcFlash* flashes;
+    uint32_t n_remote;
+    uint32_t pad;
+    const double* remote_origins;  // n_remote x 4
+};
+
+struct OrcObserver {
+    uint32_t width, height, slice_mode, pad;
+    double pos[4];
+    double rapidity[3];
+};
+
+struct OrcPixelOut {
+    uint32_t* rgb;        // w*h packed 0x00RRGGBB (required)
+    int64_t* slot;        // leaf slot of the primary hit or -1
+    uint32_t* orig;       // original simplex index of the hit (0xFFFFFFFF for a miss)
+    double* lambda;
+    double* tau;
+    double* min_bary;
+    double* denom_rel;
+    double* hdr;          // w*h*3 pre-bloom radiance
+    uint64_t* stats;      // w*h*4: internal pops, leaf pops, tets tested, shadow rays
+};
+}
+
+namespace {
+struct SceneBox {
+    bool fp64;
+    std::unique_ptr<SynthOut<float>> f;
+    std::unique_ptr<SynthOut<double>> d;
+};
+
+template <class T> Tetrad<T> make_tetrad(const OrcCamera& c) {
+    Tetrad<T> t = Tetrad<T>::rest();
+    if (c.use_tetrad) {
+        for (int a = 0; a < 4; ++a) t.e[a] = V4<T>((T)c.tetrad[4 * a], (T)c.tetrad[4 * a + 1], (T)c.tetrad[4 * a + 2], (T)c.tetrad[4 * a + 3]);
+        return t;
+    }
+    t.boost_local(V3<T>((T)c.rapidity[0], (T)c.rapidity[1], (T)c.rapidity[2]));
+    if (c.yaw != 0 || c.pitch != 0 || c.roll != 0) t.rotate_local((T)c.yaw, (T)c.pitch, (T)c.roll);
+    return t;
+}
+
+template <class T>
+int render_t(const Scene<T>& scene, const OrcCamera* c, const OrcConfig* cf, const OrcDynamics* dy, int threads,
+             int perturb, const OrcPixelOut* out) {
+    Camera4D<T> cam;
+    cam.position = V4<T>((T)c->pos[0], (T)c->pos[1], (T)c->pos[2], (T)c->pos[3]);
+    cam.tetrad = make_tetrad<T>(*c);
+    cam.proper_time = (T)c->proper_time;
+    // Camera4D::new: fov_deg.to_radians() (renderer.rs:57-64) in the scalar type.
+    cam.fov_y_rad = (T)c->fov_deg * (C<T>::PI / T(180));
+    RenderConfig cfg;
+    cfg.width = cf->width;
+    cfg.height = cf->height;
+    cfg.mode = (RenderMode)cf->mode;
+    cfg.shadow_mode = (ShadowMode)cf->shadow_mode;
+    cfg.slice_mode = (ViewMode)cf->slice_mode;
+    cfg.prophecy_delta = cf->prophecy_delta;
+    if (cf->full_height) {
+        cfg.full_height = cf->full_height;
+        cfg.row_stride = cf->row_stride ? cf->row_stride : 1;
+        cfg.row_offset = cf->row_offset;
+    }
+    FrameDynamics<T> dyn;
+    if (dy) {
+        dyn.has_frontier = dy->has_frontier != 0;
+        dyn.frontier.origin = V4<T>((T)dy->frontier_origin[0], (T)dy->frontier_origin[1], (T)dy->frontier_origin[2], (T)dy->frontier_origin[3]);
+        dyn.frontier.proper_time = (T)dy->frontier_tau;
+        dyn.frontier_lag = (T)dy->frontier_lag;
+        for (uint32_t i = 0; i < dy->n_flashes; ++i) {
+            const OrcFlash& f = dy->flashes[i];
+            dyn.flashes.push_back({V4<T>((T)f.at[0], (T)f.at[1], (T)f.at[2], (T)f.at[3]), (T)f.width, (T)f.intensity,
+                                   V3<T>((T)f.color[0], (T)f.color[1], (T)f.color[2])});
+        }
+        for (uint32_t i = 0; i < dy->n_remote; ++i)
+            dyn.remote_origins.push_back(V4<T>((T)dy->remote_origins[4 * i], (T)dy->remote_origins[4 * i + 1],
+                                               (T)dy->remote_origins[4 * i + 2], (T)dy->remote_origins[4 * i + 3]));
+    }
+    perturb_ulps() = perturb;
+    Renderer<T> r{scene, cam, cfg, dyn};
+    bool want_aux = out->slot || out->orig || out->lambda || out->tau || out->min_bary || out->denom_rel || out->stats;
+    std::vector<PixelAux<T>> aux;
+    std::vector<V3<T>> hdr;
+    r.render(out->rgb, want_aux ? &aux : nullptr, out->hdr ? &hdr : nullptr, threads <= 0 ? 1u : (unsigned)threads);
+    perturb_ulps() = 0;
+    size_t n = (size_t)cfg.width * cfg.height;
+    for (size_t i = 0; i < n && want_aux; ++i) {
+        const auto& a = aux[i];
+        if (out->slot) out->slot[i] = a.slot;
+        if (out->orig) out->orig[i] = a.slot < 0 ? 0xFFFFFFFFu : scene.bvh.order[(size_t)a.slot];
+        if (out->lambda) out->lambda[i] = (double)a.lambda;
+        if (out->tau) out->tau[i] = (double)a.tau;
+        if (out->min_bary) out->min_bary[i] = (double)a.min_bary;
+        if (out->denom_rel) out->denom_rel[i] = (double)a.denom_rel;
+        if (out->stats) {
+            out->stats[4 * i] = a.stats.internal_pops;
+            out->stats[4 * i + 1] = a.stats.leaf_pops;
+            out->stats[4 * i + 2] = a.stats.tets_tested;
+            out->stats[4 * i + 3] = a.shadow_rays;
+        }
+    }
+    if (out->hdr)
+        for (size_t i = 0; i < n; ++i) {
+            out->hdr[3 * i] = (double)hdr[i].x;
+            out->hdr[3 * i + 1] = (double)hdr[i].y;
+            out->hdr[3 * i + 2] = (double)hdr[i].z;
+        }
+    return 0;
+}
+
+template <class T> void info_t(const SynthOut<T>& s, OrcSceneInfo* o) {
+    o->n_prims = s.scene.bvh.hot.size();
+    o->n_nodes = s.scene.bvh.nodes.size();
+    o->n_stars = s.scene.stars.size();
+    size_t segs = 0;
+    for (auto& st : s.scene.stars) segs += st.segments.size();
+    o->n_star_vec4 = s.scene.stars.size() + 3 * segs;
+    o->n_materials = s.scene.materials.size();
+    o->depth = s.scene.bvh.depth();
+    o->rindler_ok = s.rindler_ok;
+    o->superluminal = s.superluminal;
+    o->clamped_accel = s.clamped_accel;
+    for (int k = 0; k < 4; ++k) o->cam_pos[k] = s.cam_pos[k];
+    for (int k = 0; k < 3; ++k) o->cam_rapidity[k] = s.cam_rapidity[k];
+    if (!s.scene.bvh.nodes.empty()) {
+        const auto& b = s.scene.bvh.nodes[0].aabb;
+        for (int k = 0; k < 4; ++k) { o->bounds_min[k] = (double)b.min.axis(k); o->bounds_max[k] = (double)b.max.axis(k); }
+    }
+}
+}  // namespace
+
+extern "C" {
+
+void* orc_scene_new(const OrcSynthParams* p, int fp64) {
+    SynthParams sp;
+    sp.config = p->config;
+    sp.seed = p->seed;
+    sp.n_bodies = p->n_bodies;
+    sp.steps = p->steps;
+    sp.subdiv = p->subdiv;
+    sp.n_stars = p->n_stars;
+    for (int k = 0; k < 4; ++k) sp.translate[k] = p->translate[k];
+    auto* b = new SceneBox();
+    b->fp64 = fp64 != 0;
+    if (b->fp64) b->d = std::make_unique<SynthOut<double>>(synth_scene<double>(sp));
+    else b->f = std::make_unique<SynthOut<float>>(synth_scene<float>(sp));
+    return b;
+}
+
+void orc_scene_free(void* s) { delete (SceneBox*)s; }
+
+// A float scene from the reference's packed arrays (gpu.rs:44-119 layouts): the BVH nodes and hot
+// records as given, the cold attributes as leaf-ordered simplices (order = identity). Lets the
+// oracle render exactly the input a caller uploads, without rebuilding it.
+void* orc_scene_from_packed(const void* nodes_, uint32_t n_nodes, const void* geoms_, const void* attrs_,
+                            uint32_t n_prims, const void* mats_, uint32_t n_mats, const float* stars, uint64_t n_star_vec4,
+                            uint32_t n_stars, const float* light_pos) {
+    const PNode* nodes = (const PNode*)nodes_;
+    const PGeom* geoms = (const PGeom*)geoms_;
+    const PAttr* attrs = (const PAttr*)attrs_;
+    const PMat* mats = (const PMat*)mats_;
+    auto* b = new SceneBox();
+    b->fp64 = false;
+    b->f = std::make_unique<SynthOut<float>>();
+    Scene<float>& sc = b->f->scene;
+    auto v4 = [](const float* p) { return V4<float>(p[0], p[1], p[2], p[3]); };
+    sc.bvh.nodes.resize(n_nodes);
+    for (uint32_t i = 0; i < n_nodes; ++i) {
+        auto& n = sc.bvh.nodes[i];
+        n.aabb.min = v4(nodes[i].min);
+        n.aabb.max = v4(nodes[i].max);
+        n.right_or_first = nodes[i].right_or_first;
+        n.count = nodes[i].count;
+        n.left = nodes[i].left;
+    }
+    sc.bvh.hot.resize(n_prims);
+    sc.bvh.order.resize(n_prims);
+    sc.bvh.simplices.resize(n_prims);
+    for (uint32_t i = 0; i < n_prims; ++i) {
+        Geom<float>& g = sc.bvh.hot[i];
+        g.v0 = v4(geoms[i].v0); g.n = v4(geoms[i].n); g.b1 = v4(geoms[i].b1); g.b2 = v4(geoms[i].b2); g.b3 = v4(geoms[i].b3);
+        sc.bvh.order[i] = i;
+        Simplex<float>& s = sc.bvh.simplices[i];
+        s.g = g;
+        const PAttr& a = attrs[i];
+        for (int k = 0; k < 4; ++k) {
+            s.uv_u[k] = a.uv_u[k]; s.uv_v[k] = a.uv_v[k];
+            s.tri_bary[k] = V3<float>(a.tb_x[k], a.tb_y[k], a.tb_z[k]);
+            s.tau[k] = a.tau[k]; s.grad_u[k] = a.grad_u[k]; s.grad_v[k] = a.grad_v[k];
+            s.decided_at[k] = a.decided_at[k];
+        }
+        s.normal = v4(a.normal);
+        s.four_vel = v4(a.four_vel);
+        s.uvs_u = a.misc[0];
+        s.uvs_v = a.misc[1];
+        std::memcpy(&s.material_id, &a.misc[2], 4);
+    }
+    for (uint32_t i = 0; i < n_mats; ++i) {
+        Material<float> m;
+        m.base_color = V3<float>(mats[i].base[0], mats[i].base[1], mats[i].base[2]);
+        m.emission = mats[i].base[3];
+        m.checker_color = V3<float>(mats[i].checker[0], mats[i].checker[1], mats[i].checker[2]);
+        m.grid_scale = mats[i].checker[3];
+        m.wireframe_width = mats[i].params[0];
+        uint32_t pat;
+        std::memcpy(&pat, &mats[i].params[1], 4);
+        m.pattern = (Pattern)pat;
+        m.cavity_length = mats[i].params[2];
+        sc.materials.push_back(m);
+    }
+    sc.light_pos = V3<float>(light_pos[1], light_pos[2], light_pos[3]);
+    const float* segs = stars + 4ull * n_stars;
+    for (uint32_t i = 0; i < n_stars; ++i) {
+        PointStar<float> st;
+        st.temperature = stars[4 * i];
+        uint32_t first, count;
+        std::memcpy(&first, &stars[4 * i + 2], 4);
+        std::memcpy(&count, &stars[4 * i + 3], 4);
+        for (uint32_t k = first; k < first + count && 12ull * (k + 1) <= 4 * (n_star_vec4 - n_stars); ++k) {
+            const float* p = segs + 12ull * k;
+            st.segments.push_back({v4(p), v4(p + 4), p[8], p[9]});
+        }
+        sc.stars.push_back(st);
+        sc.star_cn.push_back(stars[4 * i + 1]);
+    }
+    return b;
+}
+
+int orc_scene_info(void* s, OrcSceneInfo* o) {
+    auto* b = (SceneBox*)s;
+    std::memset(o, 0, sizeof(*o));
+    if (b->fp64) info_t(*b->d, o);
+    else info_t(*b->f, o);
+    return 0;
+}
+
+int orc_scene_pack(void* s, void* nodes, void* geoms, void* attrs, void* mats, float* stars, uint32_t* order) {
+    auto* b = (SceneBox*)s;
+    if (b->fp64) return -1;
+    pack_scene(b->f->scene, (PNode*)nodes, (PGeom*)geoms, (PAttr*)attrs, (PMat*)mats, stars, order);
+    return 0;
+}
+
+int orc_render(void* s, const OrcCamera* c, const OrcConfig* cf, const OrcDynamics* dy, int threads, int perturb,
+               const OrcPixelOut* out) {
+    auto* b = (SceneBox*)s;
+    if (!out || !out->rgb || cf->width == 0 || cf->height == 0) return -1;
+    if (b->fp64) return render_t(b->d->scene, c, cf, dy, threads, perturb, out);
+    return render_t(b->f->scene, c, cf, dy, threads, perturb, out);
+}
+
+int orc_observers(uint64_t seed, uint32_t n, OrcObserver* out) {
+    auto obs = synth_observers(seed, n);
+    for (uint32_t i = 0; i < n; ++i) {
+        out[i].width = obs[i].width;
+        out[i].height = obs[i].height;
+        out[i].slice_mode = obs[i].slice_mode;
+        out[i].pad = 0;
+        for (int k = 0; k < 4; ++k) out[i].pos[k] = obs[i].pos[k];
+        for (int k = 0; k < 3; ++k) out[i].rapidity[k] = obs[i].rapidity[k];
+    }
+    return 0;
+}
+
+// The camera tetrad the oracle renders with (rows e0..e3), in float or double.
+int orc_tetrad(const OrcCamera* c, int fp64, double* out16) {
+    if (fp64) {
+        auto t = make_tetrad<double>(*c);
+        for (int a = 0; a < 4; ++a) for (int k = 0; k < 4; ++k) out16[4 * a + k] = t.e[a].axis(k);
+    } else {
+        auto t = make_tetrad<float>(*c);
+        for (int a = 0; a < 4; ++a) for (int k = 0; k < 4; ++k) out16[4 * a + k] = (double)t.e[a].axis(k);
+    }
+    return 0;
+}
+
+// The reference's gamma LUT (renderer.rs:1102-1114).
+int orc_gamma_lut(uint8_t* out4096) {
+    const auto& l = gamma_lut();
+    std::memcpy(out4096, l.data(), l.size());
+    return 0;
+}
+
+// Bloom + pack of a float HDR image (bloom.rs:93-125 then renderer.rs:1116-1129).
+int orc_bloom_pack(const float* hdr3, uint32_t w, uint32_t h, uint32_t* rgb, float* bloomed3) {
+    std::vector<V3<float>> img((size_t)w * h);
+    for (size_t i = 0; i < img.size(); ++i) img[i] = V3<float>(hdr3[3 * i], hdr3[3 * i + 1], hdr3[3 * i + 2]);
+    bloom_apply(img, w, h);
+    for (size_t i = 0; i < img.size(); ++i) {
+        if (rgb) rgb[i] = pack_rgb(img[i]);
+        if (bloomed3) { bloomed3[3 * i] = img[i].x; bloomed3[3 * i + 1] = img[i].y; bloomed3[3 * i + 2] = img[i].z; }
+    }
+    return 0;
+}
+
+}  // extern "C"

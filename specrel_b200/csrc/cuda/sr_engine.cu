@@ -1,0 +1,497 @@
+// The C ABI of include/specrel.h: contexts, scene upload (with host-side validation), frame
+// buffers and the render entry points. Mirrors GpuRenderer (gpu.rs:432-901): the context owns
+// the device copies of every scene, one stream, and the per-resolution frame buffers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../../include/specrel.h"
+#include "../../../include/specrel_scene.h"
+#include "sr_fast.h"
+#include "sr_kernels.h"
+
+using namespace srk;
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+        if (n == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct SceneSlot {
+    bool present = false;
+    DevBuf nodes, geoms, attrs, mats, stars, l2o;
+    uint32_t num_nodes = 0, num_prims = 0, num_mats = 0, num_stars = 0;
+    uint64_t num_star_vec4 = 0;
+    float light_pos[4] = {0, 0, 0, 0};
+    double anchor[4] = {0, 0, 0, 0};
+    uint32_t depth = 0;
+    bool has_l2o = false;
+    FastScene fast;  // the B200 node layout
+    SrTuning tuning{};
+};
+
+struct Frame {
+    uint32_t w = 0, h = 0;
+    Pyramid pyr{};
+    DevBuf hdr, rgb, hit, lam, tau;
+};
+
+}  // namespace
+
+struct sr_ctx {
+    int device = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    std::string last_error;
+    std::string name;
+    DevBuf tables, counters, cam;
+    BBConst bb{};
+    std::vector<std::unique_ptr<SceneSlot>> scenes;
+    Frame frame;
+    cudaEvent_t ev[8] = {};
+    FastCtx fast;
+};
+
+namespace {
+
+sr_status fail(sr_ctx* c, sr_status s, const std::string& m) {
+    if (c) c->last_error = m;
+    return s;
+}
+sr_status cuda_fail(sr_ctx* c, cudaError_t e, const char* where) {
+    return fail(c, e == cudaErrorMemoryAllocation ? SR_ERR_OUT_OF_MEMORY : SR_ERR_CUDA,
+                std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define CK(expr, where)                                \
+    do {                                               \
+        cudaError_t e_ = (expr);                       \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
+    } while (0)
+
+// Blackbody constants (star.rs:162-180): powi(5) folded in double precision, white-point Planck
+// values in f32, as the compiled reference evaluates them.
+BBConst make_bb() {
+    auto p5 = [](float l) { return (float)std::pow((double)l, 5.0); };
+    auto planck = [&](float l, float t) {
+        float x = std::fmin(14388.0f / (l * std::fmax(t, 1.0f)), 80.0f);
+        return 1.0f / (p5(l) * (std::exp(x) - 1.0f));
+    };
+    BBConst b;
+    b.r5 = p5(0.610f);
+    b.g5 = p5(0.550f);
+    b.b5 = p5(0.465f);
+    b.wr = planck(0.610f, 6504.0f);
+    b.wg = planck(0.550f, 6504.0f);
+    b.wb = planck(0.465f, 6504.0f);
+    return b;
+}
+
+SceneDev scene_dev(const sr_ctx* ctx, const SceneSlot& s) {
+    SceneDev d{};
+    d.nodes = s.nodes.as<SrGpuNode>();
+    d.geoms = s.geoms.as<float4>();
+    d.attrs = s.attrs.as<float4>();
+    d.mats = s.mats.as<float4>();
+    d.stars = s.stars.as<float4>();
+    d.leaf_to_orig = s.has_l2o ? s.l2o.as<uint32_t>() : nullptr;
+    d.tables = ctx->tables.as<uint32_t>();
+    d.wide = s.fast.wide.as<uint4>();
+    d.num_nodes = s.num_nodes;
+    d.num_prims = s.num_prims;
+    d.num_mats = s.num_mats;
+    d.num_stars = s.num_stars;
+    return d;
+}
+
+sr_status ensure_frame(sr_ctx* ctx, uint32_t w, uint32_t h) {
+    Frame& f = ctx->frame;
+    if (f.w == w && f.h == h && f.hdr.p) return SR_OK;
+    Pyramid p = make_pyramid(w, h);
+    CK(f.hdr.ensure((size_t)p.off[SR_BLOOM_LEVELS + 1] * sizeof(float4)), "frame hdr");
+    CK(f.rgb.ensure((size_t)w * h * 4), "frame rgb");
+    f.pyr = p;
+    f.w = w;
+    f.h = h;
+    return SR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+sr_status sr_create(int device, sr_ctx** out, char* err, size_t errlen) {
+    auto set = [&](const std::string& m) {
+        if (err && errlen) { std::strncpy(err, m.c_str(), errlen - 1); err[errlen - 1] = 0; }
+    };
+    if (!out) { set("out is null"); return SR_ERR_INVALID_ARGUMENT; }
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) { set(std::string("no CUDA device: ") + cudaGetErrorString(e)); return SR_ERR_NO_DEVICE; }
+    if (device < 0 || device >= n) { set("device index out of range"); return SR_ERR_INVALID_ARGUMENT; }
+    auto ctx = std::make_unique<sr_ctx>();
+    ctx->device = device;
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) { set(cudaGetErrorString(e)); return SR_ERR_CUDA; }
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, device);
+    ctx->name = std::string(prop.name) + " (CUDA sm_" + std::to_string(prop.major) + std::to_string(prop.minor) + ")";
+    if (prop.major < 10) { set("this build targets sm_100a (B200); device is " + ctx->name); return SR_ERR_UNSUPPORTED; }
+    if ((e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking)) != cudaSuccess) { set(cudaGetErrorString(e)); return SR_ERR_CUDA; }
+    ctx->stream = ctx->own;
+    std::vector<uint32_t> tables(SR_GAMMA_LUT_SIZE + 14 * 7);
+    sr_tables_build(tables.data());
+    if ((e = ctx->tables.ensure(tables.size() * 4)) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->tables.p, tables.data(), tables.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = ctx->counters.ensure(64)) != cudaSuccess || (e = cudaMemset(ctx->counters.p, 0, 64)) != cudaSuccess ||
+        (e = ctx->cam.ensure(8 * sizeof(float4))) != cudaSuccess) {
+        set(cudaGetErrorString(e));
+        return SR_ERR_CUDA;
+    }
+    for (auto& ev : ctx->ev)
+        if ((e = cudaEventCreate(&ev)) != cudaSuccess) { set(cudaGetErrorString(e)); return SR_ERR_CUDA; }
+    ctx->bb = make_bb();
+    if (fast_init(ctx->fast, prop) != cudaSuccess) { set("fast path init failed"); return SR_ERR_CUDA; }
+    *out = ctx.release();
+    return SR_OK;
+}
+
+void sr_destroy(sr_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& ev : ctx->ev) if (ev) cudaEventDestroy(ev);
+    fast_release(ctx->fast);
+    ctx->scenes.clear();
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    delete ctx;
+}
+
+const char* sr_last_error(const sr_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+sr_status sr_adapter_name(const sr_ctx* ctx, char* buf, size_t len) {
+    if (!ctx || !buf || !len) return SR_ERR_INVALID_ARGUMENT;
+    std::strncpy(buf, ctx->name.c_str(), len - 1);
+    buf[len - 1] = 0;
+    return SR_OK;
+}
+
+sr_status sr_set_stream(sr_ctx* ctx, void* s) {
+    if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+    ctx->stream = s ? (cudaStream_t)s : ctx->own;
+    return SR_OK;
+}
+
+sr_status sr_synchronize(sr_ctx* ctx) {
+    if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return SR_OK;
+}
+
+sr_status sr_upload_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d) {
+    if (!ctx || !d) return SR_ERR_INVALID_ARGUMENT;
+    if (idx > 4096) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "scene index too large");
+    uint32_t depth = 0;
+    char why[256] = {0};
+    if (sr_scene_validate(d, &depth, why, sizeof(why)) != SR_OK)
+        return fail(ctx, SR_ERR_BAD_SCENE, std::string("invalid scene: ") + why);
+    CK(cudaSetDevice(ctx->device), "set device");
+    if (ctx->scenes.size() <= idx) ctx->scenes.resize(idx + 1);
+    auto slot = std::make_unique<SceneSlot>();
+    SceneSlot& s = *slot;
+    auto up = [&](DevBuf& b, const void* src, size_t bytes, const char* what) -> cudaError_t {
+        cudaError_t e = b.ensure(std::max<size_t>(bytes, 16));
+        if (e != cudaSuccess || !bytes) return e;
+        return cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice);
+        (void)what;
+    };
+    CK(up(s.nodes, d->nodes, (size_t)d->num_nodes * sizeof(SrGpuNode), "nodes"), "upload nodes");
+    CK(up(s.geoms, d->geoms, (size_t)d->num_prims * sizeof(SrGpuGeom), "geoms"), "upload geoms");
+    CK(up(s.attrs, d->attrs, (size_t)d->num_prims * sizeof(SrGpuAttr), "attrs"), "upload attrs");
+    CK(up(s.mats, d->materials, (size_t)d->num_materials * sizeof(SrGpuMaterial), "materials"), "upload materials");
+    CK(up(s.stars, d->stars, (size_t)d->num_star_vec4 * 16, "stars"), "upload stars");
+    if (d->leaf_to_orig) {
+        CK(up(s.l2o, d->leaf_to_orig, (size_t)d->num_prims * 4, "order"), "upload order");
+        s.has_l2o = true;
+    }
+    s.num_nodes = d->num_nodes;
+    s.num_prims = d->num_prims;
+    s.num_mats = d->num_materials;
+    s.num_stars = d->num_stars;
+    s.num_star_vec4 = d->num_star_vec4;
+    s.depth = depth;
+    for (int k = 0; k < 4; ++k) {
+        s.light_pos[k] = d->light_pos[k];
+        s.anchor[k] = d->anchor ? d->anchor[k] : 0.0;
+    }
+    CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, depth, ctx->stream), "build node layout");
+    s.tuning = fast_default_tuning(ctx->fast);
+    CK(cudaStreamSynchronize(ctx->stream), "upload sync");
+    s.present = true;
+    ctx->scenes[idx] = std::move(slot);
+    return SR_OK;
+}
+
+sr_status sr_update_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d, const SrRange* nr, uint32_t n_nr,
+                          const SrRange* pr, uint32_t n_pr) {
+    if (!ctx || !d) return SR_ERR_INVALID_ARGUMENT;
+    if (idx >= ctx->scenes.size() || !ctx->scenes[idx] || !ctx->scenes[idx]->present)
+        return sr_upload_scene(ctx, idx, d);
+    SceneSlot& s = *ctx->scenes[idx];
+    bool fits = (size_t)d->num_nodes * sizeof(SrGpuNode) <= s.nodes.bytes &&
+                (size_t)d->num_prims * sizeof(SrGpuGeom) <= s.geoms.bytes &&
+                (size_t)d->num_prims * sizeof(SrGpuAttr) <= s.attrs.bytes && (size_t)d->num_star_vec4 * 16 <= s.stars.bytes &&
+                d->num_materials == s.num_mats && (!d->leaf_to_orig || s.has_l2o);
+    for (uint32_t i = 0; i < n_nr && fits; ++i) fits = nr[i].start <= nr[i].end && nr[i].end <= d->num_nodes;
+    for (uint32_t i = 0; i < n_pr && fits; ++i) fits = pr[i].start <= pr[i].end && pr[i].end <= d->num_prims;
+    if (!fits) return sr_upload_scene(ctx, idx, d);  // gpu.rs:730: upload afresh
+    uint32_t depth = 0;
+    char why[256] = {0};
+    if (sr_scene_validate(d, &depth, why, sizeof(why)) != SR_OK)
+        return fail(ctx, SR_ERR_BAD_SCENE, std::string("invalid scene: ") + why);
+    CK(cudaSetDevice(ctx->device), "set device");
+    for (uint32_t i = 0; i < n_nr; ++i) {  // write_ranges (gpu.rs:325-330)
+        size_t a = nr[i].start, b = nr[i].end;
+        if (b > a) CK(cudaMemcpyAsync(s.nodes.as<SrGpuNode>() + a, d->nodes + a, (b - a) * sizeof(SrGpuNode), cudaMemcpyHostToDevice, ctx->stream), "patch nodes");
+    }
+    for (uint32_t i = 0; i < n_pr; ++i) {
+        size_t a = pr[i].start, b = pr[i].end;
+        if (b <= a) continue;
+        CK(cudaMemcpyAsync(s.geoms.as<SrGpuGeom>() + a, d->geoms + a, (b - a) * sizeof(SrGpuGeom), cudaMemcpyHostToDevice, ctx->stream), "patch geoms");
+        CK(cudaMemcpyAsync(s.attrs.as<SrGpuAttr>() + a, d->attrs + a, (b - a) * sizeof(SrGpuAttr), cudaMemcpyHostToDevice, ctx->stream), "patch attrs");
+        if (d->leaf_to_orig)
+            CK(cudaMemcpyAsync(s.l2o.as<uint32_t>() + a, d->leaf_to_orig + a, (b - a) * 4, cudaMemcpyHostToDevice, ctx->stream), "patch order");
+    }
+    if (d->num_star_vec4)
+        CK(cudaMemcpyAsync(s.stars.p, d->stars, (size_t)d->num_star_vec4 * 16, cudaMemcpyHostToDevice, ctx->stream), "patch stars");
+    s.num_nodes = d->num_nodes;
+    s.num_prims = d->num_prims;
+    s.num_stars = d->num_stars;
+    s.num_star_vec4 = d->num_star_vec4;
+    s.depth = depth;
+    CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, depth, ctx->stream), "rebuild node layout");
+    CK(cudaStreamSynchronize(ctx->stream), "update sync");
+    return SR_OK;
+}
+
+sr_status sr_scene_stats(const sr_ctx* ctx, uint32_t idx, SrSceneStats* o) {
+    if (!ctx || !o || idx >= ctx->scenes.size() || !ctx->scenes[idx]) return SR_ERR_INVALID_ARGUMENT;
+    const SceneSlot& s = *ctx->scenes[idx];
+    std::memset(o, 0, sizeof(*o));
+    o->num_nodes = s.num_nodes;
+    o->num_prims = s.num_prims;
+    o->num_stars = s.num_stars;
+    o->bvh_depth = s.depth;
+    o->device_bytes = s.nodes.bytes + s.geoms.bytes + s.attrs.bytes + s.mats.bytes + s.stars.bytes + s.l2o.bytes + s.fast.bytes();
+    o->fast_nodes = s.fast.num_wide;
+    return SR_OK;
+}
+
+sr_status sr_get_tuning(const sr_ctx* ctx, uint32_t idx, SrTuning* t) {
+    if (!ctx || !t || idx >= ctx->scenes.size() || !ctx->scenes[idx]) return SR_ERR_INVALID_ARGUMENT;
+    *t = ctx->scenes[idx]->tuning;
+    return SR_OK;
+}
+
+sr_status sr_set_tuning(sr_ctx* ctx, uint32_t idx, const SrTuning* t) {
+    if (!ctx || !t || idx >= ctx->scenes.size() || !ctx->scenes[idx]) return SR_ERR_INVALID_ARGUMENT;
+    if (!fast_tuning_valid(ctx->fast, *t)) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "tuning outside the supported set");
+    ctx->scenes[idx]->tuning = *t;
+    return SR_OK;
+}
+
+sr_status sr_render_ex(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const SrRenderOpts* opts, const SrOutputs* out,
+                       SrTimings* timings) {
+    if (!ctx || !u || !out || !out->rgb) return SR_ERR_INVALID_ARGUMENT;
+    if (idx >= ctx->scenes.size() || !ctx->scenes[idx] || !ctx->scenes[idx]->present)
+        return fail(ctx, SR_ERR_NO_SCENE, "scene " + std::to_string(idx) + " is not uploaded");
+    if (u->size[0] == 0 || u->size[1] == 0 || (uint64_t)u->size[0] * u->size[1] > (1ull << 28))
+        return fail(ctx, SR_ERR_INVALID_ARGUMENT, "frame size must be non-zero and at most 2^28 pixels");
+    if (u->mode > 3 || u->shadow_mode > 2 || u->slice_mode > 3 || u->num_flashes > SR_MAX_FLASHES || u->num_haze > SR_MAX_HAZE_ORIGINS)
+        return fail(ctx, SR_ERR_INVALID_ARGUMENT, "uniform block out of range");
+    SceneSlot& s = *ctx->scenes[idx];
+    const uint32_t path = opts ? opts->path : SR_PATH_FAST;
+    const uint32_t flags = opts ? opts->flags : 0u;
+    const bool dev_out = (flags & SR_FLAG_DEVICE_OUTPUT) != 0;
+    const bool timing = (flags & SR_FLAG_TIMING) != 0;
+    if (path != SR_PATH_PLAIN && path != SR_PATH_FAST) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "unknown path");
+    CK(cudaSetDevice(ctx->device), "set device");
+    sr_status st = ensure_frame(ctx, u->size[0], u->size[1]);
+    if (st != SR_OK) return st;
+    Frame& fr = ctx->frame;
+    const size_t npx = (size_t)u->size[0] * u->size[1];
+    FrameDev f{};
+    f.hdr = fr.hdr.as<float4>();
+    f.width = u->size[0];
+    f.height = u->size[1];
+    f.counters = ctx->counters.as<uint32_t>();
+    if (dev_out) {
+        f.rgb = out->rgb;
+        f.hit_id = out->hit_id;
+        f.lambda = out->lambda;
+        f.tau = out->tau;
+    } else {
+        f.rgb = fr.rgb.as<uint32_t>();
+        if (out->hit_id) { CK(fr.hit.ensure(npx * 4), "aux"); f.hit_id = fr.hit.as<uint32_t>(); }
+        if (out->lambda) { CK(fr.lam.ensure(npx * 4), "aux"); f.lambda = fr.lam.as<float>(); }
+        if (out->tau) { CK(fr.tau.ensure(npx * 4), "aux"); f.tau = fr.tau.as<float>(); }
+    }
+    cudaStream_t sm = ctx->stream;
+    cudaEvent_t* ev = ctx->ev;
+    auto t_host0 = std::chrono::steady_clock::now();
+    if (timing) CK(cudaEventRecord(ev[0], sm), "event");
+    CK(cudaMemsetAsync(ctx->counters.p, 0, 16, sm), "counters");
+    const float4* cam_dev = nullptr;
+    if (opts && opts->cam64) {
+        CK(launch_camera_f64(*opts->cam64, s.anchor, *u, ctx->cam.as<float4>(), sm), "camera kernel");
+        cam_dev = ctx->cam.as<float4>();
+    }
+    if (timing) CK(cudaEventRecord(ev[1], sm), "event");
+    SceneDev sd = scene_dev(ctx, s);
+    if (path == SR_PATH_PLAIN) {
+        CK(launch_render_plain(sd, *u, cam_dev, f, ctx->bb, sm), "plain render");
+        if (timing) { CK(cudaEventRecord(ev[2], sm), "event"); CK(cudaEventRecord(ev[3], sm), "event"); }
+    } else {
+        CK(fast_render(ctx->fast, s.fast, s.tuning, sd, *u, cam_dev, f, ctx->bb, sm, timing ? ev + 2 : nullptr), "fast render");
+    }
+    if (timing) CK(cudaEventRecord(ev[4], sm), "event");
+    CK(launch_bloom(f, fr.pyr, ctx->tables.as<uint32_t>(), sm), "bloom");
+    if (timing) CK(cudaEventRecord(ev[5], sm), "event");
+    if (out->hdr) CK(cudaMemcpyAsync(out->hdr, fr.hdr.p, npx * 16, dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, sm), "hdr copy");
+    if (dev_out && !timings) return SR_OK;
+    auto t_host1 = std::chrono::steady_clock::now();
+    if (!dev_out) {
+        CK(cudaMemcpyAsync(out->rgb, f.rgb, npx * 4, cudaMemcpyDeviceToHost, sm), "readback");
+        if (out->hit_id) CK(cudaMemcpyAsync(out->hit_id, f.hit_id, npx * 4, cudaMemcpyDeviceToHost, sm), "readback");
+        if (out->lambda) CK(cudaMemcpyAsync(out->lambda, f.lambda, npx * 4, cudaMemcpyDeviceToHost, sm), "readback");
+        if (out->tau) CK(cudaMemcpyAsync(out->tau, f.tau, npx * 4, cudaMemcpyDeviceToHost, sm), "readback");
+    }
+    uint32_t counters[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(counters, ctx->counters.p, 16, cudaMemcpyDeviceToHost, sm), "counters");
+    CK(cudaStreamSynchronize(sm), "render sync");
+    auto t_host2 = std::chrono::steady_clock::now();
+    if (timings) {
+        std::memset(timings, 0, sizeof(*timings));
+        timings->submit_ms = std::chrono::duration<float, std::milli>(t_host1 - t_host0).count();
+        timings->wait_ms = std::chrono::duration<float, std::milli>(t_host2 - t_host1).count();
+        timings->shadow_rays = counters[0];
+        if (timing) {
+            cudaEventElapsedTime(&timings->kernel_ms, ev[0], ev[5]);
+            cudaEventElapsedTime(&timings->camera_ms, ev[0], ev[1]);
+            cudaEventElapsedTime(&timings->trace_ms, ev[1], ev[2]);
+            cudaEventElapsedTime(&timings->shade_ms, ev[2], ev[3]);
+            cudaEventElapsedTime(&timings->stars_ms, ev[3], ev[4]);
+            cudaEventElapsedTime(&timings->bloom_ms, ev[4], ev[5]);
+        }
+    }
+    if (counters[1] & ERR_TRAVERSAL_LIMIT) return fail(ctx, SR_ERR_TRAVERSAL_LIMIT, "a ray exceeded the traversal visit limit");
+    if (counters[1]) return fail(ctx, SR_ERR_BAD_SCENE, "device reported a bad index (flags " + std::to_string(counters[1]) + ")");
+    return SR_OK;
+}
+
+sr_status sr_render(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_t* fb, uint64_t fb_len, SrTimings* t) {
+    if (!ctx || !u || !fb) return SR_ERR_INVALID_ARGUMENT;
+    if (fb_len != (uint64_t)u->size[0] * u->size[1])
+        return fail(ctx, SR_ERR_INVALID_ARGUMENT, "framebuffer size mismatch");  // gpu.rs:808
+    SrOutputs o{};
+    o.rgb = fb;
+    return sr_render_ex(ctx, idx, u, nullptr, &o, t);
+}
+
+sr_status sr_render_batch(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const SrCameraF64* cam64, uint32_t n,
+                          uint32_t* rgb_out, uint64_t rgb_len, uint32_t flags, SrTimings* timings) {
+    if (!ctx || (!u && n) || (!rgb_out && n)) return SR_ERR_INVALID_ARGUMENT;
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < n; ++i) total += (uint64_t)u[i].size[0] * u[i].size[1];
+    if (total != rgb_len) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "rgb_len must equal the sum of the observers' pixels");
+    const bool dev_out = (flags & SR_FLAG_DEVICE_OUTPUT) != 0;
+    DevBuf staging;
+    uint32_t* dst = rgb_out;
+    if (!dev_out) {
+        CK(staging.ensure(total * 4), "batch staging");
+        dst = staging.as<uint32_t>();
+    }
+    cudaEvent_t* ev = ctx->ev;
+    if (timings) CK(cudaEventRecord(ev[6], ctx->stream), "event");
+    uint64_t off = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        SrRenderOpts o{SR_PATH_FAST, SR_FLAG_DEVICE_OUTPUT, cam64 ? cam64 + i : nullptr};
+        SrOutputs out{};
+        out.rgb = dst + off;
+        sr_status s = sr_render_ex(ctx, idx, u + i, &o, &out, nullptr);
+        if (s != SR_OK) return s;
+        off += (uint64_t)u[i].size[0] * u[i].size[1];
+    }
+    if (timings) CK(cudaEventRecord(ev[7], ctx->stream), "event");
+    if (!dev_out) CK(cudaMemcpyAsync(rgb_out, dst, total * 4, cudaMemcpyDeviceToHost, ctx->stream), "batch readback");
+    if (!dev_out || timings) CK(cudaStreamSynchronize(ctx->stream), "batch sync");
+    if (timings) {
+        std::memset(timings, 0, sizeof(*timings));
+        cudaEventElapsedTime(&timings->kernel_ms, ev[6], ev[7]);
+    }
+    return SR_OK;
+}
+
+sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_t n, SrTuning* best, float* best_ms) {
+    if (!ctx || !u || idx >= ctx->scenes.size() || !ctx->scenes[idx]) return SR_ERR_INVALID_ARGUMENT;
+    SceneSlot& s = *ctx->scenes[idx];
+    const size_t npx = (size_t)u->size[0] * u->size[1];
+    DevBuf out;
+    CK(out.ensure(npx * 4), "autotune output");
+    SrOutputs o{};
+    o.rgb = out.as<uint32_t>();
+    SrRenderOpts opts{SR_PATH_FAST, SR_FLAG_DEVICE_OUTPUT, nullptr};
+    SrTuning keep = s.tuning, win = s.tuning;
+    float win_ms = INFINITY;
+    const uint32_t threads[] = {64, 128, 256};
+    const uint32_t per_sm[] = {4, 8, 16};
+    const uint32_t tiles[][2] = {{8, 4}, {4, 8}, {16, 2}};
+    for (uint32_t bt : threads)
+        for (uint32_t bs : per_sm)
+            for (auto& tl : tiles) {
+                SrTuning t = keep;
+                t.block_threads = bt;
+                t.blocks_per_sm = bs;
+                t.tile_w = tl[0];
+                t.tile_h = tl[1];
+                if (!fast_tuning_valid(ctx->fast, t)) continue;
+                s.tuning = t;
+                sr_status st = sr_render_ex(ctx, idx, u, &opts, &o, nullptr);  // warm-up
+                if (st != SR_OK) { s.tuning = keep; return st; }
+                CK(cudaEventRecord(ctx->ev[6], ctx->stream), "event");
+                for (uint32_t i = 0; i < std::max(1u, n); ++i) {
+                    st = sr_render_ex(ctx, idx, u, &opts, &o, nullptr);
+                    if (st != SR_OK) { s.tuning = keep; return st; }
+                }
+                CK(cudaEventRecord(ctx->ev[7], ctx->stream), "event");
+                CK(cudaEventSynchronize(ctx->ev[7]), "event sync");
+                float ms = 0;
+                cudaEventElapsedTime(&ms, ctx->ev[6], ctx->ev[7]);
+                ms /= (float)std::max(1u, n);
+                if (ms < win_ms) { win_ms = ms; win = t; }
+            }
+    s.tuning = win;
+    if (best) *best = win;
+    if (best_ms) *best_ms = win_ms;
+    return SR_OK;
+}
+
+}  // extern "C"

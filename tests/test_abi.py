@@ -1,0 +1,104 @@
+"""The C ABI: the library loads without a GPU, exports every function the headers declare, its
+structs have the reference's layouts, and the host-side scene checks reject bad input."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def declared_functions():
+    names = set()
+    for h in ("specrel.h", "specrel_scene.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(sr_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    import specrel_b200._lib as L
+    lib = C.CDLL(L.LIB_PATH)
+    names = declared_functions()
+    assert len(names) >= 25
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert names == set(L.SIGNATURES), sorted(names ^ set(L.SIGNATURES))
+
+
+def test_struct_layouts_match_the_reference():
+    import specrel_b200._lib as L
+    assert L.NODE_DTYPE.itemsize == 48       # GpuNode, gpu.rs:44-51
+    assert L.GEOM_DTYPE.itemsize == 80       # GpuGeom, gpu.rs:68-74
+    assert L.ATTR_DTYPE.itemsize == 192      # GpuAttr, gpu.rs:79-92
+    assert L.MAT_DTYPE.itemsize == 48        # GpuMaterial, gpu.rs:96-100
+    assert C.sizeof(L.GpuUniforms) == 768    # GpuUniforms, gpu.rs:122-144
+    U = L.GpuUniforms
+    offs = {"light_pos": 80, "num_nodes": 124, "frontier_origin": 128, "frontier_view_offset": 144,
+            "num_flashes": 148, "frontier_tau": 152, "num_haze": 160, "num_stars": 164, "haze_origin": 176,
+            "flash_at": 256, "flash_col_width": 512}
+    for k, v in offs.items():
+        assert getattr(U, k).offset == v, k
+    assert L.ATTR_DTYPE.fields["misc"][1] == 160 and L.ATTR_DTYPE.fields["decided_at"][1] == 176
+
+
+def test_create_without_device_fails_cleanly():
+    import specrel_b200 as sr
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(sr.SrError) as e:
+        sr.Engine(0)
+    assert e.value.status == sr._lib.SR_ERR_NO_DEVICE
+
+
+def _tiny_scene():
+    import specrel_b200 as sr
+    s = sr.synth_scene(1, 3, n_bodies=2, steps=2)
+    return s.packed()
+
+
+def test_validate_accepts_built_scene():
+    import specrel_b200 as sr
+    p = _tiny_scene()
+    st, depth, msg = sr.validate(p)
+    assert st == 0, msg
+    assert depth >= 2
+
+
+@pytest.mark.parametrize("breakage", ["child_out_of_range", "cycle", "leaf_range", "material", "order", "star"])
+def test_validate_rejects_corrupt_scene(breakage):
+    import specrel_b200 as sr
+    p = _tiny_scene()
+    nodes = p.nodes.copy()
+    internal = np.nonzero(nodes["count"] == 0)[0]
+    leaves = np.nonzero(nodes["count"] > 0)[0]
+    if breakage == "child_out_of_range":
+        nodes["left"][internal[0]] = len(nodes) + 5
+    elif breakage == "cycle":
+        nodes["right_or_first"][internal[-1]] = 0
+    elif breakage == "leaf_range":
+        nodes["right_or_first"][leaves[0]] = len(p.geoms)
+    elif breakage == "material":
+        attrs = p.attrs.copy()
+        attrs["misc"][0, 2] = np.uint32(99).view(np.float32)
+        p.attrs = attrs
+    elif breakage == "order":
+        p.leaf_to_orig = p.leaf_to_orig.copy()
+        p.leaf_to_orig[3] = len(p.geoms) + 1
+    elif breakage == "star":
+        st = np.zeros(4 + 12, np.float32)
+        st[2] = np.uint32(0).view(np.float32)
+        st[3] = np.uint32(2).view(np.float32)  # two segments, only one present
+        p.stars = st
+        p.num_stars = 1
+    p.nodes = nodes
+    status, _, msg = sr.validate(p)
+    assert status == sr._lib.SR_ERR_BAD_SCENE, breakage
+    assert msg

@@ -1,0 +1,138 @@
+"""GPU parity: the engine's plain and fast paths against the CPU oracle on the same packed scene.
+
+Bar: hit ids equal on non-grazing rays (the engine also matches on grazing ones, since it visits
+the tree in the reference's order), lambda and tau within 1e-5 relative (they are bit-identical
+here), RGB8 within 1/255 outside the near-threshold mask, and the reference's own CPU/GPU criterion
+(fewer than 0.5% of pixels differ by more than 4, gpu.rs:1233-1251) everywhere.
+"""
+import numpy as np
+import pytest
+
+import specrel_b200 as sr
+from oracle import oracle as O
+from parity import compare, oracle_frames, packed_from_oracle
+
+pytestmark = pytest.mark.gpu
+
+PATHS = [sr.SR_PATH_PLAIN, sr.SR_PATH_FAST]
+
+
+def _assert_parity(rep, label, near_max=0.02):
+    print(label, rep)
+    assert rep.hit_match_nongrazing == 1.0, (label, str(rep))
+    assert rep.hit_match >= 0.9999, (label, str(rep))
+    assert rep.lam_max_rel <= 1e-5 and rep.tau_max_rel <= 1e-5, (label, str(rep))
+    assert rep.rgb_max_unmasked <= 1, (label, str(rep))
+    assert rep.near_threshold_frac <= near_max, (label, str(rep))
+    assert rep.frac_gt4 < 0.005, (label, str(rep))
+
+
+@pytest.fixture(scope="module")
+def cubes(engine):
+    s = O.Scene(O.synth_params(1, 1))
+    engine.upload(0, packed_from_oracle(s))
+    return s
+
+
+def _render_both(engine, idx, scene, cam_o, cam_e, w, h, mode=0, shadow=0, slice_=0, dyn=None, uargs=None,
+                 path=sr.SR_PATH_FAST):
+    cfg = O.make_config(w, h, mode, shadow, slice_)
+    base, near = oracle_frames(scene, cam_o, cfg, dyn)
+    u = sr.uniforms(cam_e, w, h, mode, shadow, slice_, num_nodes=int(scene.info.n_nodes),
+                    num_stars=int(scene.info.n_stars), **(uargs or {}))
+    fr = engine.render(idx, u, path=path, aux=True)
+    return compare(fr, base, near), fr, base
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_config1_320x200_matches_oracle(engine, cubes, path):
+    """64 inertial cubes, camera at rest at the origin, 90 degrees, past cone, no shadows."""
+    rep, fr, base = _render_both(engine, 0, cubes, O.make_camera(), sr.camera(), 320, 200, path=path)
+    _assert_parity(rep, f"config1 path={path}")
+    assert (fr.hit_id != 0xFFFFFFFF).sum() > 100
+    # lambda and tau are bit-identical (same operations, no FMA contraction).
+    hit = base.orig != 0xFFFFFFFF
+    assert (fr.lam[hit] == base.lam[hit].astype(np.float32)).all()
+    assert (fr.tau[hit] == base.tau[hit].astype(np.float32)).all()
+
+
+MODES = [  # gpu.rs:1268-1278
+    (0, 1, 0), (0, 2, 1), (1, 0, 0), (2, 0, 0), (3, 0, 0), (3, 0, 3), (0, 1, 2), (0, 2, 3), (1, 0, 2),
+]
+
+
+@pytest.mark.parametrize("mode,shadow,slice_", MODES)
+@pytest.mark.parametrize("path", PATHS)
+def test_modes_with_boosted_rotated_observer(engine, cubes, mode, shadow, slice_, path):
+    pos = (-8.0, 2.0, 1.0, -26.0)
+    kw = dict(rapidity=(0.2, 0.0, 0.6), yaw=0.15, pitch=-0.05)
+    co = O.make_camera(pos=pos, fov_deg=65.0, **kw)
+    ce = sr.camera(pos, 65.0, **kw)
+    rep, fr, base = _render_both(engine, 0, cubes, co, ce, 192, 120, mode, shadow, slice_, path=path)
+    _assert_parity(rep, f"mode={mode} shadow={shadow} slice={slice_} path={path}", near_max=0.05)
+
+
+def test_flashes_haze_and_frontier(engine, cubes):
+    pos = (0.0, 0.0, 0.0, -24.0)
+    co, ce = O.make_camera(pos=pos, fov_deg=65.0), sr.camera(pos, 65.0)
+    flashes = [((pos[0] - 6.0, pos[1], pos[2], pos[3]), 1.2, 2.0, (1.0, 0.3, 0.2)),
+               ((pos[0] - 12.0, pos[1], pos[2], pos[3]), 1.5, 3.0, (0.2, 0.6, 1.0))]
+    remote = [(pos[0] - 3.0, 2.0, 0.0, pos[3] + 6.0)]
+    frontier = ((pos[0] - 0.5, 0.2, 0.0, pos[3]), 24.0)
+    for mode, shadow, slice_ in [(0, 1, 0), (3, 0, 1), (3, 0, 3), (0, 0, 3)]:
+        dyn = O.DynamicsSpec(frontier=frontier, flashes=flashes, remote_origins=remote)
+        rep, fr, base = _render_both(engine, 0, cubes, co, ce, 192, 120, mode, shadow, slice_, dyn,
+                                     uargs=dict(frontier=frontier, flashes=flashes, remote_origins=remote))
+        # Flash colours reach the kernel premultiplied by intensity (gpu.rs:160-167), one rounding
+        # away from the CPU's product; that can move a pixel by one level.
+        _assert_parity(rep, f"dynamics mode={mode} slice={slice_}", near_max=0.05)
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_config2_reduced_accelerated_bodies_with_null_shadows(engine, path):
+    """configs[1]'s scene type at reduced size: accelerated icospheres, boosted observer, null shadows."""
+    s = O.Scene(O.synth_params(2, 4, n_bodies=24, steps=24))
+    engine.upload(1, packed_from_oracle(s))
+    rap = tuple(s.info.cam_rapidity)
+    rep, fr, base = _render_both(engine, 1, s, O.make_camera(rapidity=rap), sr.camera(rapidity=rap), 320, 200,
+                                 0, 1, 0, path=path)
+    _assert_parity(rep, f"config2-reduced path={path}")
+    assert (fr.hit_id != 0xFFFFFFFF).mean() > 0.02
+    assert fr.timings.shadow_rays > 500
+
+
+def test_stars_reduced(engine):
+    """Point stars with Doppler colour over the cube occluders (configs[4]'s scene at reduced size)."""
+    s = O.Scene(O.synth_params(5, 2, n_bodies=8, steps=16, n_stars=3000))
+    engine.upload(2, packed_from_oracle(s))
+    rap = tuple(s.info.cam_rapidity)
+    for path in PATHS:
+        rep, fr, base = _render_both(engine, 2, s, O.make_camera(rapidity=rap), sr.camera(rapidity=rap), 256, 160,
+                                     path=path)
+        _assert_parity(rep, f"stars path={path}", near_max=0.05)
+
+
+def test_host_render_entry_point_equals_render_ex(engine, cubes):
+    u = sr.uniforms(sr.camera(), 160, 100, num_nodes=int(cubes.info.n_nodes))
+    fb = np.zeros(160 * 100, np.uint32)
+    t = engine.render_host(0, u, fb)
+    fr = engine.render(0, u)
+    assert (fb == fr.rgb).all()
+    assert t.wait_ms >= 0
+
+
+def test_errors_are_statuses(engine):
+    u = sr.uniforms(sr.camera(), 64, 40)
+    with pytest.raises(sr.SrError) as e:
+        engine.render(77, u)
+    assert e.value.status == sr._lib.SR_ERR_NO_SCENE
+    fb = np.zeros(10, np.uint32)
+    with pytest.raises(sr.SrError) as e:
+        engine.render_host(0, u, fb)
+    assert e.value.status == sr._lib.SR_ERR_INVALID_ARGUMENT
+    bad = sr.synth_scene(1, 3, n_bodies=2, steps=2).packed()
+    bad.nodes = bad.nodes.copy()
+    bad.nodes["left"][0] = 10 ** 6
+    with pytest.raises(sr.SrError) as e:
+        engine.upload(9, bad)
+    assert e.value.status == sr._lib.SR_ERR_BAD_SCENE
