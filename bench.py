@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Headline benchmark: primary rays per second on the 7.9M-tetrahedron 1280x800 scene.
+
+Workload: 64 accelerated icospheres (subdivision 2) on Fermi-Walker
+worldlines, 128 time steps, ~7.9M tetrahedra; observers at t = 0 at the origin with rapidities
+|phi| <= 2; 1280x800; past light cone; Lorentz-invariant null shadows from a point light at
+(0, 50, 0); FP32 traversal. Synthetic, seeded (the reference ships no scenes for these configs).
+
+One step renders a batch of B observers (B frames of 1,024,000 rays each) through the batched
+fast path with the FP64 camera (tetrad and event built in double on the GPU, rebased to the scene
+anchor). `value` is Mrays/s over all ranks (weak scaling: every rank renders its own batch of
+observers, no data-path collective). The plain single-frame path is timed on the same observers
+for comparison (`plain`), as is the end-to-end call through the C ABI with host buffers (`e2e`).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H = 1280, 800
+RAYS_PER_FRAME = W * H
+METRIC = "Mrays/s on 1 B200, 1280x800 8M-tet scene (batched fast path); primary rays"
+UNIT = "Mrays/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--batch", type=int, default=8, help="observers (1280x800 frames) per step per GPU")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch parameters")
+    ap.add_argument("--bodies", type=int, default=64,
+                    help="icospheres in the scene (64 is the workload; fewer only for small profiling captures)")
+    return ap.parse_args()
+
+
+def observer_rapidities(seed: int, rank: int, n: int, first):
+    """Rapidities of a rank's observers: the workload's own observer first, then seeded draws
+    uniform in the ball |phi| <= 2."""
+    rng = np.random.default_rng(seed * 7919 + rank)
+    out = []
+    for i in range(n):
+        if rank == 0 and i == 0:
+            out.append(tuple(float(x) for x in first))
+            continue
+        while True:
+            v = rng.uniform(-1.0, 1.0, 3)
+            if v @ v < 1.0:
+                break
+        out.append(tuple(float(2.0 * x) for x in v))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "trace_fast_config2.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch"), d
+    return None, None
+
+
+def cpu_baseline(packed, cam_rapidity, sample_stride=8):
+    """The reference CPU renderer (oracle/: the C++ restatement of renderer.rs, f32, rows over all
+    host threads, serial bloom) on a bounded sample of the same frame: every `sample_stride`-th row
+    of the 1280x800 frame (1280 x 100 rays), one warm-up then the median of 3."""
+    from oracle import oracle as O
+    sc = O.Scene.from_packed(packed.nodes, packed.geoms, packed.attrs, packed.materials, packed.stars,
+                             packed.num_stars, packed.light_pos)
+    cam = O.make_camera(rapidity=cam_rapidity)
+    rows = H // sample_stride
+    cfg = O.make_config(W, rows, 0, 1, 0, full_height=H, row_stride=sample_stride, row_offset=sample_stride // 2)
+    threads = os.cpu_count() or 1
+    O.render(sc, cam, cfg, threads=threads, aux=False)
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        O.render(sc, cam, cfg, threads=threads, aux=False)
+        ts.append(time.perf_counter() - t0)
+    t = float(np.median(ts))
+    return {"value": W * rows / t / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"rows {sample_stride // 2}::{sample_stride} of the 1280x800 frame ({W}x{rows} rays, shadows "
+                      f"on, bloom on the sample), oracle C++ f32 restatement of render_frame, median of 3 after a "
+                      f"warm-up; {t * 1e3:.1f} ms per sample"}
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the reference's CPU renderer (Rust) cannot be built here (no cargo/rustc),
+    so its C++ restatement in oracle/ is timed on the host cores, on the engine arm's workload."""
+    if rank != 0:
+        return
+    import specrel_b200 as sr
+    from oracle import oracle as O
+    scene = sr.synth_scene(2, args.seed)
+    p = scene.packed()
+    sc = O.Scene.from_packed(p.nodes, p.geoms, p.attrs, p.materials, p.stars, p.num_stars, p.light_pos)
+    rap = tuple(scene.info.cam_rapidity)
+    cam = O.make_camera(rapidity=rap)
+    stride = 8
+    rows = H // stride
+    cfg = O.make_config(W, rows, 0, 1, 0, full_height=H, row_stride=stride, row_offset=stride // 2)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        O.render(sc, cam, cfg, threads=threads, aux=False)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.render(sc, cam, cfg, threads=threads, aux=False)
+        ts.append(time.perf_counter() - t0)
+    t = float(np.mean(ts))
+    v = W * rows / t / 1e6
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded configs[1] scene)", "impl": "reference",
+            "config": {"workload": "configs[1]: 64 accelerated icospheres, 7.9M tets, 1280x800, null shadows",
+                       "sample": f"every {stride}th row ({W}x{rows} rays) per step"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"every {stride}th row of the 1280x800 frame, all host threads; the Rust "
+                                       "renderer is not buildable here (no cargo/rustc), so the oracle's C++ "
+                                       "restatement of render_frame is timed"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_engine(args, rank, world, local):
+    import torch
+    import specrel_b200 as sr
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    ncpu = os.cpu_count() or 1
+    t0 = time.time()
+    scene = sr.synth_scene(2, args.seed, n_bodies=args.bodies, threads=max(1, ncpu // max(1, world)))
+    build_s = time.time() - t0
+    eng = sr.Engine(local)
+    eng.upload(0, scene)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    B = args.batch
+    raps = observer_rapidities(args.seed, rank, B, scene.info.cam_rapidity)
+    cams = [sr.camera(rapidity=r) for r in raps]
+    us = [sr.uniforms(c, W, H, 0, 1, 0, num_nodes=scene.num_nodes, light_pos=scene.light_pos) for c in cams]
+    c64 = [sr.cam64((0.0, 0.0, 0.0, 0.0), r) for r in raps]
+    out = torch.empty(B * RAYS_PER_FRAME, dtype=torch.int32, device=f"cuda:{local}")
+    ptr = out.data_ptr()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    with torch.cuda.stream(stream):
+        # Launch parameters for this scene, untimed.
+        if not args.no_autotune:
+            eng.autotune(0, us[0], 2)
+
+        def batch_step():
+            eng.render_batch(0, us, ptr, B * RAYS_PER_FRAME, cams=c64, device_output=True)
+
+        def plain_step():
+            for i in range(B):
+                eng.render_into(0, us[i], ptr + 4 * i * RAYS_PER_FRAME, path=sr.SR_PATH_PLAIN)
+
+        for _ in range(args.warmup):
+            batch_step()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clocks:
+            torch.cuda.nvtx.range_push("timed")
+            e0.record(stream)
+            for _ in range(args.steps):
+                batch_step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
+        barrier()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        ms_max = max_over_ranks(ms)
+
+        # The plain single-frame path on the same observers.
+        for _ in range(max(1, args.warmup)):
+            plain_step()
+        torch.cuda.synchronize()
+        barrier()
+        e0.record(stream)
+        k_plain = max(2, args.steps // 2)
+        for _ in range(k_plain):
+            plain_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = max_over_ranks(e0.elapsed_time(e1) / k_plain)
+
+        # End to end through the C ABI with host buffers: uniforms from pinned host memory in,
+        # framebuffers out to pinned host memory, every step.
+        host = torch.empty(B * RAYS_PER_FRAME, dtype=torch.int32, pin_memory=True)
+        hptr = host.data_ptr()
+        for _ in range(max(1, args.warmup)):
+            eng.render_batch(0, us, hptr, B * RAYS_PER_FRAME, cams=c64, device_output=False)
+        barrier()
+        torch.cuda.synchronize()
+        t_e2e = time.perf_counter()
+        e0.record(stream)
+        for _ in range(args.steps):
+            eng.render_batch(0, us, hptr, B * RAYS_PER_FRAME, cams=c64, device_output=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall_e2e = (time.perf_counter() - t_e2e) / args.steps * 1e3
+        e2e_ms = max_over_ranks(max(e0.elapsed_time(e1) / args.steps, wall_e2e))
+
+        # The dominant kernel (primary traversal), timed with events on the launching stream
+        # inside the library, and the traversal work of the same frames (counting variant).
+        trace_ms, frame_ms, shade_ms, bloom_ms = [], [], [], []
+        for i in range(B):
+            fr = eng.render(0, us[i], path=sr.SR_PATH_FAST, timing=True, cam=c64[i])
+            t = fr.timings
+            trace_ms.append(t.trace_ms)
+            shade_ms.append(t.shade_ms)
+            bloom_ms.append(t.bloom_ms)
+            frame_ms.append(t.kernel_ms)
+        work = []
+        for i in range(B):
+            fr = eng.render(0, us[i], path=sr.SR_PATH_FAST, cam=c64[i], count=True)
+            t = fr.timings
+            work.append((t.nodes_visited, t.leaves_visited, t.tets_tested, t.shadow_nodes_visited,
+                         t.shadow_leaves_visited, t.shadow_tets_tested, t.shadow_rays))
+        work = np.array(work, dtype=np.float64)
+        tuning = eng.tuning(0)
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        eng.close()
+        return
+
+    total_rays = B * RAYS_PER_FRAME * world
+    value = total_rays / (ms_max / 1e3) / 1e6
+    plain_value = total_rays / (plain_ms / 1e3) / 1e6
+    e2e_value = total_rays / (e2e_ms / 1e3) / 1e6
+    # Algorithmic bytes of one launch of the trace kernel in the B200 layout: one 80-byte wide
+    # node per internal visit, one 80-byte hot record per tetrahedron test, the 20-byte hit record
+    # written per ray, per frame (the node visits are the reference traversal's own: same order).
+    per_frame = work.mean(axis=0)
+    trace_bytes = 80.0 * per_frame[0] + 80.0 * per_frame[2] + 20.0 * RAYS_PER_FRAME
+    trace_s = float(np.median(trace_ms)) / 1e3
+    achieved = trace_bytes / trace_s / 1e9
+    peak, peak_kind = load_peaks()
+    traffic, traffic_src = load_traffic()
+    clk = clocks.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded configs[1] scene: no dataset; the reference ships no such scene)",
+        "config": {"workload": "configs[1]: 64 accelerated icospheres (subdiv 2), 128 steps, "
+                               f"{scene.num_prims} tets, 1280x800, past light cone, Lorentz-invariant null shadows, "
+                               "light (0,50,0), FP32 traversal + FP64 camera",
+                   "observers_per_step_per_gpu": B, "rays_per_step": total_rays, "seed": args.seed,
+                   "l2": "inputs larger than L2 (scene %.2f GB on the device vs 126 MB L2)" % (eng.stats(0).device_bytes / 1e9),
+                   "tuning": {k: getattr(tuning, k) for k, _ in tuning._fields_},
+                   "scene_build_s": round(build_s, 2), "parallelism": f"replicas x{world}, observers sharded"},
+        "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms,
+                  "speedup_batched_over_plain": value / plain_value},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 768 * B + 80 * B,
+                "d2h_bytes_per_step": 4 * RAYS_PER_FRAME * B},
+        "gpu_launches": int(args.steps * B * 15),
+        "roofline": {"bound": "hbm", "kernel": "k_trace_fast", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic,
+                     "algorithmic_bytes_per_launch": trace_bytes, "trace_ms": trace_s * 1e3,
+                     "frame_ms": float(np.median(frame_ms)), "shade_ms": float(np.median(shade_ms)),
+                     "bloom_ms": float(np.median(bloom_ms)),
+                     "per_frame_work": {"node_visits": per_frame[0], "leaf_visits": per_frame[1],
+                                        "tet_tests": per_frame[2], "shadow_node_visits": per_frame[3],
+                                        "shadow_tet_tests": per_frame[5], "shadow_rays": per_frame[6]}},
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(scene.packed(), tuple(scene.info.cam_rapidity))
+        except Exception as exc:  # the baseline is reported, not required for the GPU number
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"failed: {exc}"}
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_engine(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -293,7 +293,7 @@ class Engine:
         return s
 
     def render(self, idx: int, u: GpuUniforms, path: int = SR_PATH_FAST, aux: bool = False, hdr: bool = False,
-               timing: bool = False, cam: CameraF64 | None = None) -> Frame:
+               timing: bool = False, cam: CameraF64 | None = None, count: bool = False) -> Frame:
         n = u.size[0] * u.size[1]
         fr = Frame(rgb=np.zeros(n, np.uint32))
         out = _lib.Outputs()
@@ -306,7 +306,8 @@ class Engine:
         if hdr:
             fr.hdr = np.zeros((n, 4), np.float32)
             out.hdr = fr.hdr.ctypes.data
-        opts = _lib.RenderOpts(path, SR_FLAG_TIMING if timing else 0, C.pointer(cam) if cam is not None else None)
+        flags = (SR_FLAG_TIMING if timing else 0) | (_lib.SR_FLAG_COUNT_WORK if count else 0)
+        opts = _lib.RenderOpts(path, flags, C.pointer(cam) if cam is not None else None)
         t = _lib.Timings()
         _check(self.L.sr_render_ex(self.h, idx, C.byref(u), C.byref(opts), C.byref(out), C.byref(t)), self.h,
                "render")

@@ -330,9 +330,11 @@ sr_status sr_render_ex(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const 
     SceneSlot& s = *ctx->scenes[idx];
     const uint32_t path = opts ? opts->path : SR_PATH_FAST;
     const uint32_t flags = opts ? opts->flags : 0u;
-    const bool dev_out = (flags & SR_FLAG_DEVICE_OUTPUT) != 0;
+    const bool count = (flags & SR_FLAG_COUNT_WORK) != 0;
+    const bool dev_out = (flags & SR_FLAG_DEVICE_OUTPUT) != 0 && !count;
     const bool timing = (flags & SR_FLAG_TIMING) != 0;
     if (path != SR_PATH_PLAIN && path != SR_PATH_FAST) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "unknown path");
+    if (count && (flags & SR_FLAG_DEVICE_OUTPUT)) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "work counting returns host outputs");
     CK(cudaSetDevice(ctx->device), "set device");
     sr_status st = ensure_frame(ctx, u->size[0], u->size[1]);
     if (st != SR_OK) return st;
@@ -358,7 +360,7 @@ sr_status sr_render_ex(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const 
     cudaEvent_t* ev = ctx->ev;
     auto t_host0 = std::chrono::steady_clock::now();
     if (timing) CK(cudaEventRecord(ev[0], sm), "event");
-    CK(cudaMemsetAsync(ctx->counters.p, 0, 16, sm), "counters");
+    CK(cudaMemsetAsync(ctx->counters.p, 0, count ? 64 : 16, sm), "counters");
     const float4* cam_dev = nullptr;
     if (opts && opts->cam64) {
         CK(launch_camera_f64(*opts->cam64, s.anchor, *u, ctx->cam.as<float4>(), sm), "camera kernel");
@@ -370,7 +372,8 @@ sr_status sr_render_ex(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const 
         CK(launch_render_plain(sd, *u, cam_dev, f, ctx->bb, sm), "plain render");
         if (timing) { CK(cudaEventRecord(ev[2], sm), "event"); CK(cudaEventRecord(ev[3], sm), "event"); }
     } else {
-        CK(fast_render(ctx->fast, s.fast, s.tuning, sd, *u, cam_dev, f, ctx->bb, sm, timing ? ev + 2 : nullptr), "fast render");
+        CK(fast_render(ctx->fast, s.fast, s.tuning, sd, *u, cam_dev, f, ctx->bb, sm, timing ? ev + 2 : nullptr, count),
+           "fast render");
     }
     if (timing) CK(cudaEventRecord(ev[4], sm), "event");
     CK(launch_bloom(f, fr.pyr, ctx->tables.as<uint32_t>(), sm), "bloom");
@@ -384,8 +387,8 @@ sr_status sr_render_ex(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const 
         if (out->lambda) CK(cudaMemcpyAsync(out->lambda, f.lambda, npx * 4, cudaMemcpyDeviceToHost, sm), "readback");
         if (out->tau) CK(cudaMemcpyAsync(out->tau, f.tau, npx * 4, cudaMemcpyDeviceToHost, sm), "readback");
     }
-    uint32_t counters[4] = {0, 0, 0, 0};
-    CK(cudaMemcpyAsync(counters, ctx->counters.p, 16, cudaMemcpyDeviceToHost, sm), "counters");
+    uint32_t counters[16] = {0};
+    CK(cudaMemcpyAsync(counters, ctx->counters.p, 64, cudaMemcpyDeviceToHost, sm), "counters");
     CK(cudaStreamSynchronize(sm), "render sync");
     auto t_host2 = std::chrono::steady_clock::now();
     if (timings) {
@@ -393,6 +396,16 @@ sr_status sr_render_ex(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const 
         timings->submit_ms = std::chrono::duration<float, std::milli>(t_host1 - t_host0).count();
         timings->wait_ms = std::chrono::duration<float, std::milli>(t_host2 - t_host1).count();
         timings->shadow_rays = counters[0];
+        if (count && path == SR_PATH_FAST) {
+            uint64_t w[6];
+            std::memcpy(w, counters + 4, sizeof(w));
+            timings->nodes_visited = w[0];
+            timings->leaves_visited = w[1];
+            timings->tets_tested = w[2];
+            timings->shadow_nodes_visited = w[3];
+            timings->shadow_leaves_visited = w[4];
+            timings->shadow_tets_tested = w[5];
+        }
         if (timing) {
             cudaEventElapsedTime(&timings->kernel_ms, ev[0], ev[5]);
             cudaEventElapsedTime(&timings->camera_ms, ev[0], ev[1]);

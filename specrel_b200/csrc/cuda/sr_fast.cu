@@ -136,9 +136,15 @@ __device__ __forceinline__ void load_wide(const uint4* w, uint32_t i, float4* lm
     *rmax = make_float4(__uint_as_float(d.x), __uint_as_float(d.y), __uint_as_float(d.z), __uint_as_float(d.w));
 }
 
+// Traversal work of one thread (the SR_FLAG_COUNT_WORK variant only).
+struct Work {
+    uint32_t nodes, leaves, tets;
+};
+
 // Closest hit over the wide layout; returns the leaf slot or -1.
+template <bool COUNT>
 __device__ __noinline__ int trace_fast(const WideScene& s, float4 o, float4 d, float t_min, float t_max, GeomHit* best,
-                                       uint32_t* err) {
+                                       uint32_t* err, Work* work) {
     float4 inv = v4(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z), safe_inv(d.w));
     int slot = -1;
     uint32_t cur, cur_cnt;
@@ -162,6 +168,7 @@ __device__ __noinline__ int trace_fast(const WideScene& s, float4 o, float4 d, f
         if (++visits > MAX_VISITS_FAST) { atomicOr(err, ERR_TRAVERSAL_LIMIT); break; }
         bool descend = false;
         if (cur_cnt == 0u) {
+            if (COUNT) ++work->nodes;
             float4 lmin, lmax, rmin, rmax;
             uint4 m;
             load_wide(s.wide, cur, &lmin, &lmax, &rmin, &rmax, &m);
@@ -190,6 +197,7 @@ __device__ __noinline__ int trace_fast(const WideScene& s, float4 o, float4 d, f
                 if (tr < t_max) { cur = m.y; cur_cnt = m.w; descend = true; }
             }
         } else {
+            if (COUNT) { ++work->leaves; work->tets += cur_cnt; }
             for (uint32_t k = cur; k < cur + cur_cnt; ++k) {
                 GeomHit gh;
                 if (intersect_geom(s.geoms + 5u * k, o, d, t_min, t_max, &gh)) {
@@ -211,7 +219,9 @@ __device__ __noinline__ int trace_fast(const WideScene& s, float4 o, float4 d, f
 }
 
 // Any hit in (t_min, t_max) over the wide layout (Bvh4D::is_occluded, bvh4d.rs:523-578).
-__device__ __noinline__ bool occluded_fast(const WideScene& s, float4 o, float4 d, float t_min, float t_max, uint32_t* err) {
+template <bool COUNT>
+__device__ __noinline__ bool occluded_fast(const WideScene& s, float4 o, float4 d, float t_min, float t_max, uint32_t* err,
+                                           Work* work) {
     float4 inv = v4(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z), safe_inv(d.w));
     if (slab_enter(s.root_min, s.root_max, o, inv, t_min, t_max) < 0.0f) return false;
     uint32_t cur = s.root_is_leaf ? s.root_first : 0u, cur_cnt = s.root_is_leaf ? s.root_count : 0u;
@@ -223,6 +233,7 @@ __device__ __noinline__ bool occluded_fast(const WideScene& s, float4 o, float4 
         if (++visits > MAX_VISITS_FAST) { atomicOr(err, ERR_TRAVERSAL_LIMIT); return false; }
         bool descend = false;
         if (cur_cnt == 0u) {
+            if (COUNT) ++work->nodes;
             float4 lmin, lmax, rmin, rmax;
             uint4 m;
             load_wide(s.wide, cur, &lmin, &lmax, &rmin, &rmax, &m);
@@ -237,7 +248,9 @@ __device__ __noinline__ bool occluded_fast(const WideScene& s, float4 o, float4 
                 cur = m.y; cur_cnt = m.w; descend = true;
             }
         } else {
+            if (COUNT) ++work->leaves;
             for (uint32_t k = cur; k < cur + cur_cnt; ++k) {
+                if (COUNT) ++work->tets;
                 GeomHit gh;
                 if (intersect_geom(s.geoms + 5u * k, o, d, t_min, t_max, &gh)) return true;
             }
@@ -250,11 +263,22 @@ __device__ __noinline__ bool occluded_fast(const WideScene& s, float4 o, float4 
     }
 }
 
+template <bool COUNT>
 struct FastOccluder {
     const WideScene* s;
     uint32_t* err;
-    __device__ bool operator()(float4 o, float4 d, float t0, float t1) { return occluded_fast(*s, o, d, t0, t1, err); }
+    Work* work;
+    __device__ bool operator()(float4 o, float4 d, float t0, float t1) {
+        return occluded_fast<COUNT>(*s, o, d, t0, t1, err, work);
+    }
 };
+
+// Adds a warp's work to the 64-bit counters (counting variant only).
+__device__ __forceinline__ void add_work(unsigned long long* c, const Work& w) {
+    atomicAdd(c + 0, (unsigned long long)w.nodes);
+    atomicAdd(c + 1, (unsigned long long)w.leaves);
+    atomicAdd(c + 2, (unsigned long long)w.tets);
+}
 
 struct TraceArgs {
     WideScene ws;
@@ -263,12 +287,15 @@ struct TraceArgs {
     uint32_t* slot;
     uint32_t* counter;
     uint32_t* err;
+    unsigned long long* work;  // 6 counters (primary nodes, leaves, tets; shadow nodes, leaves, tets)
 };
 
 // Persistent primary-ray kernel: each warp takes a tile_w x tile_h tile of pixels at a time.
+template <bool COUNT>
 __global__ void __launch_bounds__(512) k_trace_fast(TraceArgs a, SrGpuUniforms U, const float4* cam_dev) {
     const uint32_t lane = threadIdx.x & 31u;
     const Cam cam = load_cam(U, cam_dev);
+    Work work{0, 0, 0};
     for (;;) {
         uint32_t t = 0;
         if (lane == 0) t = atomicAdd(a.counter, 1u);
@@ -281,15 +308,18 @@ __global__ void __launch_bounds__(512) k_trace_fast(TraceArgs a, SrGpuUniforms U
         float sx, sy;
         camera_ray(U, cam, px, py, &o, &d, &sx, &sy);
         GeomHit gh;
-        int slot = trace_fast(a.ws, o, d, 1e-3f, 180.0f, &gh, a.err);
+        int slot = trace_fast<COUNT>(a.ws, o, d, 1e-3f, 180.0f, &gh, a.err, &work);
         size_t idx = (size_t)py * a.width + px;
         a.hit[idx] = make_float4(gh.lambda, gh.u, gh.v, gh.w);
         a.slot[idx] = slot < 0 ? 0xFFFFFFFFu : (uint32_t)slot;
     }
+    if (COUNT) add_work(a.work, work);
 }
 
+template <bool COUNT>
 __global__ void __launch_bounds__(256) k_shade_fast(SceneDev s, WideScene ws, SrGpuUniforms U, const float4* cam_dev,
-                                                     FrameDev f, const float4* hits, const uint32_t* slots, BBConst bb) {
+                                                     FrameDev f, const float4* hits, const uint32_t* slots, BBConst bb,
+                                                     unsigned long long* work_out) {
     uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t py = blockIdx.y * blockDim.y + threadIdx.y;
     if (px >= U.size[0] || py >= U.size[1]) return;
@@ -308,9 +338,11 @@ __global__ void __launch_bounds__(256) k_shade_fast(SceneDev s, WideScene ws, Sr
         float4 hr = hits[idx];
         GeomHit gh{hr.x, hr.y, hr.z, hr.w};
         interpolate(s.attrs + 12u * slot, o, d, gh, &h);
-        FastOccluder occ{&ws, f.counters + 1};
+        Work work{0, 0, 0};
+        FastOccluder<COUNT> occ{&ws, f.counters + 1, &work};
         color = shade_hit(s, U, cam, d, h, occ, &shadow_rays);
         if (U.num_haze > 0u) color = apply_haze(color, h.event, U);
+        if (COUNT && work.nodes) add_work(work_out + 3, work);
     } else {
         color = shade_sky(d);
     }
@@ -324,7 +356,8 @@ __global__ void __launch_bounds__(256) k_shade_fast(SceneDev s, WideScene ws, Sr
 }
 
 cudaError_t fast_render(FastCtx& c, const FastScene& s, const SrTuning& t, const SceneDev& sd, const SrGpuUniforms& u,
-                        const float4* cam_dev, const FrameDev& f, const BBConst& bb, cudaStream_t st, cudaEvent_t* ev) {
+                        const float4* cam_dev, const FrameDev& f, const BBConst& bb, cudaStream_t st, cudaEvent_t* ev,
+                        bool count_work) {
     if (s.depth > FAST_MAX_DEPTH) {
         // The reference's 64-entry stack may overflow and drop children on such trees; the plain
         // path reproduces that exactly.
@@ -358,14 +391,19 @@ cudaError_t fast_render(FastCtx& c, const FastScene& s, const SrTuning& t, const
     a.slot = c.slots.as<uint32_t>();
     a.counter = f.counters + 2;
     a.err = f.counters + 1;
+    a.work = reinterpret_cast<unsigned long long*>(f.counters + 4);
     uint32_t blocks = (uint32_t)c.num_sms * t.blocks_per_sm;
     uint32_t max_blocks = (a.n_tiles * 32 + t.block_threads - 1) / t.block_threads;
     if (blocks > max_blocks) blocks = max_blocks;
-    k_trace_fast<<<blocks, t.block_threads, 0, st>>>(a, u, cam_dev);
+    if (count_work) k_trace_fast<true><<<blocks, t.block_threads, 0, st>>>(a, u, cam_dev);
+    else k_trace_fast<false><<<blocks, t.block_threads, 0, st>>>(a, u, cam_dev);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[0], st);
     dim3 b(16, 16), g((u.size[0] + 15) / 16, (u.size[1] + 15) / 16);
-    k_shade_fast<<<g, b, 0, st>>>(sd, ws, u, cam_dev, f, c.hits.as<float4>(), c.slots.as<uint32_t>(), bb);
+    if (count_work)
+        k_shade_fast<true><<<g, b, 0, st>>>(sd, ws, u, cam_dev, f, c.hits.as<float4>(), c.slots.as<uint32_t>(), bb, a.work);
+    else
+        k_shade_fast<false><<<g, b, 0, st>>>(sd, ws, u, cam_dev, f, c.hits.as<float4>(), c.slots.as<uint32_t>(), bb, a.work);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[1], st);
     return cudaSuccess;

@@ -56,6 +56,7 @@ bool fast_tuning_valid(const FastCtx& c, const SrTuning& t);
 // Renders the HDR image (and side outputs) of one frame; `ev` (optional) receives events after the
 // trace and shade phases (ev[0], ev[1]).
 cudaError_t fast_render(FastCtx& c, const FastScene& s, const SrTuning& t, const SceneDev& sd, const SrGpuUniforms& u,
-                        const float4* cam_dev, const FrameDev& f, const BBConst& bb, cudaStream_t st, cudaEvent_t* ev);
+                        const float4* cam_dev, const FrameDev& f, const BBConst& bb, cudaStream_t st, cudaEvent_t* ev,
+                        bool count_work = false);
 
 }  // namespace srk
