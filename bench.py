@@ -300,23 +300,20 @@ def run_engine(args, rank, world, local):
         wall_e2e = (time.perf_counter() - t_e2e) / args.steps * 1e3
         e2e_ms = max_over_ranks(max(e0.elapsed_time(e1) / args.steps, wall_e2e))
 
-        # The dominant kernel (primary traversal), timed with events on the launching stream
-        # inside the library, and the traversal work of the same frames (counting variant).
+        # The dominant kernel (k_trace_batch: primary rays and the main light's shadow rays of all
+        # B observers in one launch), timed with CUDA events the library records on the launching
+        # stream around each phase of the same batch, then the traversal work of that batch
+        # (counting variant).
         trace_ms, frame_ms, shade_ms, bloom_ms = [], [], [], []
-        for i in range(B):
-            fr = eng.render(0, us[i], path=sr.SR_PATH_FAST, timing=True, cam=c64[i])
-            t = fr.timings
+        for _ in range(args.steps):
+            t = eng.render_batch(0, us, ptr, B * RAYS_PER_FRAME, cams=c64, device_output=True, phases=True)
             trace_ms.append(t.trace_ms)
             shade_ms.append(t.shade_ms)
             bloom_ms.append(t.bloom_ms)
             frame_ms.append(t.kernel_ms)
-        work = []
-        for i in range(B):
-            fr = eng.render(0, us[i], path=sr.SR_PATH_FAST, cam=c64[i], count=True)
-            t = fr.timings
-            work.append((t.nodes_visited, t.leaves_visited, t.tets_tested, t.shadow_nodes_visited,
-                         t.shadow_leaves_visited, t.shadow_tets_tested, t.shadow_rays))
-        work = np.array(work, dtype=np.float64)
+        t = eng.render_batch(0, us, ptr, B * RAYS_PER_FRAME, cams=c64, device_output=True, count=True)
+        work = np.array([t.nodes_visited, t.leaves_visited, t.tets_tested, t.shadow_nodes_visited,
+                         t.shadow_leaves_visited, t.shadow_tets_tested, t.shadow_rays], dtype=np.float64)
         tuning = eng.tuning(0)
 
     if dist is not None:
@@ -330,11 +327,11 @@ def run_engine(args, rank, world, local):
     value = total_rays / (ms_max / 1e3) / 1e6
     plain_value = total_rays / (plain_ms / 1e3) / 1e6
     e2e_value = total_rays / (e2e_ms / 1e3) / 1e6
-    # Algorithmic bytes of one launch of the trace kernel in the B200 layout: one 80-byte wide
-    # node per internal visit, one 80-byte hot record per tetrahedron test, the 20-byte hit record
-    # written per ray, per frame (the node visits are the reference traversal's own: same order).
-    per_frame = work.mean(axis=0)
-    trace_bytes = 80.0 * per_frame[0] + 80.0 * per_frame[2] + 20.0 * RAYS_PER_FRAME
+    # Algorithmic bytes of one launch of the trace kernel (B frames) in the B200 layout: one 72-byte
+    # wide node (two child boxes + references) per internal visit, one 80-byte hot record per
+    # tetrahedron test, for primary and shadow rays (the visits are the reference traversal's own),
+    # plus the 21 bytes of hit record, slot and shadow state written per ray.
+    trace_bytes = 72.0 * (work[0] + work[3]) + 80.0 * (work[2] + work[5]) + 21.0 * RAYS_PER_FRAME * B
     trace_s = float(np.median(trace_ms)) / 1e3
     achieved = trace_bytes / trace_s / 1e9
     peak, peak_kind = load_peaks()
@@ -355,16 +352,18 @@ def run_engine(args, rank, world, local):
                   "speedup_batched_over_plain": value / plain_value},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 768 * B + 80 * B,
                 "d2h_bytes_per_step": 4 * RAYS_PER_FRAME * B},
-        "gpu_launches": int(args.steps * B * 15),
-        "roofline": {"bound": "hbm", "kernel": "k_trace_fast", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        # Kernels per step: camera, trace, shade, 6 bloom down, 5 bloom up, composite.
+        "gpu_launches": int(args.steps * 15),
+        "roofline": {"bound": "hbm", "kernel": "k_trace_batch", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic,
-                     "algorithmic_bytes_per_launch": trace_bytes, "trace_ms": trace_s * 1e3,
-                     "frame_ms": float(np.median(frame_ms)), "shade_ms": float(np.median(shade_ms)),
+                     "algorithmic_bytes_per_launch": trace_bytes, "frames_per_launch": B,
+                     "trace_ms_per_launch": trace_s * 1e3,
+                     "batch_ms": float(np.median(frame_ms)), "shade_ms": float(np.median(shade_ms)),
                      "bloom_ms": float(np.median(bloom_ms)),
-                     "per_frame_work": {"node_visits": per_frame[0], "leaf_visits": per_frame[1],
-                                        "tet_tests": per_frame[2], "shadow_node_visits": per_frame[3],
-                                        "shadow_tet_tests": per_frame[5], "shadow_rays": per_frame[6]}},
+                     "per_frame_work": {"node_visits": work[0] / B, "leaf_visits": work[1] / B,
+                                        "tet_tests": work[2] / B, "shadow_node_visits": work[3] / B,
+                                        "shadow_tet_tests": work[5] / B, "shadow_rays": work[6] / B}},
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
     }
     if world == 1 and not args.no_cpu_baseline:

@@ -140,8 +140,9 @@ typedef struct SrTimings {
     float kernel_ms;    /* whole frame on the device */
     float readback_ms;
     float camera_ms;    /* FP64 camera / rebase kernel */
-    float trace_ms;     /* primary traversal (+ shading for the plain path) */
-    float shade_ms;     /* shading + shadow rays (fast path) */
+    float trace_ms;     /* primary traversal (+ shading for the plain path; + the main
+                           light's shadow rays for the fast path) */
+    float shade_ms;     /* shading, with the flashes' shadow rays (fast path) */
     float stars_ms;     /* star cone events, binning and gather */
     float bloom_ms;     /* bloom pyramid + tone map + pack */
     uint32_t shadow_rays;
@@ -155,7 +156,7 @@ typedef struct SrTimings {
 
 /* Which implementation renders a frame. */
 #define SR_PATH_PLAIN 0   /* one thread per pixel, the reference's BVH2 traversal order */
-#define SR_PATH_FAST 1    /* persistent, warp-cooperative traversal over the B200 node layout */
+#define SR_PATH_FAST 1    /* persistent traversal over the B200 node layout, per-lane ray fetch */
 
 #define SR_FLAG_TIMING 1u          /* record per-phase CUDA events into SrTimings */
 #define SR_FLAG_DEVICE_OUTPUT 2u   /* output pointers are device pointers; return without syncing */
@@ -237,18 +238,23 @@ sr_status sr_render_ex(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, 
 
 /* Many observers of one scene in one persistent launch (recorded once into a CUDA graph and
  * replayed). Observer i renders with uniforms `u[i]` (and `cam64[i]` when cam64 is not NULL)
- * into `rgb_out + offset_i`, offset_i = sum of width*height of observers before it. */
+ * into `rgb_out + offset_i`, offset_i = sum of width*height of observers before it.
+ * With `timings`, the batch's device time is returned (kernel_ms); SR_FLAG_TIMING adds the
+ * per-phase times and SR_FLAG_COUNT_WORK the traversal work; both run the launch sequence
+ * outside its graph. */
 sr_status sr_render_batch(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, const SrCameraF64* cam64,
                           uint32_t n_observers, uint32_t* rgb_out, uint64_t rgb_len, uint32_t flags,
                           SrTimings* timings);
 
 /* Launch parameters of the fast path; the autotuner (sr_autotune) picks them per scene. */
 typedef struct SrTuning {
-    uint32_t block_threads;   /* threads per block of the persistent traversal kernel */
-    uint32_t blocks_per_sm;   /* resident blocks per SM */
-    uint32_t stack_depth;     /* traversal stack entries in shared memory before spilling */
-    uint32_t smem_levels;     /* top BVH levels staged in shared memory */
-    uint32_t tile_w, tile_h;  /* pixel tile a warp takes at a time */
+    uint32_t block_threads;   /* threads per block of the persistent traversal kernel: 64..512 */
+    uint32_t blocks_per_sm;   /* resident blocks per SM: 1..16 */
+    uint32_t tile_w, tile_h;  /* pixel tile of 32 consecutive rays (tile_w * tile_h == 32) */
+    uint32_t chunk_tiles;     /* tiles a warp takes from the frame at a time: 1..64 */
+    uint32_t refill_lanes;    /* idle lanes that make a warp load new rays: 1..32 (32: all idle) */
+    uint32_t leaf_coop;       /* 1: a warp tests the leaves of all its lanes together */
+    uint32_t leaf_batch;      /* lanes on a leaf before the warp tests leaves: 1..32 */
 } SrTuning;
 sr_status sr_get_tuning(const sr_ctx* ctx, uint32_t scene_idx, SrTuning* out);
 sr_status sr_set_tuning(sr_ctx* ctx, uint32_t scene_idx, const SrTuning* t);
@@ -266,6 +272,7 @@ static_assert(sizeof(SrGpuGeom) == 80, "GpuGeom is 80 bytes (gpu.rs:68-74)");
 static_assert(sizeof(SrGpuAttr) == 192, "GpuAttr is 192 bytes (gpu.rs:79-92)");
 static_assert(sizeof(SrGpuMaterial) == 48, "GpuMaterial is 48 bytes (gpu.rs:96-100)");
 static_assert(sizeof(SrGpuUniforms) == 768, "GpuUniforms is 768 bytes (gpu.rs:122-144)");
+static_assert(sizeof(SrTuning) == 32, "SrTuning is 8 words");
 static_assert(offsetof(SrGpuUniforms, light_pos) == 80, "Uniforms.light_pos");
 static_assert(offsetof(SrGpuUniforms, num_nodes) == 124, "Uniforms.num_nodes");
 static_assert(offsetof(SrGpuUniforms, frontier_origin) == 128, "Uniforms.frontier_origin");

@@ -331,12 +331,18 @@ class Engine:
         return t
 
     def render_batch(self, idx: int, us: list, rgb_ptr: int, rgb_len: int, cams: list | None = None,
-                     device_output: bool = True, timing: bool = False) -> _lib.Timings:
+                     device_output: bool = True, timing: bool = False, phases: bool = False,
+                     count: bool = False) -> _lib.Timings:
+        """Renders observers `us` into `rgb_ptr` (concatenated frames). `timing` returns the batch's
+        device time; `phases` adds per-phase times, `count` the traversal work (both run the launch
+        sequence outside its CUDA graph)."""
         n = len(us)
         ua = (GpuUniforms * n)(*us)
         ca = (CameraF64 * n)(*cams) if cams else None
         t = _lib.Timings()
         flags = SR_FLAG_DEVICE_OUTPUT if device_output else 0
+        flags |= (_lib.SR_FLAG_TIMING if phases else 0) | (_lib.SR_FLAG_COUNT_WORK if count else 0)
+        timing = timing or phases or count
         _check(self.L.sr_render_batch(self.h, idx, ua, ca, n, rgb_ptr, rgb_len, flags,
                                       C.byref(t) if timing else None), self.h, "render_batch")
         return t

@@ -441,6 +441,7 @@ sr_status sr_render_ex(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const 
         }
     }
     if (counters[1] & ERR_TRAVERSAL_LIMIT) return fail(ctx, SR_ERR_TRAVERSAL_LIMIT, "a ray exceeded the traversal visit limit");
+    if (counters[1] & ERR_SHADOW_MISMATCH) return fail(ctx, SR_ERR_CUDA, "internal error: shadow state mismatch");
     if (counters[1]) return fail(ctx, SR_ERR_BAD_SCENE, "device reported a bad index (flags " + std::to_string(counters[1]) + ")");
     return SR_OK;
 }
@@ -499,6 +500,9 @@ sr_status sr_render_batch(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, con
         br.cam64 = cam64;
         br.rgb = dev_out ? rgb_out : nullptr;
         br.use_graph = true;
+        // Per-phase events and work counting run the sequence outside its graph.
+        br.ev = (timings && (flags & SR_FLAG_TIMING)) ? ev + 1 : nullptr;
+        br.count_work = timings && (flags & SR_FLAG_COUNT_WORK);
         SceneDev sd = scene_dev(ctx, s);
         if (timings) CK(cudaEventRecord(ev[6], sm), "event");
         CK(fast_render_batch(ctx->fast, s.fast, s.tuning, sd, s.anchor, ctx->bb, ctx->counters.as<uint32_t>(), br, sm),
@@ -507,15 +511,33 @@ sr_status sr_render_batch(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, con
         if (!dev_out) CK(cudaMemcpyAsync(rgb_out, ctx->fast.rgb.p, total * 4, cudaMemcpyDeviceToHost, sm), "batch readback");
     }
     if (!dev_out || timings) {
-        uint32_t counters[4] = {0, 0, 0, 0};
-        CK(cudaMemcpyAsync(counters, ctx->counters.p, 16, cudaMemcpyDeviceToHost, sm), "counters");
+        uint32_t counters[16] = {0};
+        CK(cudaMemcpyAsync(counters, ctx->counters.p, 64, cudaMemcpyDeviceToHost, sm), "counters");
         CK(cudaStreamSynchronize(sm), "batch sync");
         if (timings) {
             std::memset(timings, 0, sizeof(*timings));
             cudaEventElapsedTime(&timings->kernel_ms, ev[6], ev[7]);
             timings->shadow_rays = counters[0];
+            if (s.fast.usable && (flags & SR_FLAG_TIMING)) {
+                cudaEventElapsedTime(&timings->camera_ms, ev[6], ev[1]);
+                cudaEventElapsedTime(&timings->trace_ms, ev[1], ev[2]);
+                cudaEventElapsedTime(&timings->shade_ms, ev[2], ev[3]);
+                cudaEventElapsedTime(&timings->stars_ms, ev[3], ev[4]);
+                cudaEventElapsedTime(&timings->bloom_ms, ev[4], ev[5]);
+            }
+            if (s.fast.usable && (flags & SR_FLAG_COUNT_WORK)) {
+                uint64_t w[6];
+                std::memcpy(w, counters + 4, sizeof(w));
+                timings->nodes_visited = w[0];
+                timings->leaves_visited = w[1];
+                timings->tets_tested = w[2];
+                timings->shadow_nodes_visited = w[3];
+                timings->shadow_leaves_visited = w[4];
+                timings->shadow_tets_tested = w[5];
+            }
         }
         if (counters[1] & ERR_TRAVERSAL_LIMIT) return fail(ctx, SR_ERR_TRAVERSAL_LIMIT, "a ray exceeded the traversal visit limit");
+        if (counters[1] & ERR_SHADOW_MISMATCH) return fail(ctx, SR_ERR_CUDA, "internal error: shadow state mismatch");
         if (counters[1]) return fail(ctx, SR_ERR_BAD_SCENE, "device reported a bad index");
     }
     return SR_OK;
@@ -532,33 +554,45 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
     SrRenderOpts opts{SR_PATH_FAST, SR_FLAG_DEVICE_OUTPUT, nullptr};
     SrTuning keep = s.tuning, win = s.tuning;
     float win_ms = INFINITY;
-    const uint32_t threads[] = {64, 128, 256};
-    const uint32_t per_sm[] = {4, 8, 16};
-    const uint32_t tiles[][2] = {{8, 4}, {4, 8}, {16, 2}};
+    // The schedules worth timing: whole-warp refills of single tiles were fastest on every scene
+    // measured (wider chunks or partial refills spread the rays in flight over more of the tree).
+    const uint32_t threads[] = {128, 256};
+    const uint32_t per_sm[] = {4, 8};
+    const uint32_t tiles[][2] = {{8, 4}, {4, 8}};
+    const uint32_t leaf_batches[] = {1, 8};
+    std::vector<SrTuning> cand;
     for (uint32_t bt : threads)
         for (uint32_t bs : per_sm)
-            for (auto& tl : tiles) {
-                SrTuning t = keep;
-                t.block_threads = bt;
-                t.blocks_per_sm = bs;
-                t.tile_w = tl[0];
-                t.tile_h = tl[1];
-                if (!fast_tuning_valid(ctx->fast, t)) continue;
-                s.tuning = t;
-                sr_status st = sr_render_ex(ctx, idx, u, &opts, &o, nullptr);  // warm-up
-                if (st != SR_OK) { s.tuning = keep; return st; }
-                CK(cudaEventRecord(ctx->ev[6], ctx->stream), "event");
-                for (uint32_t i = 0; i < std::max(1u, n); ++i) {
-                    st = sr_render_ex(ctx, idx, u, &opts, &o, nullptr);
-                    if (st != SR_OK) { s.tuning = keep; return st; }
-                }
-                CK(cudaEventRecord(ctx->ev[7], ctx->stream), "event");
-                CK(cudaEventSynchronize(ctx->ev[7]), "event sync");
-                float ms = 0;
-                cudaEventElapsedTime(&ms, ctx->ev[6], ctx->ev[7]);
-                ms /= (float)std::max(1u, n);
-                if (ms < win_ms) { win_ms = ms; win = t; }
-            }
+            for (auto& tl : tiles)
+                for (uint32_t lb : leaf_batches)
+                    for (uint32_t coop = 0; coop <= 1; ++coop) {
+                        SrTuning t = keep;
+                        t.block_threads = bt;
+                        t.blocks_per_sm = bs;
+                        t.tile_w = tl[0];
+                        t.tile_h = tl[1];
+                        t.chunk_tiles = 1;
+                        t.refill_lanes = 32;
+                        t.leaf_coop = coop;
+                        t.leaf_batch = lb;
+                        if (fast_tuning_valid(ctx->fast, t)) cand.push_back(t);
+                    }
+    for (const SrTuning& t : cand) {
+        s.tuning = t;
+        sr_status st = sr_render_ex(ctx, idx, u, &opts, &o, nullptr);  // warm-up
+        if (st != SR_OK) { s.tuning = keep; return st; }
+        CK(cudaEventRecord(ctx->ev[6], ctx->stream), "event");
+        for (uint32_t i = 0; i < std::max(1u, n); ++i) {
+            st = sr_render_ex(ctx, idx, u, &opts, &o, nullptr);
+            if (st != SR_OK) { s.tuning = keep; return st; }
+        }
+        CK(cudaEventRecord(ctx->ev[7], ctx->stream), "event");
+        CK(cudaEventSynchronize(ctx->ev[7]), "event sync");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[6], ctx->ev[7]);
+        ms /= (float)std::max(1u, n);
+        if (ms < win_ms) { win_ms = ms; win = t; }
+    }
     s.tuning = win;
     if (best) *best = win;
     if (best_ms) *best_ms = win_ms;

@@ -2,17 +2,17 @@
 // launches (captured once into a CUDA graph and replayed):
 //
 //   k_camera_batch   FP64 observers (tetrad from rapidity in double, event rebased to the anchor)
-//   k_trace_batch    persistent: each warp takes a 32-pixel tile of any observer from one global
-//                    counter and writes the primary hit records
-//   k_shade_batch    one thread per pixel: interpolation and shading; a pixel whose main-light
-//                    shadow ray is due goes to a compacted queue instead (warp-aggregated append)
-//   k_shadow_batch   persistent any-hit traversal of the queue, so the few long shadow rays spread
-//                    over every SM instead of stretching the blocks that happen to hold them
-//   k_finish_batch   the queued pixels, shaded with their shadow result
+//   k_trace_batch    persistent traversal, one ray per lane, refilled from a per-warp chunk of
+//                    neighbouring tiles. A pixel's work is its primary ray (closest hit), then, when
+//                    the main light needs it, the shadow ray (any hit) as a second phase of the same
+//                    loop, so shadow rays spread over all lanes instead of forming a separate tail.
+//   k_shade_batch    one thread per pixel: interpolation and shading, with the main light's
+//                    shadow result from the trace kernel (renderer.rs:414-489, 609-653)
 //   bloom            the pyramid of every observer, one launch per level
 //
-// Shading is one device function used by k_shade_batch and k_finish_batch, so a queued pixel's
-// colour is computed by the same operations as any other (renderer.rs:414-489, 609-653).
+// The trace kernel decides "shadow ray needed" with the same code the shading evaluates
+// (checkerboard material, light in front in the surface's rest frame), and the shading checks the
+// two agree.
 #include <cub/cub.cuh>
 
 #include <cstring>
@@ -109,10 +109,12 @@ SrTuning fast_default_tuning(const FastCtx& c) {
     SrTuning t{};
     t.block_threads = 128;
     t.blocks_per_sm = 8;
-    t.stack_depth = FAST_STACK;
-    t.smem_levels = 0;
     t.tile_w = 8;
     t.tile_h = 4;
+    t.chunk_tiles = 1;
+    t.refill_lanes = 32;
+    t.leaf_coop = 0;
+    t.leaf_batch = 1;
     return t;
 }
 
@@ -120,7 +122,8 @@ bool fast_tuning_valid(const FastCtx& c, const SrTuning& t) {
     (void)c;
     bool bt = t.block_threads == 64 || t.block_threads == 128 || t.block_threads == 256 || t.block_threads == 512;
     return bt && t.blocks_per_sm >= 1 && t.blocks_per_sm <= 16 && t.tile_w >= 1 && t.tile_w * t.tile_h == 32 &&
-           t.stack_depth == (uint32_t)FAST_STACK && t.smem_levels == 0;
+           t.chunk_tiles >= 1 && t.chunk_tiles <= 64 && t.refill_lanes >= 1 && t.refill_lanes <= 32 &&
+           t.leaf_coop <= 1 && t.leaf_batch >= 1 && t.leaf_batch <= 32;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -166,54 +169,354 @@ __global__ void k_camera_batch(uint32_t n, const SrGpuUniforms* U, const SrCamer
     }
 }
 
-struct TraceBatchArgs {
-    WideScene ws;
-    const SrGpuUniforms* U;
-    const float4* cam;
-    const ObsDev* obs;
-    const uint32_t* tile_pre;
-    uint32_t n, total_tiles, tile_w, tile_h;
-    float4* hits;
-    uint32_t* slots;
-    uint32_t* counter;
-    uint32_t* err;
-    unsigned long long* work;
-};
-
 __device__ __forceinline__ void add_work(unsigned long long* c, const Work& w) {
     atomicAdd(c + 0, (unsigned long long)w.nodes);
     atomicAdd(c + 1, (unsigned long long)w.leaves);
     atomicAdd(c + 2, (unsigned long long)w.tets);
 }
 
-template <bool COUNT>
+struct TraceBatchArgs {
+    WideScene ws;
+    const float4* attrs;
+    const float4* mats;
+    const SrGpuUniforms* U;
+    const float4* cam;
+    const ObsDev* obs;
+    const uint32_t* tile_pre;
+    uint32_t n, total_rays, tile_w, tile_h;
+    uint32_t chunk_rays;    // rays a warp takes from the global counter at a time (a multiple of 32)
+    uint32_t refill_lanes;  // idle lanes that make the warp fetch new rays
+    uint32_t leaf_batch;    // lanes on a leaf before the warp tests leaves
+    float4* hits;
+    uint32_t* slots;
+    uint8_t* shadow;  // 0: no main-light shadow ray, 1: cast and clear, 2: cast and occluded
+    uint32_t* counter;
+    uint32_t* err;
+    unsigned long long* work;
+};
+
+// Ray index r -> pixel: rays run tile by tile (32 consecutive rays = one tile_w x tile_h tile).
+__device__ __forceinline__ bool ray_pixel(const TraceBatchArgs& a, uint32_t r, uint32_t* obs, uint32_t* px, uint32_t* py,
+                                          uint32_t* p) {
+    uint32_t t = r >> 5, l = r & 31u;
+    uint32_t o = find_obs(a.tile_pre, a.n, t);
+    const ObsDev& od = a.obs[o];
+    uint32_t lt = t - __ldg(a.tile_pre + o);
+    uint32_t x = (lt % od.tiles_x) * a.tile_w + l % a.tile_w;
+    uint32_t y = (lt / od.tiles_x) * a.tile_h + l / a.tile_w;
+    if (x >= od.width || y >= od.height) return false;
+    *obs = o;
+    *px = x;
+    *py = y;
+    *p = od.pix_base + y * od.width + x;
+    return true;
+}
+
+// Shared memory of one warp for the cooperative leaf tests: the rays of the lanes at a leaf, and
+// per lane the best (lambda bits << 32 | tetrahedron index in the leaf) key with its barycentrics.
+constexpr uint32_t COOP_SMEM_PER_WARP = 32u * 4u * sizeof(float4) + 32u * sizeof(unsigned long long);
+
+// Persistent traversal (see the top of the file). Each pass of the loop, with the warp converged:
+//   refill     when at least `refill_lanes` lanes are idle, they take the next rays of the warp's
+//              chunk (chunk_rays consecutive rays, a block of neighbouring tiles);
+//   internal   every lane standing on an internal node takes one step (descend, push, or pop);
+//   leaves     lanes standing on a leaf wait until `leaf_batch` lanes do (or no lane is on an
+//              internal node); then the leaves are tested. With COOP the warp tests all its lanes'
+//              tetrahedra together, 32 at a time, and each lane keeps the smallest lambda, ties going
+//              to the first tetrahedron of the leaf, as in the sequential loop (whose test
+//              `lambda >= t_max` rejects an equal lambda).
+// Each ray visits exactly the nodes of the reference's traversal, in its order.
+template <bool COUNT, bool COOP>
 __global__ void __launch_bounds__(512) k_trace_batch(TraceBatchArgs a) {
-    const uint32_t lane = threadIdx.x & 31u;
-    Work work{0, 0, 0};
+    extern __shared__ float4 coop_smem[];
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t lanes_below = (1u << lane) - 1u;
+    float4* s_o = coop_smem + warp * 128u;
+    float4* s_d = s_o + 32;
+    float4* s_t = s_d + 32;
+    float4* s_h = s_t + 32;
+    unsigned long long* s_key = reinterpret_cast<unsigned long long*>(coop_smem + (blockDim.x >> 5) * 128u) + warp * 32u;
+
+    Work wp{0, 0, 0}, wsh{0, 0, 0};
+    bool has = false, occluded = false;
+    uint32_t obs = 0, pix = 0, phase = 0, cur = 0, visits = 0;
+    int sp = 0, slot = -1;
+    float4 o = v4(0, 0, 0, 0), d = o, inv = o;
+    float t_min = 0.0f, t_max = 0.0f;
+    GeomHit best{0.0f, 0.0f, 0.0f, 0.0f};
+    uint32_t st_ref[FAST_STACK];
+    float st_t[FAST_STACK];
+    uint32_t c_next = 0, c_end = 0;  // the warp's chunk (uniform across the warp)
+    bool exhausted = false;          // uniform
+
+    // Next node from the stack; primary rays skip entries entered at or beyond the closest hit.
+    auto pop = [&]() -> bool {
+        while (sp > 0) {
+            --sp;
+            if (phase != 0 || st_t[sp] < t_max) {
+                cur = st_ref[sp];
+                return true;
+            }
+        }
+        return false;
+    };
+    // The current query is over: store its result, and start the shadow query when the main light
+    // needs one.
+    auto end_phase = [&]() {
+        if (phase != 0) {
+            a.shadow[pix] = occluded ? 2 : 1;
+            has = false;
+            return;
+        }
+        a.hits[pix] = make_float4(best.lambda, best.u, best.v, best.w);
+        a.slots[pix] = slot < 0 ? 0xFFFFFFFFu : (uint32_t)slot;
+        uint8_t sh_state = 0;
+        has = false;
+        const SrGpuUniforms& U = a.U[obs];
+        if (slot >= 0 && U.mode == 0u && U.shadow_mode != 0u && U.num_flashes == 0u) {
+            // compute_illumination's shadow-ray condition (renderer.rs:617-633).
+            const float4* at = a.attrs + 12u * (uint32_t)slot;
+            uint32_t mat = __float_as_uint(__ldg(at + 10).z);
+            if (__float_as_uint(__ldg(a.mats + 3u * mat + 2u).y) == 0u) {
+                float4 ev = add4(o, mul4(d, best.lambda));
+                const Cam cam = cam_of(a.cam, obs);
+                float4 tl;
+                float dist;
+                light_ray(U, cam, ev, &tl, &dist);
+                if (fmaxf(rest_frame_cos(tl, __ldg(at + 8), __ldg(at + 9)), 0.0f) > 0.0f) {
+                    // Bvh4D::is_occluded(hit.event, to_light, 2e-3, dist - 2e-3) (renderer.rs:636-641).
+                    sh_state = 1;
+                    o = ev;
+                    d = tl;
+                    inv = v4(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z), safe_inv(d.w));
+                    t_min = 2e-3f;
+                    t_max = dist - 2e-3f;
+                    phase = 1;
+                    occluded = false;
+                    visits = 0;
+                    sp = 0;
+                    if (slab_enter(a.ws.root_min, a.ws.root_max, o, inv, t_min, t_max) >= 0.0f) {
+                        cur = a.ws.root_ref;
+                        has = true;
+                    }
+                }
+            }
+        }
+        if (!has) a.shadow[pix] = sh_state;
+    };
+
+    // One internal node of the lane's query: descend into the nearer child box, push the farther,
+    // or pop; ends the query when the stack runs dry.
+    auto node_step = [&]() {
+        if (++visits > MAX_VISITS_FAST) {
+            atomicOr(a.err, ERR_TRAVERSAL_LIMIT);
+            sp = 0;
+            end_phase();
+            return;
+        }
+        if (COUNT) ++(phase ? wsh : wp).nodes;
+        const float4* bx = a.ws.boxes + 4ull * cur;
+        float4 lmin = __ldg(bx), lmax = __ldg(bx + 1), rmin = __ldg(bx + 2), rmax = __ldg(bx + 3);
+        uint2 rf = __ldg(a.ws.refs + cur);
+        float tl = slab_enter(lmin, lmax, o, inv, t_min, t_max);
+        float tr = slab_enter(rmin, rmax, o, inv, t_min, t_max);
+        bool hl = tl >= 0.0f, hr = tr >= 0.0f;
+        // Primary rays cull boxes entered at or beyond the closest hit (bvh4d.rs:461); the
+        // any-hit query has no such cull (bvh4d.rs:541-575) and visits left before right.
+        const bool any = phase != 0;
+        if (hl && hr) {
+            bool left_near = any || tl <= tr;
+            float tn = left_near ? tl : tr;
+            if (any || tn < t_max) {
+                if (sp < FAST_STACK) {
+                    st_ref[sp] = left_near ? rf.y : rf.x;
+                    st_t[sp] = left_near ? tr : tl;
+                    ++sp;
+                } else {
+                    atomicOr(a.err, ERR_BAD_INDEX);
+                }
+                cur = left_near ? rf.x : rf.y;
+                return;
+            }
+        } else if (hl && (any || tl < t_max)) {
+            cur = rf.x;
+            return;
+        } else if (hr && (any || tr < t_max)) {
+            cur = rf.y;
+            return;
+        }
+        if (!pop()) end_phase();
+    };
+
     for (;;) {
-        uint32_t t = 0;
-        if (lane == 0) t = atomicAdd(a.counter, 1u);
-        t = __shfl_sync(0xFFFFFFFFu, t, 0);
-        if (t >= a.total_tiles) break;
-        uint32_t o = find_obs(a.tile_pre, a.n, t);
-        const ObsDev& od = a.obs[o];
-        uint32_t lt = t - __ldg(a.tile_pre + o);
-        uint32_t tiles_x = od.tiles_x;
-        uint32_t px = (lt % tiles_x) * a.tile_w + lane % a.tile_w;
-        uint32_t py = (lt / tiles_x) * a.tile_h + lane / a.tile_w;
-        uint32_t w = od.width, h = od.height;
-        if (px >= w || py >= h) continue;
-        const Cam cam = cam_of(a.cam, o);
-        float4 ro, rd;
-        float sx, sy;
-        camera_ray(a.U[o], cam, px, py, &ro, &rd, &sx, &sy);
-        GeomHit gh;
-        int slot = trace_wide<COUNT>(a.ws, ro, rd, 1e-3f, 180.0f, &gh, a.err, &work);
-        size_t p = (size_t)od.pix_base + (size_t)py * w + px;
-        a.hits[p] = make_float4(gh.lambda, gh.u, gh.v, gh.w);
-        a.slots[p] = slot < 0 ? 0xFFFFFFFFu : (uint32_t)slot;
+        // Refill.
+        unsigned idle = __ballot_sync(FULL, !has);
+        if (!exhausted && idle != 0u && (idle == FULL || (uint32_t)__popc(idle) >= a.refill_lanes)) {
+            while (idle != 0u) {
+                if (c_next == c_end) {
+                    uint32_t base = 0;
+                    if (lane == 0) base = atomicAdd(a.counter, a.chunk_rays);
+                    base = __shfl_sync(FULL, base, 0);
+                    if (base >= a.total_rays) {
+                        exhausted = true;
+                        break;
+                    }
+                    c_next = base;
+                    c_end = min(base + a.chunk_rays, a.total_rays);
+                }
+                uint32_t take = min(c_end - c_next, (uint32_t)__popc(idle));
+                bool mine = ((idle >> lane) & 1u) && (uint32_t)__popc(idle & lanes_below) < take;
+                if (mine) {
+                    uint32_t r = c_next + (uint32_t)__popc(idle & lanes_below);
+                    uint32_t px, py;
+                    if (ray_pixel(a, r, &obs, &px, &py, &pix)) {
+                        const Cam cam = cam_of(a.cam, obs);
+                        float sx, sy;
+                        camera_ray(a.U[obs], cam, px, py, &o, &d, &sx, &sy);
+                        inv = v4(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z), safe_inv(d.w));
+                        t_min = 1e-3f;
+                        t_max = 180.0f;
+                        slot = -1;
+                        phase = 0;
+                        visits = 0;
+                        sp = 0;
+                        float re = a.ws.empty ? -1.0f : slab_enter(a.ws.root_min, a.ws.root_max, o, inv, t_min, t_max);
+                        if (re >= 0.0f && re < t_max) {
+                            cur = a.ws.root_ref;
+                            has = true;
+                        } else {  // the ray misses the scene's box (bvh4d.rs:451)
+                            a.hits[pix] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                            a.slots[pix] = 0xFFFFFFFFu;
+                            a.shadow[pix] = 0;
+                        }
+                    }
+                }
+                idle &= ~__ballot_sync(FULL, mine);
+                c_next += take;
+            }
+        }
+
+        // One internal node for every lane that stands on one.
+        if (has && !(cur & REF_LEAF)) node_step();
+
+        // Leaves: postponed until `leaf_batch` lanes stand on one, or no lane is on an internal node.
+        const bool at_leaf = has && (cur & REF_LEAF);
+        const unsigned lm = __ballot_sync(FULL, at_leaf);
+        const unsigned nm = __ballot_sync(FULL, has && !(cur & REF_LEAF));
+        if (lm == 0u) {
+            if (nm == 0u && exhausted) break;
+            continue;
+        }
+        if (nm != 0u && (uint32_t)__popc(lm) < a.leaf_batch) continue;
+
+        if (!COOP) {
+            if (at_leaf) {
+                if (++visits > MAX_VISITS_FAST) {
+                    atomicOr(a.err, ERR_TRAVERSAL_LIMIT);
+                    sp = 0;
+                } else {
+                    uint32_t first = cur & REF_FIRST_MASK, cnt = (cur >> REF_COUNT_SHIFT) & 63u;
+                    if (COUNT) ++(phase ? wsh : wp).leaves;
+                    for (uint32_t k = first; k < first + cnt; ++k) {
+                        if (COUNT) ++(phase ? wsh : wp).tets;
+                        GeomHit gh;
+                        if (intersect_geom(a.ws.geoms + 5u * k, o, d, t_min, t_max, &gh)) {
+                            if (phase == 0) {
+                                t_max = gh.lambda;
+                                best = gh;
+                                slot = (int)k;
+                            } else {
+                                occluded = true;
+                                sp = 0;
+                                break;
+                            }
+                        }
+                    }
+                }
+                if (!pop()) end_phase();
+            }
+            continue;
+        }
+        uint32_t first = 0, cnt = 0;
+        if (at_leaf) {
+            if (++visits > MAX_VISITS_FAST) {
+                atomicOr(a.err, ERR_TRAVERSAL_LIMIT);
+                sp = 0;
+            } else {
+                first = cur & REF_FIRST_MASK;
+                cnt = (cur >> REF_COUNT_SHIFT) & 63u;
+                if (COUNT) {
+                    ++(phase ? wsh : wp).leaves;
+                    (phase ? wsh : wp).tets += cnt;
+                }
+            }
+            s_o[lane] = o;
+            s_d[lane] = d;
+            s_t[lane] = make_float4(t_min, t_max, 0.0f, 0.0f);
+            s_key[lane] = ~0ull;
+        }
+        uint32_t incl = cnt;
+#pragma unroll
+        for (uint32_t s = 1; s < 32; s <<= 1) {
+            uint32_t v = __shfl_up_sync(FULL, incl, s);
+            if (lane >= s) incl += v;
+        }
+        const uint32_t total = __shfl_sync(FULL, incl, 31);
+        const uint32_t excl = incl - cnt;
+        __syncwarp();
+        for (uint32_t base = 0; base < total; base += 32) {
+            const uint32_t j = base + lane;
+            // The owner: the first lane whose inclusive count exceeds j.
+            uint32_t L = 0;
+#pragma unroll
+            for (uint32_t s = 16; s >= 1; s >>= 1) {
+                uint32_t v = __shfl_sync(FULL, incl, L + s - 1);
+                if (v <= j) L += s;
+            }
+            L = min(L, 31u);
+            const uint32_t l_excl = __shfl_sync(FULL, excl, L);
+            const uint32_t l_first = __shfl_sync(FULL, first, L);
+            bool hit = false;
+            unsigned long long key = 0;
+            GeomHit gh;
+            if (j < total) {
+                const uint32_t i = j - l_excl;
+                const float4 tt = s_t[L];
+                if (intersect_geom(a.ws.geoms + 5u * (l_first + i), s_o[L], s_d[L], tt.x, tt.y, &gh)) {
+                    key = ((unsigned long long)__float_as_uint(gh.lambda) << 32) | i;
+                    atomicMin(s_key + L, key);
+                    hit = true;
+                }
+            }
+            __syncwarp();
+            if (hit && s_key[L] == key) s_h[L] = make_float4(gh.u, gh.v, gh.w, 0.0f);
+            __syncwarp();
+        }
+        if (at_leaf) {
+            const unsigned long long k = s_key[lane];
+            if (k != ~0ull) {
+                if (phase == 0) {
+                    const float4 h = s_h[lane];
+                    best.lambda = __uint_as_float((uint32_t)(k >> 32));
+                    best.u = h.x;
+                    best.v = h.y;
+                    best.w = h.z;
+                    t_max = best.lambda;
+                    slot = (int)(first + (uint32_t)(k & 0xFFFFFFFFull));
+                } else {
+                    occluded = true;
+                    sp = 0;
+                }
+            }
+            if (!pop()) end_phase();
+        }
+        __syncwarp();
     }
-    if (COUNT) add_work(a.work, work);
+    if (COUNT) {
+        add_work(a.work, wp);
+        add_work(a.work + 3, wsh);
+    }
 }
 
 struct ShadeBatchArgs {
@@ -226,259 +529,78 @@ struct ShadeBatchArgs {
     uint32_t n, total_px;
     const float4* hits;
     const uint32_t* slots;
+    const uint8_t* shadow;
     float4* hdr;
     uint32_t* hit_id;
     float* lambda;
     float* tau;
-    ShadowRay* queue;
-    uint8_t* qflags;
-    uint32_t* counters;  // [0] shadow rays, [1] errors, [2] tile counter, [3] queue length
+    uint32_t* counters;  // [0] shadow rays, [1] errors
     unsigned long long* work;
     BBConst bb;
 };
 
-// Any-hit queries from inside the shading, traced on the spot (the flash rays of a pixel).
+// The shadow queries of a pixel's shading: the main light's was traced by the trace kernel (its
+// state must say so); with flashes in the frame every query is traced here.
 template <bool COUNT>
-struct InlineOccluder {
+struct FrameOccluder {
     const WideScene* s;
     uint32_t* err;
     Work* work;
-    __device__ bool operator()(float4 o, float4 d, float t0, float t1) { return occluded_wide<COUNT>(*s, o, d, t0, t1, err, work); }
-};
-// The main light's shadow ray of a queued pixel, already traced.
-struct QueuedOccluder {
-    bool result;
-    __device__ bool operator()(float4, float4, float, float) const { return result; }
-};
-
-struct PixelRef {
-    uint32_t o, px, py, l;
-};
-__device__ __forceinline__ PixelRef pixel_of(const ShadeBatchArgs& a, uint32_t p) {
-    PixelRef r;
-    r.o = find_obs(a.pix_pre, a.n, p);
-    r.l = p - __ldg(a.pix_pre + r.o);
-    uint32_t w = a.obs[r.o].width;
-    r.px = r.l % w;
-    r.py = r.l / w;
-    return r;
-}
-
-// The HDR colour of pixel `p` (renderer.rs:369-404), with shadow rays answered by `occ`.
-template <class Occ>
-__device__ __forceinline__ F3 pixel_color(const ShadeBatchArgs& a, const PixelRef& pr, uint32_t p, Occ& occ, Hit* h,
-                                          uint32_t* shadow_rays) {
-    const SrGpuUniforms& U = a.U[pr.o];
-    const Cam cam = cam_of(a.cam, pr.o);
-    float4 ro, rd;
-    float sx, sy;
-    camera_ray(U, cam, pr.px, pr.py, &ro, &rd, &sx, &sy);
-    uint32_t slot = a.slots[p];
-    F3 color;
-    if (slot != 0xFFFFFFFFu) {
-        float4 hr = a.hits[p];
-        GeomHit gh{hr.x, hr.y, hr.z, hr.w};
-        interpolate(a.s.attrs + 12u * slot, ro, rd, gh, h);
-        color = shade_hit(a.s, U, cam, rd, *h, occ, shadow_rays);
-        if (U.num_haze > 0u) color = apply_haze(color, h->event, U);
-    } else {
-        color = shade_sky(rd);
+    uint8_t state;
+    bool trace_here;
+    __device__ bool operator()(float4 o, float4 d, float t0, float t1) {
+        if (trace_here) return occluded_wide<COUNT>(*s, o, d, t0, t1, err, work);
+        if (state == 0) atomicOr(err, ERR_SHADOW_MISMATCH);
+        return state == 2;
     }
-    if (U.mode == 0u && a.s.num_stars > 0u)
-        color = add(color, stars_brute(a.s, U, cam, ro, rd, sx, sy, slot != 0xFFFFFFFFu ? h->lambda : INFINITY, a.bb));
-    return color;
-}
-
-__device__ __forceinline__ void write_pixel(const ShadeBatchArgs& a, const PixelRef& pr, uint32_t p, F3 color, const Hit& h,
-                                            uint32_t slot) {
-    const ObsDev& od = a.obs[pr.o];
-    a.hdr[(size_t)od.pyr_base + pr.l] = make_float4(color.x, color.y, color.z, 0.0f);
-    if (a.hit_id)
-        a.hit_id[p] = slot == 0xFFFFFFFFu ? 0xFFFFFFFFu : (a.s.leaf_to_orig ? __ldg(a.s.leaf_to_orig + slot) : slot);
-    if (a.lambda) a.lambda[p] = slot == 0xFFFFFFFFu ? 0.0f : h.lambda;
-    if (a.tau) a.tau[p] = slot == 0xFFFFFFFFu ? 0.0f : h.tau;
-}
+};
 
 template <bool COUNT>
 __global__ void __launch_bounds__(256) k_shade_batch(ShadeBatchArgs a) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    bool live = p < a.total_px;
-    // Does this pixel's main light need a shadow ray (compute_illumination, renderer.rs:617-645)?
-    bool queued = false;
-    ShadowRay sr;
-    PixelRef pr{0, 0, 0, 0};
-    uint32_t slot = 0xFFFFFFFFu;
-    if (live) {
-        pr = pixel_of(a, p);
-        slot = a.slots[p];
-        const SrGpuUniforms& U = a.U[pr.o];
-        if (slot != 0xFFFFFFFFu && U.mode == 0u && U.shadow_mode != 0u && U.num_flashes == 0u) {
-            const Cam cam = cam_of(a.cam, pr.o);
-            float4 ro, rd;
-            float sx, sy;
-            camera_ray(U, cam, pr.px, pr.py, &ro, &rd, &sx, &sy);
-            float4 hr = a.hits[p];
-            GeomHit gh{hr.x, hr.y, hr.z, hr.w};
-            Hit h;
-            interpolate(a.s.attrs + 12u * slot, ro, rd, gh, &h);
-            Mat m = load_mat(a.s.mats, h.material);
-            if (m.pattern == 0u) {
-                float4 tl;
-                float dist;
-                light_ray(U, cam, h.event, &tl, &dist);
-                if (fmaxf(rest_frame_cos(tl, h.normal, h.four_vel), 0.0f) > 0.0f) {
-                    queued = true;
-                    sr.origin = h.event;
-                    sr.dir = tl;
-                    sr.t_max = dist - 2e-3f;
-                    sr.pixel = p;
-                }
-            }
-        }
-    }
-    // Warp-aggregated append to the shadow queue.
-    unsigned mask = __ballot_sync(0xFFFFFFFFu, queued);
-    if (mask) {
-        uint32_t lane = threadIdx.x & 31u, leader = __ffs(mask) - 1u, base = 0;
-        if (lane == leader) base = atomicAdd(a.counters + 3, (uint32_t)__popc(mask));
-        base = __shfl_sync(0xFFFFFFFFu, base, leader);
-        if (queued) a.queue[base + __popc(mask & ((1u << lane) - 1u))] = sr;
-    }
-    if (!live || queued) return;
+    if (p >= a.total_px) return;
+    uint32_t o = find_obs(a.pix_pre, a.n, p);
+    uint32_t l = p - __ldg(a.pix_pre + o);
+    const ObsDev& od = a.obs[o];
+    uint32_t px = l % od.width, py = l / od.width;
+    const SrGpuUniforms& U = a.U[o];
+    const Cam cam = cam_of(a.cam, o);
+    float4 ro, rd;
+    float sx, sy;
+    camera_ray(U, cam, px, py, &ro, &rd, &sx, &sy);
+    uint32_t slot = a.slots[p];
     Work work{0, 0, 0};
-    InlineOccluder<COUNT> occ{&a.ws, a.counters + 1, &work};
     uint32_t shadow_rays = 0;
     Hit h;
     h.lambda = 0.0f;
     h.tau = 0.0f;
-    F3 color = pixel_color(a, pr, p, occ, &h, &shadow_rays);
-    write_pixel(a, pr, p, color, h, slot);
+    F3 color;
+    if (slot != 0xFFFFFFFFu) {
+        float4 hr = a.hits[p];
+        GeomHit gh{hr.x, hr.y, hr.z, hr.w};
+        interpolate(a.s.attrs + 12u * slot, ro, rd, gh, &h);
+        FrameOccluder<COUNT> occ{&a.ws, a.counters + 1, &work, a.shadow[p], U.num_flashes != 0u};
+        color = shade_hit(a.s, U, cam, rd, h, occ, &shadow_rays);
+        if (U.num_haze > 0u) color = apply_haze(color, h.event, U);
+    } else {
+        color = shade_sky(rd);
+    }
+    if (U.mode == 0u && a.s.num_stars > 0u)
+        color = add(color, stars_brute(a.s, U, cam, ro, rd, sx, sy, slot != 0xFFFFFFFFu ? h.lambda : INFINITY, a.bb));
+    a.hdr[(size_t)od.pyr_base + l] = make_float4(color.x, color.y, color.z, 0.0f);
+    if (a.hit_id)
+        a.hit_id[p] = slot == 0xFFFFFFFFu ? 0xFFFFFFFFu : (a.s.leaf_to_orig ? __ldg(a.s.leaf_to_orig + slot) : slot);
+    if (a.lambda) a.lambda[p] = h.lambda;
+    if (a.tau) a.tau[p] = h.tau;
     if (shadow_rays) atomicAdd(a.counters, shadow_rays);
     if (COUNT && work.nodes) add_work(a.work + 3, work);
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(256) k_shadow_batch(WideScene ws, const ShadowRay* queue, const uint32_t* qlen,
-                                                       uint8_t* qflags, uint32_t* fetch, uint32_t* err,
-                                                       unsigned long long* work_out) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t n = *qlen;
-    Work work{0, 0, 0};
-    for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(fetch, 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= n) break;
-        uint32_t i = base + lane;
-        if (i < n) {
-            const ShadowRay& r = queue[i];
-            qflags[i] = occluded_wide<COUNT>(ws, r.origin, r.dir, 2e-3f, r.t_max, err, &work) ? 1 : 0;
-        }
-    }
-    if (COUNT && work.nodes) add_work(work_out + 3, work);
-}
+}  // namespace srk
 
-__global__ void __launch_bounds__(256) k_finish_batch(ShadeBatchArgs a) {
-    const uint32_t n = a.counters[3];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t p = a.queue[i].pixel;
-        PixelRef pr = pixel_of(a, p);
-        QueuedOccluder occ{a.qflags[i] != 0};
-        uint32_t shadow_rays = 0;
-        Hit h;
-        F3 color = pixel_color(a, pr, p, occ, &h, &shadow_rays);
-        write_pixel(a, pr, p, color, h, a.slots[p]);
-        atomicAdd(a.counters, shadow_rays);
-    }
-}
+#include "sr_batch_bloom.cuh"
 
-// Bloom over every observer's pyramid (bloom.rs:54-125); `pre` is the per-observer prefix of the
-// level's pixel counts.
-__constant__ float DOWN_WB[4] = {0.125f, 0.375f, 0.375f, 0.125f};
-
-__global__ void k_bloom_down_batch(float4* hdr, const ObsDev* obs, const uint32_t* pre, uint32_t n, int k) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= __ldg(pre + n)) return;
-    uint32_t o = find_obs(pre, n, i);
-    const ObsDev& od = obs[o];
-    uint32_t l = i - __ldg(pre + o);
-    uint32_t dw = od.lw[k], x = l % dw, y = l / dw;
-    uint32_t sw = od.lw[k - 1], sh = od.lh[k - 1];
-    const float4* src = hdr + od.pyr_base + od.loff[k - 1];
-    float ax = 0.0f, ay = 0.0f, az = 0.0f;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        int syi = 2 * (int)y - 1 + j;
-        syi = syi < 0 ? 0 : (syi > (int)sh - 1 ? (int)sh - 1 : syi);
-        float rx = 0.0f, ry = 0.0f, rz = 0.0f;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            int sxi = 2 * (int)x - 1 + q;
-            sxi = sxi < 0 ? 0 : (sxi > (int)sw - 1 ? (int)sw - 1 : sxi);
-            float4 v = src[(size_t)syi * sw + sxi];
-            rx = rx + v.x * DOWN_WB[q];
-            ry = ry + v.y * DOWN_WB[q];
-            rz = rz + v.z * DOWN_WB[q];
-        }
-        ax = ax + rx * DOWN_WB[j];
-        ay = ay + ry * DOWN_WB[j];
-        az = az + rz * DOWN_WB[j];
-    }
-    hdr[od.pyr_base + od.loff[k] + l] = make_float4(ax, ay, az, 0.0f);
-}
-
-__device__ __forceinline__ float4 upsample_b(const float4* c, uint32_t cw, uint32_t ch, uint32_t x, uint32_t y) {
-    uint32_t mx = x / 2, my = y / 2;
-    int ox = (x % 2 == 0) ? (int)mx - 1 : (int)mx + 1;
-    int oy = (y % 2 == 0) ? (int)my - 1 : (int)my + 1;
-    uint32_t x1 = (uint32_t)(ox < 0 ? 0 : (ox > (int)cw - 1 ? (int)cw - 1 : ox));
-    uint32_t y1 = (uint32_t)(oy < 0 ? 0 : (oy > (int)ch - 1 ? (int)ch - 1 : oy));
-    float4 A = c[(size_t)my * cw + mx], B = c[(size_t)my * cw + x1];
-    float4 E = c[(size_t)y1 * cw + mx], G = c[(size_t)y1 * cw + x1];
-    float r0x = A.x * 0.75f + B.x * 0.25f, r0y = A.y * 0.75f + B.y * 0.25f, r0z = A.z * 0.75f + B.z * 0.25f;
-    float r1x = E.x * 0.75f + G.x * 0.25f, r1y = E.y * 0.75f + G.y * 0.25f, r1z = E.z * 0.75f + G.z * 0.25f;
-    return make_float4(r0x * 0.75f + r1x * 0.25f, r0y * 0.75f + r1y * 0.25f, r0z * 0.75f + r1z * 0.25f, 0.0f);
-}
-
-__global__ void k_bloom_up_batch(float4* hdr, const ObsDev* obs, const uint32_t* pre, uint32_t n, int k) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= __ldg(pre + n)) return;
-    uint32_t o = find_obs(pre, n, i);
-    const ObsDev& od = obs[o];
-    uint32_t l = i - __ldg(pre + o);
-    uint32_t w = od.lw[k], x = l % w, y = l / w;
-    float4 up = upsample_b(hdr + od.pyr_base + od.loff[k + 1], od.lw[k + 1], od.lh[k + 1], x, y);
-    float4* dst = hdr + od.pyr_base + od.loff[k] + l;
-    float4 v = *dst;
-    *dst = make_float4(v.x + up.x, v.y + up.y, v.z + up.z, 0.0f);
-}
-
-__global__ void __launch_bounds__(256) k_bloom_composite_batch(const float4* hdr, const ObsDev* obs, const uint32_t* pre,
-                                                               uint32_t n, uint32_t* rgb, const uint32_t* tables) {
-    __shared__ uint8_t lut[SR_GAMMA_LUT_SIZE];
-    for (uint32_t i = threadIdx.x; i < SR_GAMMA_LUT_SIZE; i += blockDim.x) lut[i] = (uint8_t)__ldg(tables + i);
-    __syncthreads();
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= __ldg(pre + n)) return;
-    uint32_t o = find_obs(pre, n, i);
-    const ObsDev& od = obs[o];
-    uint32_t l = i - __ldg(pre + o);
-    uint32_t w = od.lw[0], x = l % w, y = l / w;
-    const float strength = 0.04f;
-    const float keep = 1.0f - strength;
-    const float halo = strength / (float)SR_BLOOM_LEVELS;
-    float4 up = upsample_b(hdr + od.pyr_base + od.loff[1], od.lw[1], od.lh[1], x, y);
-    float4 c = hdr[od.pyr_base + l];
-    float cx = c.x * keep + up.x * halo, cy = c.y * keep + up.y * halo, cz = c.z * keep + up.z * halo;
-    float mx = cx / (1.0f + cx * 0.35f), my = cy / (1.0f + cy * 0.35f), mz = cz / (1.0f + cz * 0.35f);
-    mx = mx < 0.0f ? 0.0f : (mx > 1.0f ? 1.0f : mx);
-    my = my < 0.0f ? 0.0f : (my > 1.0f ? 1.0f : my);
-    mz = mz < 0.0f ? 0.0f : (mz > 1.0f ? 1.0f : mz);
-    const float scale = (float)(SR_GAMMA_LUT_SIZE - 1);
-    float fx = mx * scale, fy = my * scale, fz = mz * scale;
-    uint32_t ix = fx > 0.0f ? (uint32_t)fx : 0u, iy = fy > 0.0f ? (uint32_t)fy : 0u, iz = fz > 0.0f ? (uint32_t)fz : 0u;
-    rgb[i] = ((uint32_t)lut[ix] << 16) | ((uint32_t)lut[iy] << 8) | (uint32_t)lut[iz];
-}
+namespace srk {
 
 // ---------------------------------------------------------------------------------------------
 // The batch sequence.
@@ -542,9 +664,10 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
     if (r.n == 0) return cudaSuccess;
     Shape sh = make_shape(r, t);
     const uint32_t n = r.n, stride = n + 1;
+    if ((uint64_t)sh.total_tiles * 32 >= (1ull << 32)) return cudaErrorInvalidValue;
     cudaError_t e;
     // Buffers (grown on demand; a growth invalidates every captured graph).
-    size_t old_hits = c.hits.bytes, old_hdr = c.hdr.bytes, old_U = c.U.bytes, old_q = c.queue.bytes, old_rgb = c.rgb.bytes;
+    size_t old_hits = c.hits.bytes, old_hdr = c.hdr.bytes, old_U = c.U.bytes, old_sh = c.shadow.bytes, old_rgb = c.rgb.bytes;
     if ((e = c.U.ensure(n * sizeof(SrGpuUniforms))) != cudaSuccess) return e;
     if ((e = c.cam64.ensure(n * sizeof(SrCameraF64))) != cudaSuccess) return e;
     if ((e = c.cam.ensure(n * 6 * sizeof(float4))) != cudaSuccess) return e;
@@ -552,15 +675,14 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
     if ((e = c.lvl_pre.ensure(sh.pre.size() * 4)) != cudaSuccess) return e;
     if ((e = c.hits.ensure((size_t)sh.total_px * sizeof(float4))) != cudaSuccess) return e;
     if ((e = c.slots.ensure((size_t)sh.total_px * 4)) != cudaSuccess) return e;
-    if ((e = c.queue.ensure((size_t)sh.total_px * sizeof(ShadowRay))) != cudaSuccess) return e;
-    if ((e = c.qflags.ensure((size_t)sh.total_px)) != cudaSuccess) return e;
+    if ((e = c.shadow.ensure((size_t)sh.total_px)) != cudaSuccess) return e;  // shadow states
     if ((e = c.hdr.ensure((size_t)sh.total_pyr * sizeof(float4))) != cudaSuccess) return e;
     if (!r.rgb && (e = c.rgb.ensure((size_t)sh.total_px * 4)) != cudaSuccess) return e;
     if ((e = c.hU.ensure(n * sizeof(SrGpuUniforms))) != cudaSuccess) return e;
     if ((e = c.hcam64.ensure(n * sizeof(SrCameraF64))) != cudaSuccess) return e;
     if ((e = c.hobs.ensure(n * sizeof(ObsDev))) != cudaSuccess) return e;
     if ((e = c.hlvl.ensure(sh.pre.size() * 4)) != cudaSuccess) return e;
-    if (c.hits.bytes != old_hits || c.hdr.bytes != old_hdr || c.U.bytes != old_U || c.queue.bytes != old_q ||
+    if (c.hits.bytes != old_hits || c.hdr.bytes != old_hdr || c.U.bytes != old_U || c.shadow.bytes != old_sh ||
         c.rgb.bytes != old_rgb)
         fast_release(c);
     // The previous batch's copies from the pinned staging must have run before it is rewritten.
@@ -595,24 +717,36 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
         if (timed) cudaEventRecord(r.ev[0], st);
         TraceBatchArgs ta;
         ta.ws = ws;
+        ta.attrs = sd.attrs;
+        ta.mats = sd.mats;
         ta.U = c.U.as<SrGpuUniforms>();
         ta.cam = c.cam.as<float4>();
         ta.obs = c.obs.as<ObsDev>();
         ta.tile_pre = tile_pre;
         ta.n = n;
-        ta.total_tiles = sh.total_tiles;
+        ta.total_rays = sh.total_tiles * 32u;
         ta.tile_w = t.tile_w;
         ta.tile_h = t.tile_h;
         ta.hits = c.hits.as<float4>();
         ta.slots = c.slots.as<uint32_t>();
+        ta.shadow = c.shadow.as<uint8_t>();
+        ta.chunk_rays = 32u * t.chunk_tiles;
+        ta.refill_lanes = t.refill_lanes;
+        ta.leaf_batch = t.leaf_batch;
         ta.counter = counters + 2;
         ta.err = counters + 1;
         ta.work = work;
         uint32_t blocks = (uint32_t)c.num_sms * t.blocks_per_sm;
         uint32_t need = (uint32_t)(((uint64_t)sh.total_tiles * 32 + t.block_threads - 1) / t.block_threads);
         if (blocks > need) blocks = need;
-        if (r.count_work) k_trace_batch<true><<<blocks, t.block_threads, 0, st>>>(ta);
-        else k_trace_batch<false><<<blocks, t.block_threads, 0, st>>>(ta);
+        const size_t smem = t.leaf_coop ? (size_t)(t.block_threads / 32) * COOP_SMEM_PER_WARP : 0;
+        if (t.leaf_coop) {
+            if (r.count_work) k_trace_batch<true, true><<<blocks, t.block_threads, smem, st>>>(ta);
+            else k_trace_batch<false, true><<<blocks, t.block_threads, smem, st>>>(ta);
+        } else {
+            if (r.count_work) k_trace_batch<true, false><<<blocks, t.block_threads, 0, st>>>(ta);
+            else k_trace_batch<false, false><<<blocks, t.block_threads, 0, st>>>(ta);
+        }
         if ((x = cudaGetLastError()) != cudaSuccess) return x;
         if (timed) cudaEventRecord(r.ev[1], st);
         ShadeBatchArgs sa;
@@ -626,26 +760,17 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
         sa.total_px = sh.total_px;
         sa.hits = ta.hits;
         sa.slots = ta.slots;
+        sa.shadow = ta.shadow;
         sa.hdr = c.hdr.as<float4>();
         sa.hit_id = r.hit_id;
         sa.lambda = r.lambda;
         sa.tau = r.tau;
-        sa.queue = c.queue.as<ShadowRay>();
-        sa.qflags = c.qflags.as<uint8_t>();
         sa.counters = counters;
         sa.work = work;
         sa.bb = bb;
         uint32_t gpx = (sh.total_px + 255) / 256;
         if (r.count_work) k_shade_batch<true><<<gpx, 256, 0, st>>>(sa);
         else k_shade_batch<false><<<gpx, 256, 0, st>>>(sa);
-        // The shadow queue: reuse the tile counter slot ([2]) for fetching after the trace is done.
-        if ((x = cudaMemsetAsync(counters + 2, 0, 4, st)) != cudaSuccess) return x;
-        uint32_t sblocks = (uint32_t)c.num_sms * 8;
-        if (r.count_work)
-            k_shadow_batch<true><<<sblocks, 256, 0, st>>>(ws, sa.queue, counters + 3, sa.qflags, counters + 2, counters + 1, work);
-        else
-            k_shadow_batch<false><<<sblocks, 256, 0, st>>>(ws, sa.queue, counters + 3, sa.qflags, counters + 2, counters + 1, work);
-        k_finish_batch<<<(uint32_t)c.num_sms * 4, 256, 0, st>>>(sa);
         if ((x = cudaGetLastError()) != cudaSuccess) return x;
         if (timed) {
             cudaEventRecord(r.ev[2], st);
@@ -681,6 +806,8 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
     key = mix(key, reinterpret_cast<uintptr_t>(ws.boxes));
     key = mix(key, ((uint64_t)t.block_threads << 32) | t.blocks_per_sm);
     key = mix(key, ((uint64_t)t.tile_w << 32) | t.tile_h);
+    key = mix(key, ((uint64_t)t.chunk_tiles << 40) | ((uint64_t)t.refill_lanes << 24) | ((uint64_t)t.leaf_batch << 8) |
+                       t.leaf_coop);
     for (auto& o : sh.obs) key = mix(key, ((uint64_t)o.width << 32) | o.height);
     auto it = c.graphs.find(key);
     if (it == c.graphs.end()) {

@@ -67,15 +67,6 @@ struct ObsDev {
     uint32_t loff[SR_BLOOM_LEVELS + 2];  // level offsets inside this observer's pyramid
 };
 
-// Shadow-ray queue entry: the main light's shadow ray of one pixel.
-struct ShadowRay {
-    float4 origin;
-    float4 dir;
-    float t_max;
-    uint32_t pixel;  // global pixel index of the batch
-    uint32_t pad[2];
-};
-
 // A captured batch sequence, replayed while the batch's shape is unchanged.
 struct GraphEntry {
     cudaGraph_t graph = nullptr;
@@ -86,7 +77,8 @@ struct FastCtx {
     int num_sms = 148;
     int max_smem = 0;
     // Batch buffers, grown on demand.
-    DevMem U, cam64, cam, obs, lvl_pre, hits, slots, queue, qflags, hdr, rgb;
+    // shadow: one byte per pixel, the main light's shadow ray as traced (0 none, 1 clear, 2 occluded)
+    DevMem U, cam64, cam, obs, lvl_pre, hits, slots, shadow, hdr, rgb;
     HostMem hU, hcam64, hobs, hlvl;
     uint32_t cap_obs = 0;
     std::map<uint64_t, GraphEntry> graphs;

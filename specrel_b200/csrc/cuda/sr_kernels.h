@@ -44,6 +44,9 @@ struct FrameDev {
 constexpr uint32_t ERR_TRAVERSAL_LIMIT = 1u;
 constexpr uint32_t ERR_BAD_MATERIAL = 2u;
 constexpr uint32_t ERR_BAD_INDEX = 4u;
+// The fast path's shading asked for a main-light shadow result the trace kernel did not produce
+// (the two evaluate the same condition; a mismatch is an internal error).
+constexpr uint32_t ERR_SHADOW_MISMATCH = 8u;
 
 // Pyramid geometry of bloom.rs:28-49 for one frame.
 struct Pyramid {

@@ -71,6 +71,34 @@ def test_fp64_camera_batch_equals_single_frames(engine, scene):
         off += n
 
 
+@pytest.mark.parametrize("tiling", [(8, 4, 1, 32, 0, 1), (8, 4, 16, 1, 1, 32), (4, 8, 4, 16, 1, 8), (8, 4, 4, 8, 0, 16)])
+def test_every_schedule_gives_the_same_frames(engine, scene, tiling):
+    """Chunk size, refill threshold, leaf batching and cooperative leaf tests change only the schedule: every
+    setting gives the plain path's frames (with shadows, FP64 cameras)."""
+    tw, th, chunk, refill, coop, leaf_batch = tiling
+    keep = engine.tuning(3)
+    t = engine.tuning(3)
+    t.tile_w, t.tile_h, t.chunk_tiles, t.refill_lanes, t.leaf_coop, t.leaf_batch = tw, th, chunk, refill, coop, leaf_batch
+    engine.set_tuning(3, t)
+    try:
+        obs, us, cams = _observers(13, 4, int(scene.info.n_nodes), scale=4)
+        out = _batch(engine, 3, us, cams)
+    finally:
+        engine.set_tuning(3, keep)
+    off = 0
+    for u, c in zip(us, cams):
+        n = u.size[0] * u.size[1]
+        assert (out[off:off + n] == engine.render(3, u, path=sr.SR_PATH_PLAIN, cam=c).rgb).all()
+        off += n
+
+
+def test_invalid_tuning_rejected(engine, scene):
+    t = engine.tuning(3)
+    t.refill_lanes = 0
+    with pytest.raises(sr.SrError):
+        engine.set_tuning(3, t)
+
+
 def test_fast_traversal_visits_the_reference_nodes(engine, scene):
     """The fast path's traversal work equals the oracle's instrumented Bvh4D::trace: the same
     internal nodes and the same tetrahedron tests, frame total."""
