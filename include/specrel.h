@@ -255,6 +255,9 @@ typedef struct SrTuning {
     uint32_t refill_lanes;    /* idle lanes that make a warp load new rays: 1..32 (32: all idle) */
     uint32_t leaf_coop;       /* 1: a warp tests the leaves of all its lanes together */
     uint32_t leaf_batch;      /* lanes on a leaf before the warp tests leaves: 1..32 */
+    uint32_t home_pct;        /* share of the tiles (0..100) split into one band per SM, which the
+                                 warps on that SM take first; the rest go in frame order */
+    uint32_t reserved[3];     /* 0 */
 } SrTuning;
 sr_status sr_get_tuning(const sr_ctx* ctx, uint32_t scene_idx, SrTuning* out);
 sr_status sr_set_tuning(sr_ctx* ctx, uint32_t scene_idx, const SrTuning* t);
@@ -272,7 +275,7 @@ static_assert(sizeof(SrGpuGeom) == 80, "GpuGeom is 80 bytes (gpu.rs:68-74)");
 static_assert(sizeof(SrGpuAttr) == 192, "GpuAttr is 192 bytes (gpu.rs:79-92)");
 static_assert(sizeof(SrGpuMaterial) == 48, "GpuMaterial is 48 bytes (gpu.rs:96-100)");
 static_assert(sizeof(SrGpuUniforms) == 768, "GpuUniforms is 768 bytes (gpu.rs:122-144)");
-static_assert(sizeof(SrTuning) == 32, "SrTuning is 8 words");
+static_assert(sizeof(SrTuning) == 48, "SrTuning is 12 words");
 static_assert(offsetof(SrGpuUniforms, light_pos) == 80, "Uniforms.light_pos");
 static_assert(offsetof(SrGpuUniforms, num_nodes) == 124, "Uniforms.num_nodes");
 static_assert(offsetof(SrGpuUniforms, frontier_origin) == 128, "Uniforms.frontier_origin");

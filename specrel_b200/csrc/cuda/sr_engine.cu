@@ -557,9 +557,9 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
     // The schedules worth timing: whole-warp refills of single tiles were fastest on every scene
     // measured (wider chunks or partial refills spread the rays in flight over more of the tree).
     const uint32_t threads[] = {128, 256};
-    const uint32_t per_sm[] = {4, 8};
+    const uint32_t per_sm[] = {6, 12};
     const uint32_t tiles[][2] = {{8, 4}, {4, 8}};
-    const uint32_t leaf_batches[] = {1, 8};
+    const uint32_t leaf_batches[] = {1};
     std::vector<SrTuning> cand;
     for (uint32_t bt : threads)
         for (uint32_t bs : per_sm)

@@ -108,13 +108,14 @@ SrTuning fast_default_tuning(const FastCtx& c) {
     (void)c;
     SrTuning t{};
     t.block_threads = 128;
-    t.blocks_per_sm = 8;
-    t.tile_w = 8;
-    t.tile_h = 4;
+    t.blocks_per_sm = 12;
+    t.tile_w = 4;
+    t.tile_h = 8;
     t.chunk_tiles = 1;
     t.refill_lanes = 32;
     t.leaf_coop = 0;
     t.leaf_batch = 1;
+    t.home_pct = 0;
     return t;
 }
 
@@ -123,7 +124,8 @@ bool fast_tuning_valid(const FastCtx& c, const SrTuning& t) {
     bool bt = t.block_threads == 64 || t.block_threads == 128 || t.block_threads == 256 || t.block_threads == 512;
     return bt && t.blocks_per_sm >= 1 && t.blocks_per_sm <= 16 && t.tile_w >= 1 && t.tile_w * t.tile_h == 32 &&
            t.chunk_tiles >= 1 && t.chunk_tiles <= 64 && t.refill_lanes >= 1 && t.refill_lanes <= 32 &&
-           t.leaf_coop <= 1 && t.leaf_batch >= 1 && t.leaf_batch <= 32;
+           t.leaf_coop <= 1 && t.leaf_batch >= 1 && t.leaf_batch <= 32 && t.home_pct <= 100 &&
+           t.reserved[0] == 0 && t.reserved[1] == 0 && t.reserved[2] == 0;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -187,6 +189,11 @@ struct TraceBatchArgs {
     uint32_t chunk_rays;    // rays a warp takes from the global counter at a time (a multiple of 32)
     uint32_t refill_lanes;  // idle lanes that make the warp fetch new rays
     uint32_t leaf_batch;    // lanes on a leaf before the warp tests leaves
+    // Lean kernel tile order: SM band b holds tiles [b * band_tiles, (b + 1) * band_tiles) and is
+    // taken through sched[b]; the shared pool, tiles [num_bands * band_tiles, total), through
+    // sched[num_bands].
+    uint32_t num_bands, band_tiles;
+    uint32_t* sched;
     float4* hits;
     uint32_t* slots;
     uint8_t* shadow;  // 0: no main-light shadow ray, 1: cast and clear, 2: cast and occluded
@@ -519,6 +526,106 @@ __global__ void __launch_bounds__(512) k_trace_batch(TraceBatchArgs a) {
     }
 }
 
+// The default schedule (whole-tile refills, one tile per fetch, leaves tested per lane) in its lean
+// form: a warp takes the next 32-ray tile when all its lanes are done, and each lane runs its
+// primary query and then, when the main light needs it, its shadow query to the end, with no
+// warp-wide bookkeeping per step.
+__device__ __forceinline__ uint32_t sm_id() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+    return r;
+}
+
+// The next tile of a warp (called by one lane): its SM's band first, then the shared pool in
+// frame order, then what is left in other SMs' bands. Returns ~0u when every tile is taken.
+// `stage` and `steal` persist across calls (0: band, 1: pool, 2: stealing from band steal).
+__device__ __forceinline__ uint32_t next_tile(const TraceBatchArgs& a, uint32_t home, uint32_t& stage, uint32_t& steal) {
+    const uint32_t total_tiles = a.total_rays >> 5;
+    if (stage == 0) {
+        uint32_t v = atomicAdd(a.sched + home, 1u);
+        if (v < a.band_tiles) return home * a.band_tiles + v;
+        stage = 1;
+    }
+    const uint32_t pool_base = a.num_bands * a.band_tiles;
+    if (stage == 1) {
+        uint32_t v = atomicAdd(a.sched + a.num_bands, 1u);
+        if (v < total_tiles - pool_base) return pool_base + v;
+        stage = 2;
+    }
+    while (steal < a.num_bands) {
+        const uint32_t b = (home + steal) % a.num_bands;
+        if (*(volatile uint32_t*)(a.sched + b) < a.band_tiles) {
+            uint32_t v = atomicAdd(a.sched + b, 1u);
+            if (v < a.band_tiles) return b * a.band_tiles + v;
+        }
+        ++steal;
+    }
+    return ~0u;
+}
+
+// MINB > 0: 128-thread blocks with at least MINB resident per SM (the register budget that
+// allows); MINB == 0: any block size up to 512.
+template <bool COUNT, int MINB>
+__global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_trace_lean(TraceBatchArgs a) {
+    const uint32_t lane = threadIdx.x & 31u;
+    Work wp{0, 0, 0}, wsh{0, 0, 0};
+    uint2 st[FAST_STACK];
+    const uint32_t home = a.num_bands ? sm_id() % a.num_bands : 0u;
+    uint32_t stage = a.num_bands ? 0u : 1u, steal = 0;
+    for (;;) {
+        uint32_t tile = 0;
+        if (lane == 0) tile = next_tile(a, home, stage, steal);
+        tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+        if (tile == ~0u) break;
+        const uint32_t base = tile << 5;
+        uint32_t obs, px, py, pix;
+        if (!ray_pixel(a, base + lane, &obs, &px, &py, &pix)) continue;
+        const Cam cam = cam_of(a.cam, obs);
+        const SrGpuUniforms& U = a.U[obs];
+        float4 o, d;
+        float sx, sy;
+        camera_ray(U, cam, px, py, &o, &d, &sx, &sy);
+        const float4 inv = v4(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z), safe_inv(d.w));
+        float t_max = 180.0f;
+        GeomHit best{0.0f, 0.0f, 0.0f, 0.0f};
+        int slot = -1;
+        if (!a.ws.empty) {
+            float en, ex;
+            slab_interval(a.ws.root_min, a.ws.root_max, neg4(o), inv, 1e-3f, t_max, &en, &ex);
+            if (ex >= en && en < t_max)  // else the ray misses the scene's box (bvh4d.rs:451)
+                slot = closest_lean<COUNT>(a.ws, a.ws.root_ref, o, d, inv, 1e-3f, t_max, best, st, a.err, wp);
+        }
+        a.hits[pix] = make_float4(best.lambda, best.u, best.v, best.w);
+        a.slots[pix] = slot < 0 ? 0xFFFFFFFFu : (uint32_t)slot;
+        uint8_t sh = 0;
+        if (slot >= 0 && U.mode == 0u && U.shadow_mode != 0u && U.num_flashes == 0u) {
+            // compute_illumination's shadow-ray condition (renderer.rs:617-633).
+            const float4* at = a.attrs + 12u * (uint32_t)slot;
+            const uint32_t mat = __float_as_uint(__ldg(at + 10).z);
+            if (__float_as_uint(__ldg(a.mats + 3u * mat + 2u).y) == 0u) {
+                const float4 ev = add4(o, mul4(d, best.lambda));
+                float4 tl;
+                float dist;
+                light_ray(U, cam, ev, &tl, &dist);
+                if (fmaxf(rest_frame_cos(tl, __ldg(at + 8), __ldg(at + 9)), 0.0f) > 0.0f) {
+                    // Bvh4D::is_occluded(hit.event, to_light, 2e-3, dist - 2e-3) (renderer.rs:636-641).
+                    sh = 1;
+                    const float4 sinv = v4(safe_inv(tl.x), safe_inv(tl.y), safe_inv(tl.z), safe_inv(tl.w));
+                    const float s0 = 2e-3f, s1 = dist - 2e-3f;
+                    float en, ex;
+                    slab_interval(a.ws.root_min, a.ws.root_max, neg4(ev), sinv, s0, s1, &en, &ex);
+                    if (ex >= en && any_lean<COUNT>(a.ws, a.ws.root_ref, ev, tl, sinv, s0, s1, st, a.err, wsh)) sh = 2;
+                }
+            }
+        }
+        a.shadow[pix] = sh;
+    }
+    if (COUNT) {
+        add_work(a.work, wp);
+        add_work(a.work + 3, wsh);
+    }
+}
+
 struct ShadeBatchArgs {
     SceneDev s;
     WideScene ws;
@@ -677,6 +784,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
     if ((e = c.slots.ensure((size_t)sh.total_px * 4)) != cudaSuccess) return e;
     if ((e = c.shadow.ensure((size_t)sh.total_px)) != cudaSuccess) return e;  // shadow states
     if ((e = c.hdr.ensure((size_t)sh.total_pyr * sizeof(float4))) != cudaSuccess) return e;
+    if ((e = c.sched.ensure(((size_t)c.num_sms + 1) * 4)) != cudaSuccess) return e;
     if (!r.rgb && (e = c.rgb.ensure((size_t)sh.total_px * 4)) != cudaSuccess) return e;
     if ((e = c.hU.ensure(n * sizeof(SrGpuUniforms))) != cudaSuccess) return e;
     if ((e = c.hcam64.ensure(n * sizeof(SrCameraF64))) != cudaSuccess) return e;
@@ -712,6 +820,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
         if ((x = cudaMemcpyAsync(c.obs.p, c.hobs.p, n * sizeof(ObsDev), cudaMemcpyHostToDevice, st)) != cudaSuccess) return x;
         if ((x = cudaMemcpyAsync(c.lvl_pre.p, c.hlvl.p, sh.pre.size() * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return x;
         if ((x = cudaMemsetAsync(counters, 0, r.count_work ? 64 : 16, st)) != cudaSuccess) return x;
+        if ((x = cudaMemsetAsync(c.sched.p, 0, c.sched.bytes, st)) != cudaSuccess) return x;
         k_camera_batch<<<(n + 63) / 64, 64, 0, st>>>(n, c.U.as<SrGpuUniforms>(), c.cam64.as<SrCameraF64>(), c.obs.as<ObsDev>(),
                                                      anchor[0], anchor[1], anchor[2], anchor[3], c.cam.as<float4>());
         if (timed) cudaEventRecord(r.ev[0], st);
@@ -734,13 +843,24 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
         ta.refill_lanes = t.refill_lanes;
         ta.leaf_batch = t.leaf_batch;
         ta.counter = counters + 2;
+        ta.sched = c.sched.as<uint32_t>();
+        ta.num_bands = t.home_pct ? (uint32_t)c.num_sms : 0u;
+        ta.band_tiles = ta.num_bands ? (uint32_t)((uint64_t)sh.total_tiles * t.home_pct / 100u / ta.num_bands) : 0u;
+        if (ta.band_tiles == 0) ta.num_bands = 0;
         ta.err = counters + 1;
         ta.work = work;
         uint32_t blocks = (uint32_t)c.num_sms * t.blocks_per_sm;
         uint32_t need = (uint32_t)(((uint64_t)sh.total_tiles * 32 + t.block_threads - 1) / t.block_threads);
         if (blocks > need) blocks = need;
         const size_t smem = t.leaf_coop ? (size_t)(t.block_threads / 32) * COOP_SMEM_PER_WARP : 0;
-        if (t.leaf_coop) {
+        const bool lean = !t.leaf_coop && t.leaf_batch == 1 && t.refill_lanes == 32 && t.chunk_tiles == 1;
+        if (lean) {
+            const int capped = t.block_threads == 128 ? (t.blocks_per_sm >= 16 ? 16 : t.blocks_per_sm >= 12 ? 12 : 0) : 0;
+            if (r.count_work) k_trace_lean<true, 0><<<blocks, t.block_threads, 0, st>>>(ta);
+            else if (capped == 16) k_trace_lean<false, 16><<<blocks, t.block_threads, 0, st>>>(ta);
+            else if (capped == 12) k_trace_lean<false, 12><<<blocks, t.block_threads, 0, st>>>(ta);
+            else k_trace_lean<false, 0><<<blocks, t.block_threads, 0, st>>>(ta);
+        } else if (t.leaf_coop) {
             if (r.count_work) k_trace_batch<true, true><<<blocks, t.block_threads, smem, st>>>(ta);
             else k_trace_batch<false, true><<<blocks, t.block_threads, smem, st>>>(ta);
         } else {
@@ -808,6 +928,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
     key = mix(key, ((uint64_t)t.tile_w << 32) | t.tile_h);
     key = mix(key, ((uint64_t)t.chunk_tiles << 40) | ((uint64_t)t.refill_lanes << 24) | ((uint64_t)t.leaf_batch << 8) |
                        t.leaf_coop);
+    key = mix(key, t.home_pct);
     for (auto& o : sh.obs) key = mix(key, ((uint64_t)o.width << 32) | o.height);
     auto it = c.graphs.find(key);
     if (it == c.graphs.end()) {

@@ -78,7 +78,8 @@ struct FastCtx {
     int max_smem = 0;
     // Batch buffers, grown on demand.
     // shadow: one byte per pixel, the main light's shadow ray as traced (0 none, 1 clear, 2 occluded)
-    DevMem U, cam64, cam, obs, lvl_pre, hits, slots, shadow, hdr, rgb;
+    // sched: the tile counters of the trace kernel, one per SM band then the shared pool's
+    DevMem U, cam64, cam, obs, lvl_pre, hits, slots, shadow, hdr, rgb, sched;
     HostMem hU, hcam64, hobs, hlvl;
     uint32_t cap_obs = 0;
     std::map<uint64_t, GraphEntry> graphs;

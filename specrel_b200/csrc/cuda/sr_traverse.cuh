@@ -164,4 +164,204 @@ __device__ __noinline__ bool occluded_wide(const WideScene& s, float4 o, float4 
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// The lean forms used by the persistent batch kernel. Same visiting order and the same values as
+// trace_wide / occluded_wide; fewer instructions per step:
+//   - the five-way max / min of the slab test use the three-input max.f32 / min.f32 of sm_100
+//     (max and min are exact, the inputs are never NaN: inv is never 0 and boxes are finite);
+//   - a child is taken when its slab interval is non-empty and, for closest-hit queries, entered
+//     before the closest hit. The far child of a pair is therefore not pushed when it is entered
+//     at or beyond the closest hit; the reference pushes it and discards it when popped, so the
+//     nodes visited are the same;
+//   - a stack entry is one 8-byte word (reference, entry parameter bits);
+//   - the slab and tetrahedron arithmetic runs in paired fp32 instructions (below).
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Paired fp32 arithmetic of sm_100 (add / mul .rn.f32x2): each half is the IEEE round-to-nearest
+// result of the scalar operation, so these give the scalar code's values bit for bit, as long as
+// no paired product feeds a paired sum (ptxas fuses that pair into one fma even with --fmad=false
+// and explicit rounding; the code below never forms it). `a - b` is computed as `a + (-b)`, which
+// IEEE 754 defines to be the same operation.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    float2 r;
+    asm("{\n\t.reg .b64 pa, pb, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+        "add.rn.f32x2 pr, pa, pb;\n\tmov.b64 {%0, %1}, pr;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    float2 r;
+    asm("{\n\t.reg .b64 pa, pb, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+        "mul.rn.f32x2 pr, pa, pb;\n\tmov.b64 {%0, %1}, pr;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+// edot (minkowski.rs:198-200): ((a.t b.t + a.x b.x) + a.y b.y) + a.z b.z.
+__device__ __forceinline__ float edot_p(float4 a, float4 b) {
+    const float2 p = mul2(f2(a.x, a.y), f2(b.x, b.y)), q = mul2(f2(a.z, a.w), f2(b.z, b.w));
+    return ((p.x + p.y) + q.x) + q.y;
+}
+
+// Entry and exit parameters of the slab test (Aabb4D::intersect_ray, mesh4d.rs:114-146) for a ray
+// with origin -no: the box is hit when exit >= entry; entry >= t_min > 0.
+__device__ __forceinline__ void slab_interval(float4 bmin, float4 bmax, float4 no, float4 inv, float t_min, float t_max,
+                                              float* en, float* ex) {
+    const float2 i01 = f2(inv.x, inv.y), i23 = f2(inv.z, inv.w);
+    const float2 a01 = mul2(add2(f2(bmin.x, bmin.y), f2(no.x, no.y)), i01);
+    const float2 a23 = mul2(add2(f2(bmin.z, bmin.w), f2(no.z, no.w)), i23);
+    const float2 b01 = mul2(add2(f2(bmax.x, bmax.y), f2(no.x, no.y)), i01);
+    const float2 b23 = mul2(add2(f2(bmax.z, bmax.w), f2(no.z, no.w)), i23);
+    *en = max3f(max3f(t_min, fminf(a01.x, b01.x), fminf(a01.y, b01.y)), fminf(a23.x, b23.x), fminf(a23.y, b23.y));
+    *ex = min3f(min3f(t_max, fmaxf(a01.x, b01.x), fmaxf(a01.y, b01.y)), fmaxf(a23.x, b23.x), fmaxf(a23.y, b23.y));
+}
+
+// SimplexGeom4D::intersect_fast (mesh4d.rs:175-211) in paired arithmetic, for a ray with origin
+// o = -no: the values of intersect_geom bit for bit.
+__device__ __forceinline__ bool intersect_lean(const float4* g, float4 o, float4 no, float4 d, float t_min, float t_max,
+                                               GeomHit* h) {
+    const float4 n = __ldg(g + 1);
+    const float denom = edot_p(n, d);
+    if (fabsf(denom) < 1e-9f) return false;
+    const float4 v0 = __ldg(g);
+    const float2 w01 = add2(f2(v0.x, v0.y), f2(no.x, no.y)), w23 = add2(f2(v0.z, v0.w), f2(no.z, no.w));
+    const float lambda = edot_p(n, make_float4(w01.x, w01.y, w23.x, w23.y)) / denom;
+    if (lambda <= t_min || lambda >= t_max) return false;
+    // The event o + d * lambda in scalar arithmetic: ptxas fuses a paired product followed by a
+    // paired sum into one fused multiply-add (one rounding), whatever the rounding modifiers say.
+    const float4 ev = add4(o, mul4(d, lambda));
+    const float2 q01 = add2(f2(ev.x, ev.y), f2(-v0.x, -v0.y)), q23 = add2(f2(ev.z, ev.w), f2(-v0.z, -v0.w));
+    const float4 q = make_float4(q01.x, q01.y, q23.x, q23.y);
+    const float eps = -1e-5f;
+    const float u = edot_p(__ldg(g + 2), q);
+    if (u < eps || u > 1.0f - eps) return false;
+    const float v = edot_p(__ldg(g + 3), q);
+    if (v < eps || u + v > 1.0f - eps) return false;
+    const float w = edot_p(__ldg(g + 4), q);
+    if (w < eps || u + v + w > 1.0f - eps) return false;
+    h->lambda = lambda;
+    h->u = u;
+    h->v = v;
+    h->w = w;
+    return true;
+}
+
+// Closest hit from node `cur` (the root, already tested against the ray). Returns the slot or
+// -1; `t_max` ends as the closest hit's parameter.
+template <bool COUNT>
+__device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, float4 o, float4 d, float4 inv, float t_min,
+                                            float& t_max, GeomHit& best, uint2* st, uint32_t* err, Work& work) {
+    const float4 no = neg4(o);
+    int slot = -1, sp = 0;
+    uint32_t visits = 0;
+    for (;;) {
+        if (++visits > MAX_VISITS_FAST) {
+            atomicOr(err, ERR_TRAVERSAL_LIMIT);
+            break;
+        }
+        if (!(cur & REF_LEAF)) {
+            if (COUNT) ++work.nodes;
+            const float4* b = s.boxes + 4ull * cur;
+            const float4 lmin = __ldg(b), lmax = __ldg(b + 1), rmin = __ldg(b + 2), rmax = __ldg(b + 3);
+            const uint2 r = __ldg(s.refs + cur);
+            float enl, exl, enr, exr;
+            slab_interval(lmin, lmax, no, inv, t_min, t_max, &enl, &exl);
+            slab_interval(rmin, rmax, no, inv, t_min, t_max, &enr, &exr);
+            const bool hl = exl >= enl && enl < t_max;
+            const bool hr = exr >= enr && enr < t_max;
+            if (hl && hr) {
+                const bool ln = enl <= enr;
+                if (sp < FAST_STACK) st[sp++] = ln ? make_uint2(r.y, __float_as_uint(enr)) : make_uint2(r.x, __float_as_uint(enl));
+                else atomicOr(err, ERR_BAD_INDEX);
+                cur = ln ? r.x : r.y;
+                continue;
+            }
+            if (hl || hr) {
+                cur = hl ? r.x : r.y;
+                continue;
+            }
+        } else {
+            const uint32_t first = cur & REF_FIRST_MASK, cnt = (cur >> REF_COUNT_SHIFT) & 63u;
+            if (COUNT) { ++work.leaves; work.tets += cnt; }
+            for (uint32_t k = first; k < first + cnt; ++k) {
+                GeomHit gh;
+                if (intersect_lean(s.geoms + 5u * k, o, no, d, t_min, t_max, &gh)) {
+                    t_max = gh.lambda;
+                    best = gh;
+                    slot = (int)k;
+                }
+            }
+        }
+        bool found = false;
+        while (sp > 0) {
+            const uint2 e = st[--sp];
+            if (__uint_as_float(e.y) < t_max) {
+                cur = e.x;
+                found = true;
+                break;
+            }
+        }
+        if (!found) break;
+    }
+    return slot;
+}
+
+// Any hit in (t_min, t_max) from node `cur` (the root, already tested): left before right, no
+// culling (Bvh4D::is_occluded, bvh4d.rs:523-578).
+template <bool COUNT>
+__device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float4 o, float4 d, float4 inv, float t_min,
+                                         float t_max, uint2* st, uint32_t* err, Work& work) {
+    const float4 no = neg4(o);
+    int sp = 0;
+    uint32_t visits = 0;
+    for (;;) {
+        if (++visits > MAX_VISITS_FAST) {
+            atomicOr(err, ERR_TRAVERSAL_LIMIT);
+            return false;
+        }
+        if (!(cur & REF_LEAF)) {
+            if (COUNT) ++work.nodes;
+            const float4* b = s.boxes + 4ull * cur;
+            const float4 lmin = __ldg(b), lmax = __ldg(b + 1), rmin = __ldg(b + 2), rmax = __ldg(b + 3);
+            const uint2 r = __ldg(s.refs + cur);
+            float enl, exl, enr, exr;
+            slab_interval(lmin, lmax, no, inv, t_min, t_max, &enl, &exl);
+            slab_interval(rmin, rmax, no, inv, t_min, t_max, &enr, &exr);
+            const bool hl = exl >= enl, hr = exr >= enr;
+            if (hl && hr) {
+                if (sp < FAST_STACK) st[sp++].x = r.y;
+                else atomicOr(err, ERR_BAD_INDEX);
+                cur = r.x;
+                continue;
+            }
+            if (hl || hr) {
+                cur = hl ? r.x : r.y;
+                continue;
+            }
+        } else {
+            const uint32_t first = cur & REF_FIRST_MASK, cnt = (cur >> REF_COUNT_SHIFT) & 63u;
+            if (COUNT) ++work.leaves;
+            for (uint32_t k = first; k < first + cnt; ++k) {
+                if (COUNT) ++work.tets;
+                GeomHit gh;
+                if (intersect_lean(s.geoms + 5u * k, o, no, d, t_min, t_max, &gh)) return true;
+            }
+        }
+        if (sp == 0) return false;
+        cur = st[--sp].x;
+    }
+}
+
 }  // namespace srk

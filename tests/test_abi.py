@@ -43,7 +43,7 @@ def test_struct_layouts_match_the_reference():
     for k, v in offs.items():
         assert getattr(U, k).offset == v, k
     assert L.ATTR_DTYPE.fields["misc"][1] == 160 and L.ATTR_DTYPE.fields["decided_at"][1] == 176
-    assert C.sizeof(L.Tuning) == 32 and L.Tuning.leaf_coop.offset == 24
+    assert C.sizeof(L.Tuning) == 48 and L.Tuning.leaf_coop.offset == 24 and L.Tuning.home_pct.offset == 32
     assert C.sizeof(L.Timings) == 96
 
 

@@ -71,14 +71,17 @@ def test_fp64_camera_batch_equals_single_frames(engine, scene):
         off += n
 
 
-@pytest.mark.parametrize("tiling", [(8, 4, 1, 32, 0, 1), (8, 4, 16, 1, 1, 32), (4, 8, 4, 16, 1, 8), (8, 4, 4, 8, 0, 16)])
+@pytest.mark.parametrize("tiling", [(8, 4, 1, 32, 0, 1, 0), (8, 4, 16, 1, 1, 32, 0), (4, 8, 4, 16, 1, 8, 0),
+                                    (8, 4, 4, 8, 0, 16, 0), (4, 8, 1, 32, 0, 1, 75), (8, 4, 1, 32, 0, 1, 100)])
 def test_every_schedule_gives_the_same_frames(engine, scene, tiling):
-    """Chunk size, refill threshold, leaf batching and cooperative leaf tests change only the schedule: every
+    """Chunk size, refill threshold, leaf batching, cooperative leaf tests and per-SM tile bands
+    change only the schedule: every
     setting gives the plain path's frames (with shadows, FP64 cameras)."""
-    tw, th, chunk, refill, coop, leaf_batch = tiling
+    tw, th, chunk, refill, coop, leaf_batch, home = tiling
     keep = engine.tuning(3)
     t = engine.tuning(3)
     t.tile_w, t.tile_h, t.chunk_tiles, t.refill_lanes, t.leaf_coop, t.leaf_batch = tw, th, chunk, refill, coop, leaf_batch
+    t.home_pct = home
     engine.set_tuning(3, t)
     try:
         obs, us, cams = _observers(13, 4, int(scene.info.n_nodes), scale=4)
