@@ -246,6 +246,28 @@ sr_status sr_render_batch(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* 
                           uint32_t n_observers, uint32_t* rgb_out, uint64_t rgb_len, uint32_t flags,
                           SrTimings* timings);
 
+/* ---- Rendering without device allocation -------------------------------------------------
+ * No counterpart in the reference: an entry point for callers that cannot call cudaMalloc while
+ * they render, for instance an application whose own allocator owns all device memory under a fixed
+ * budget, or a real-time loop in which cudaMalloc/cudaFree (which can synchronize the whole device)
+ * would stall its other streams. sr_render_noalloc renders one frame on the plain path into the
+ * caller's device buffer `rgb_dev` (width*height packed 0x00RRGGBB; `cam64` optional, as in
+ * sr_render_ex) and allocates nothing: its scratch (error counters, FP64 camera rows, the HDR image
+ * and its bloom pyramid) is one static device array of SR_NOALLOC_SCRATCH_BYTES that every GPU
+ * which loads this library holds until the process exits.
+ * - Frames above SR_NOALLOC_MAX_PIXELS pixels (e.g. 512x512 or 640x400 fit) are rejected with
+ *   SR_ERR_INVALID_ARGUMENT.
+ * - The first call on a device looks up the array's device address; make that first call before
+ *   any stream capture.
+ * - Every call uses the same array and leaves its contents behind (the counters are cleared at the
+ *   start of each call). Calls that overlap on one GPU, from other streams or contexts of the
+ *   process, race on it.
+ * - The call waits for its frame (it reads the error flags back) and returns its status. */
+#define SR_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define SR_NOALLOC_MAX_PIXELS (1u << 18)
+sr_status sr_render_noalloc(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, const SrCameraF64* cam64,
+                            uint32_t* rgb_dev);
+
 /* Launch parameters of the fast path; the autotuner (sr_autotune) picks them per scene. */
 typedef struct SrTuning {
     uint32_t block_threads;   /* threads per block of the persistent traversal kernel: 64..512 */

@@ -31,6 +31,8 @@ SR_FLAG_TIMING = 1
 SR_FLAG_DEVICE_OUTPUT = 2
 SR_FLAG_STAR_BRUTE = 4
 SR_FLAG_COUNT_WORK = 8
+SR_NOALLOC_SCRATCH_BYTES = 8 << 20
+SR_NOALLOC_MAX_PIXELS = 1 << 18
 
 # ---- packed layouts (gpu.rs:44-144) ------------------------------------------------------------
 NODE_DTYPE = np.dtype([("min", "<f4", 4), ("max", "<f4", 4), ("right_or_first", "<u4"), ("count", "<u4"),
@@ -160,6 +162,7 @@ SIGNATURES = {
                                  C.POINTER(Outputs), C.POINTER(Timings)]),
     "sr_render_batch": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64),
                                     C.c_uint32, C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(Timings)]),
+    "sr_render_noalloc": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64), C.c_void_p]),
     "sr_get_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),
     "sr_set_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),
     "sr_autotune": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.c_uint32, C.POINTER(Tuning),

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -596,6 +597,86 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
     s.tuning = win;
     if (best) *best = win;
     if (best_ms) *best_ms = win_ms;
+    return SR_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// sr_render_noalloc: the plain path with all of its scratch in one static device array.
+// ---------------------------------------------------------------------------------------------
+
+// Layout of the array: error counters at 0 (the kernels' counters[0..3]), the six float4 rows of
+// the FP64 camera at 256, the HDR image and its bloom pyramid from 512 on.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SR_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr size_t NOALLOC_COUNTERS = 0, NOALLOC_CAM = 256, NOALLOC_HDR = 512;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
+
+// The device address of g_noalloc_scratch on `device`, which must be current. In host code the
+// array's name only identifies the symbol; its address on each device comes from
+// cudaGetSymbolAddress, looked up once per device and kept.
+cudaError_t noalloc_base(int device, unsigned char** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+    if (!g_noalloc_base[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_base[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_base[device]);
+    return cudaSuccess;
+}
+
+}  // namespace
+
+sr_status sr_render_noalloc(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const SrCameraF64* cam64,
+                            uint32_t* rgb_dev) {
+    if (!ctx || !u || !rgb_dev) return SR_ERR_INVALID_ARGUMENT;
+    if (idx >= ctx->scenes.size() || !ctx->scenes[idx] || !ctx->scenes[idx]->present)
+        return fail(ctx, SR_ERR_NO_SCENE, "scene " + std::to_string(idx) + " is not uploaded");
+    const uint64_t npx = (uint64_t)u->size[0] * u->size[1];
+    if (npx == 0) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "frame size must be non-zero");
+    if (npx > SR_NOALLOC_MAX_PIXELS)
+        return fail(ctx, SR_ERR_INVALID_ARGUMENT,
+                    "frame of " + std::to_string(npx) + " pixels exceeds the no-allocation limit of " +
+                        std::to_string(SR_NOALLOC_MAX_PIXELS) + " pixels (SR_NOALLOC_MAX_PIXELS)");
+    if (u->mode > 3 || u->shadow_mode > 2 || u->slice_mode > 3 || u->num_flashes > SR_MAX_FLASHES || u->num_haze > SR_MAX_HAZE_ORIGINS)
+        return fail(ctx, SR_ERR_INVALID_ARGUMENT, "uniform block out of range");
+    const Pyramid pyr = make_pyramid(u->size[0], u->size[1]);
+    if (NOALLOC_HDR + (size_t)pyr.off[SR_BLOOM_LEVELS + 1] * sizeof(float4) > SR_NOALLOC_SCRATCH_BYTES)
+        return fail(ctx, SR_ERR_INVALID_ARGUMENT, "frame's bloom pyramid exceeds the no-allocation scratch");
+    CK(cudaSetDevice(ctx->device), "set device");
+    unsigned char* base = nullptr;
+    CK(noalloc_base(ctx->device, &base), "no-allocation scratch address");
+    SceneSlot& s = *ctx->scenes[idx];
+    FrameDev f{};
+    f.hdr = reinterpret_cast<float4*>(base + NOALLOC_HDR);
+    f.rgb = rgb_dev;
+    f.counters = reinterpret_cast<uint32_t*>(base + NOALLOC_COUNTERS);
+    f.width = u->size[0];
+    f.height = u->size[1];
+    cudaStream_t sm = ctx->stream;
+    // Only the counters must start at zero: the camera rows, every HDR pixel and every pyramid
+    // level are written before they are read.
+    CK(cudaMemsetAsync(f.counters, 0, 4 * sizeof(uint32_t), sm), "clear counters");
+    const float4* cam_dev = nullptr;
+    if (cam64) {
+        float4* rows = reinterpret_cast<float4*>(base + NOALLOC_CAM);
+        CK(launch_camera_f64(*cam64, s.anchor, *u, rows, sm), "camera kernel");
+        cam_dev = rows;
+    }
+    CK(launch_render_plain(scene_dev(ctx, s), *u, cam_dev, f, ctx->bb, sm), "plain render");
+    CK(launch_bloom(f, pyr, ctx->tables.as<uint32_t>(), sm), "bloom");
+    uint32_t counters[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(counters, f.counters, sizeof(counters), cudaMemcpyDeviceToHost, sm), "counters");
+    CK(cudaStreamSynchronize(sm), "render sync");
+    if (counters[1] & ERR_TRAVERSAL_LIMIT) return fail(ctx, SR_ERR_TRAVERSAL_LIMIT, "a ray exceeded the traversal visit limit");
+    if (counters[1]) return fail(ctx, SR_ERR_BAD_SCENE, "device reported a bad index (flags " + std::to_string(counters[1]) + ")");
     return SR_OK;
 }
 
