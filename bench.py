@@ -346,7 +346,8 @@ def run_engine(args, rank, world, local):
                                "light (0,50,0), FP32 traversal + FP64 camera",
                    "observers_per_step_per_gpu": B, "rays_per_step": total_rays, "seed": args.seed,
                    "l2": "inputs larger than L2 (scene %.2f GB on the device vs 126 MB L2)" % (eng.stats(0).device_bytes / 1e9),
-                   "tuning": {k: getattr(tuning, k) for k, _ in tuning._fields_},
+                   "tuning": {k: (list(getattr(tuning, k)) if k == "reserved" else getattr(tuning, k))
+                              for k, _ in tuning._fields_},
                    "scene_build_s": round(build_s, 2), "parallelism": f"replicas x{world}, observers sharded"},
         "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms,
                   "speedup_batched_over_plain": value / plain_value},
