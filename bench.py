@@ -133,7 +133,7 @@ def load_peaks():
 
 def load_traffic():
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "trace_fast_config2.json")
+    p = os.path.join(ROOT, "profiles", "trace_lean_config2.json")
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
@@ -355,7 +355,7 @@ def run_engine(args, rank, world, local):
                 "d2h_bytes_per_step": 4 * RAYS_PER_FRAME * B},
         # Kernels per step: camera, trace, shade, 6 bloom down, 5 bloom up, composite.
         "gpu_launches": int(args.steps * 15),
-        "roofline": {"bound": "hbm", "kernel": "k_trace_batch", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "k_trace_lean", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic,
                      "algorithmic_bytes_per_launch": trace_bytes, "frames_per_launch": B,

@@ -557,27 +557,26 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
     float win_ms = INFINITY;
     // The schedules worth timing: whole-warp refills of single tiles were fastest on every scene
     // measured (wider chunks or partial refills spread the rays in flight over more of the tree).
-    const uint32_t threads[] = {128, 256};
-    const uint32_t per_sm[] = {6, 12};
+    // The schedules worth timing: whole-warp refills of single tiles were fastest on every scene
+    // measured (wider chunks or partial refills spread the rays in flight over more of the tree).
+    const uint32_t shapes[][2] = {{128, 8}, {128, 11}, {256, 4}, {256, 6}, {512, 3}};
     const uint32_t tiles[][2] = {{8, 4}, {4, 8}};
-    const uint32_t leaf_batches[] = {1};
     std::vector<SrTuning> cand;
-    for (uint32_t bt : threads)
-        for (uint32_t bs : per_sm)
-            for (auto& tl : tiles)
-                for (uint32_t lb : leaf_batches)
-                    for (uint32_t coop = 0; coop <= 1; ++coop) {
-                        SrTuning t = keep;
-                        t.block_threads = bt;
-                        t.blocks_per_sm = bs;
-                        t.tile_w = tl[0];
-                        t.tile_h = tl[1];
-                        t.chunk_tiles = 1;
-                        t.refill_lanes = 32;
-                        t.leaf_coop = coop;
-                        t.leaf_batch = lb;
-                        if (fast_tuning_valid(ctx->fast, t)) cand.push_back(t);
-                    }
+    for (auto& sh : shapes)
+        for (auto& tl : tiles)
+            for (uint32_t coop = 0; coop <= 1; ++coop) {
+                SrTuning t = keep;
+                t.block_threads = sh[0];
+                t.blocks_per_sm = sh[1];
+                t.tile_w = tl[0];
+                t.tile_h = tl[1];
+                t.chunk_tiles = 1;
+                t.refill_lanes = 32;
+                t.leaf_coop = coop;
+                t.leaf_batch = 1;
+                t.home_pct = 0;
+                if (fast_tuning_valid(ctx->fast, t)) cand.push_back(t);
+            }
     for (const SrTuning& t : cand) {
         s.tuning = t;
         sr_status st = sr_render_ex(ctx, idx, u, &opts, &o, nullptr);  // warm-up

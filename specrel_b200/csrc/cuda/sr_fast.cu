@@ -2,10 +2,11 @@
 // launches (captured once into a CUDA graph and replayed):
 //
 //   k_camera_batch   FP64 observers (tetrad from rapidity in double, event rebased to the anchor)
-//   k_trace_batch    persistent traversal, one ray per lane, refilled from a per-warp chunk of
-//                    neighbouring tiles. A pixel's work is its primary ray (closest hit), then, when
-//                    the main light needs it, the shadow ray (any hit) as a second phase of the same
-//                    loop, so shadow rays spread over all lanes instead of forming a separate tail.
+//   k_trace_lean     persistent traversal (the default schedule): warps take 32-ray tiles from a
+//                    global counter; each lane traces its pixel's primary ray (closest hit), then,
+//                    when the main light needs it, the shadow ray (any hit) in the same launch.
+//   k_trace_batch    the same work under the other schedules of SrTuning (per-warp chunks of
+//                    tiles, partial refills, postponed or cooperative leaf tests).
 //   k_shade_batch    one thread per pixel: interpolation and shading, with the main light's
 //                    shadow result from the trace kernel (renderer.rs:414-489, 609-653)
 //   bloom            the pyramid of every observer, one launch per level
@@ -108,7 +109,7 @@ SrTuning fast_default_tuning(const FastCtx& c) {
     (void)c;
     SrTuning t{};
     t.block_threads = 128;
-    t.blocks_per_sm = 12;
+    t.blocks_per_sm = 11;
     t.tile_w = 4;
     t.tile_h = 8;
     t.chunk_tiles = 1;
@@ -563,10 +564,8 @@ __device__ __forceinline__ uint32_t next_tile(const TraceBatchArgs& a, uint32_t 
     return ~0u;
 }
 
-// MINB > 0: 128-thread blocks with at least MINB resident per SM (the register budget that
-// allows); MINB == 0: any block size up to 512.
-template <bool COUNT, int MINB>
-__global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_trace_lean(TraceBatchArgs a) {
+template <bool COUNT>
+__global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
     const uint32_t lane = threadIdx.x & 31u;
     Work wp{0, 0, 0}, wsh{0, 0, 0};
     uint2 st[FAST_STACK];
@@ -855,11 +854,8 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
         const size_t smem = t.leaf_coop ? (size_t)(t.block_threads / 32) * COOP_SMEM_PER_WARP : 0;
         const bool lean = !t.leaf_coop && t.leaf_batch == 1 && t.refill_lanes == 32 && t.chunk_tiles == 1;
         if (lean) {
-            const int capped = t.block_threads == 128 ? (t.blocks_per_sm >= 16 ? 16 : t.blocks_per_sm >= 12 ? 12 : 0) : 0;
-            if (r.count_work) k_trace_lean<true, 0><<<blocks, t.block_threads, 0, st>>>(ta);
-            else if (capped == 16) k_trace_lean<false, 16><<<blocks, t.block_threads, 0, st>>>(ta);
-            else if (capped == 12) k_trace_lean<false, 12><<<blocks, t.block_threads, 0, st>>>(ta);
-            else k_trace_lean<false, 0><<<blocks, t.block_threads, 0, st>>>(ta);
+            if (r.count_work) k_trace_lean<true><<<blocks, t.block_threads, 0, st>>>(ta);
+            else k_trace_lean<false><<<blocks, t.block_threads, 0, st>>>(ta);
         } else if (t.leaf_coop) {
             if (r.count_work) k_trace_batch<true, true><<<blocks, t.block_threads, smem, st>>>(ta);
             else k_trace_batch<false, true><<<blocks, t.block_threads, smem, st>>>(ta);
