@@ -50,23 +50,6 @@ def parse():
     return ap.parse_args()
 
 
-def observer_rapidities(seed: int, rank: int, n: int, first):
-    """Rapidities of a rank's observers: the workload's own observer first, then seeded draws
-    uniform in the ball |phi| <= 2."""
-    rng = np.random.default_rng(seed * 7919 + rank)
-    out = []
-    for i in range(n):
-        if rank == 0 and i == 0:
-            out.append(tuple(float(x) for x in first))
-            continue
-        while True:
-            v = rng.uniform(-1.0, 1.0, 3)
-            if v @ v < 1.0:
-                break
-        out.append(tuple(float(2.0 * x) for x in v))
-    return out
-
-
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -206,6 +189,7 @@ def run_reference(args, rank, world):
 def run_engine(args, rank, world, local):
     import torch
     import specrel_b200 as sr
+    from specrel_b200 import shard
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -221,7 +205,7 @@ def run_engine(args, rank, world, local):
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
     B = args.batch
-    raps = observer_rapidities(args.seed, rank, B, scene.info.cam_rapidity)
+    raps = shard.observer_rapidities(args.seed, rank, B, scene.info.cam_rapidity)
     cams = [sr.camera(rapidity=r) for r in raps]
     us = [sr.uniforms(c, W, H, 0, 1, 0, num_nodes=scene.num_nodes, light_pos=scene.light_pos) for c in cams]
     c64 = [sr.cam64((0.0, 0.0, 0.0, 0.0), r) for r in raps]
@@ -233,11 +217,7 @@ def run_engine(args, rank, world, local):
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return shard.max_over_ranks(x, dist, f"cuda:{local}")
 
     with torch.cuda.stream(stream):
         # Launch parameters for this scene, untimed.
@@ -323,7 +303,7 @@ def run_engine(args, rank, world, local):
         eng.close()
         return
 
-    total_rays = B * RAYS_PER_FRAME * world
+    total_rays = shard.total_rays(B * RAYS_PER_FRAME, world)
     value = total_rays / (ms_max / 1e3) / 1e6
     plain_value = total_rays / (plain_ms / 1e3) / 1e6
     e2e_value = total_rays / (e2e_ms / 1e3) / 1e6

@@ -1,0 +1,67 @@
+"""The multi-GPU host logic on CPU: two gloo ranks on 127.0.0.1 shard the observers as bench.py does
+(one seeded stream per rank, no observer on two ranks) and reduce the timing as the max over ranks.
+The render path itself has no collective, so nothing else crosses ranks."""
+import datetime
+import os
+import socket
+
+import pytest
+
+WORLD = 2
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=WORLD, timeout=datetime.timedelta(seconds=60))
+    try:
+        from specrel_b200 import shard
+        raps = shard.observer_rapidities(5, rank, 6, first=(0.1, 0.2, 0.3))
+        gathered = [None] * WORLD
+        dist.all_gather_object(gathered, raps)
+        slowest = shard.max_over_ranks(1.5 + rank, dist)
+        dist.barrier()
+        q.put((rank, gathered, slowest, shard.total_rays(1000, WORLD)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_shard_observers_and_reduce_the_max():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, port, q)) for r in range(WORLD)]
+    for p in procs:
+        p.start()
+    try:
+        results = sorted(q.get(timeout=180) for _ in range(WORLD))
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert all(p.exitcode == 0 for p in procs)
+    (_, g0, m0, n0), (_, g1, m1, n1) = results
+    assert g0 == g1
+    r0, r1 = g0
+    assert r0[0] == (0.1, 0.2, 0.3)
+    assert not set(r0) & set(r1)
+    assert all(sum(x * x for x in phi) <= 4.0 + 1e-12 for phi in r0 + r1)
+    assert m0 == m1 == 2.5
+    assert n0 == n1 == 2000
+
+
+def test_single_process_needs_no_group():
+    from specrel_b200 import shard
+    assert shard.max_over_ranks(3.0) == 3.0
+    a = shard.observer_rapidities(5, 1, 4)
+    assert a == shard.observer_rapidities(5, 1, 4)
+    assert a != shard.observer_rapidities(5, 0, 4)
