@@ -293,7 +293,8 @@ class Engine:
         return s
 
     def render(self, idx: int, u: GpuUniforms, path: int = SR_PATH_FAST, aux: bool = False, hdr: bool = False,
-               timing: bool = False, cam: CameraF64 | None = None, count: bool = False) -> Frame:
+               timing: bool = False, cam: CameraF64 | None = None, count: bool = False,
+               star_brute: bool = False) -> Frame:
         n = u.size[0] * u.size[1]
         fr = Frame(rgb=np.zeros(n, np.uint32))
         out = _lib.Outputs()
@@ -307,6 +308,7 @@ class Engine:
             fr.hdr = np.zeros((n, 4), np.float32)
             out.hdr = fr.hdr.ctypes.data
         flags = (SR_FLAG_TIMING if timing else 0) | (_lib.SR_FLAG_COUNT_WORK if count else 0)
+        flags |= _lib.SR_FLAG_STAR_BRUTE if star_brute else 0
         opts = _lib.RenderOpts(path, flags, C.pointer(cam) if cam is not None else None)
         t = _lib.Timings()
         _check(self.L.sr_render_ex(self.h, idx, C.byref(u), C.byref(opts), C.byref(out), C.byref(t)), self.h,
@@ -332,7 +334,7 @@ class Engine:
 
     def render_batch(self, idx: int, us: list, rgb_ptr: int, rgb_len: int, cams: list | None = None,
                      device_output: bool = True, timing: bool = False, phases: bool = False,
-                     count: bool = False) -> _lib.Timings:
+                     count: bool = False, star_brute: bool = False) -> _lib.Timings:
         """Renders observers `us` into `rgb_ptr` (concatenated frames). `timing` returns the batch's
         device time; `phases` adds per-phase times, `count` the traversal work (both run the launch
         sequence outside its CUDA graph)."""
@@ -342,6 +344,7 @@ class Engine:
         t = _lib.Timings()
         flags = SR_FLAG_DEVICE_OUTPUT if device_output else 0
         flags |= (_lib.SR_FLAG_TIMING if phases else 0) | (_lib.SR_FLAG_COUNT_WORK if count else 0)
+        flags |= _lib.SR_FLAG_STAR_BRUTE if star_brute else 0
         timing = timing or phases or count
         _check(self.L.sr_render_batch(self.h, idx, ua, ca, n, rgb_ptr, rgb_len, flags,
                                       C.byref(t) if timing else None), self.h, "render_batch")

@@ -397,6 +397,7 @@ sr_status sr_render_ex(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const 
         br.tau = f.tau;
         br.count_work = count;
         br.use_graph = !timing && !count;
+        br.star_brute = (flags & SR_FLAG_STAR_BRUTE) != 0;
         br.ev = timing ? ev + 1 : nullptr;
         if (timing) CK(cudaEventRecord(ev[0], sm), "event");
         CK(fast_render_batch(ctx->fast, s.fast, s.tuning, sd, s.anchor, ctx->bb, ctx->counters.as<uint32_t>(), br, sm),
@@ -501,6 +502,7 @@ sr_status sr_render_batch(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, con
         br.cam64 = cam64;
         br.rgb = dev_out ? rgb_out : nullptr;
         br.use_graph = true;
+        br.star_brute = (flags & SR_FLAG_STAR_BRUTE) != 0;
         // Per-phase events and work counting run the sequence outside its graph.
         br.ev = (timings && (flags & SR_FLAG_TIMING)) ? ev + 1 : nullptr;
         br.count_work = timings && (flags & SR_FLAG_COUNT_WORK);

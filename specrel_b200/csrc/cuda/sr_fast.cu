@@ -16,6 +16,7 @@
 // two agree.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cstring>
 
 #include "sr_camera.cuh"
@@ -643,6 +644,7 @@ struct ShadeBatchArgs {
     uint32_t* counters;  // [0] shadow rays, [1] errors
     unsigned long long* work;
     BBConst bb;
+    uint32_t stars_binned;  // observers passing stars_binned_for get their stars from k_star_tiles
 };
 
 // The shadow queries of a pixel's shading: the main light's was traced by the trace kernel (its
@@ -691,7 +693,7 @@ __global__ void __launch_bounds__(256) k_shade_batch(ShadeBatchArgs a) {
     } else {
         color = shade_sky(rd);
     }
-    if (U.mode == 0u && a.s.num_stars > 0u)
+    if (U.mode == 0u && a.s.num_stars > 0u && !(a.stars_binned && stars_binned_for(U, a.s.num_stars)))
         color = add(color, stars_brute(a.s, U, cam, ro, rd, sx, sy, slot != 0xFFFFFFFFu ? h.lambda : INFINITY, a.bb));
     a.hdr[(size_t)od.pyr_base + l] = make_float4(color.x, color.y, color.z, 0.0f);
     if (a.hit_id)
@@ -705,6 +707,7 @@ __global__ void __launch_bounds__(256) k_shade_batch(ShadeBatchArgs a) {
 }  // namespace srk
 
 #include "sr_batch_bloom.cuh"
+#include "sr_stars.cuh"
 
 namespace srk {
 
@@ -719,18 +722,19 @@ uint64_t mix(uint64_t h, uint64_t v) {
 }
 
 struct Shape {
-    uint32_t n = 0, total_tiles = 0, total_px = 0, total_pyr = 0;
+    uint32_t n = 0, total_tiles = 0, total_px = 0, total_pyr = 0, total_star_tiles = 0;
     std::vector<ObsDev> obs;
-    std::vector<uint32_t> pre;  // (SR_BLOOM_LEVELS + 2) rows of n + 1: tiles, then levels 0..6
+    std::vector<uint32_t> pre;  // (SR_BLOOM_LEVELS + 3) rows of n + 1: tiles, levels 0..6, star tiles
 };
 
 Shape make_shape(const BatchRequest& r, const SrTuning& t) {
     Shape s;
     s.n = r.n;
     s.obs.resize(r.n);
-    const uint32_t rows = SR_BLOOM_LEVELS + 2, stride = r.n + 1;
+    // Rows of n + 1: trace tiles, bloom levels 0..6, 16x16 star tiles.
+    const uint32_t rows = SR_BLOOM_LEVELS + 3, stride = r.n + 1;
     s.pre.assign((size_t)rows * stride, 0);
-    uint32_t tiles = 0, px = 0, pyr = 0;
+    uint32_t tiles = 0, px = 0, pyr = 0, star_tiles = 0;
     for (uint32_t i = 0; i < r.n; ++i) {
         ObsDev& o = s.obs[i];
         std::memset(&o, 0, sizeof(o));
@@ -741,6 +745,9 @@ Shape make_shape(const BatchRequest& r, const SrTuning& t) {
         o.pix_base = px;
         o.pyr_base = pyr;
         o.has_cam64 = r.cam64 ? 1u : 0u;
+        o.star_tile_base = star_tiles;
+        s.pre[(size_t)(SR_BLOOM_LEVELS + 2) * stride + i] = star_tiles;
+        star_tiles += ((o.width + STAR_TILE - 1) / STAR_TILE) * ((o.height + STAR_TILE - 1) / STAR_TILE);
         Pyramid p = make_pyramid(o.width, o.height);
         for (int k = 0; k <= SR_BLOOM_LEVELS; ++k) { o.lw[k] = p.w[k]; o.lh[k] = p.h[k]; o.loff[k] = p.off[k]; }
         o.loff[SR_BLOOM_LEVELS + 1] = p.off[SR_BLOOM_LEVELS + 1];
@@ -754,6 +761,8 @@ Shape make_shape(const BatchRequest& r, const SrTuning& t) {
         pyr += p.off[SR_BLOOM_LEVELS + 1];
     }
     s.pre[r.n] = tiles;
+    s.pre[(size_t)(SR_BLOOM_LEVELS + 2) * stride + r.n] = star_tiles;
+    s.total_star_tiles = star_tiles;
     s.total_tiles = tiles;
     s.total_px = px;
     s.total_pyr = pyr;
@@ -784,6 +793,28 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
     if ((e = c.shadow.ensure((size_t)sh.total_px)) != cudaSuccess) return e;  // shadow states
     if ((e = c.hdr.ensure((size_t)sh.total_pyr * sizeof(float4))) != cudaSuccess) return e;
     if ((e = c.sched.ensure(((size_t)c.num_sms + 1) * 4)) != cudaSuccess) return e;
+    bool binned = false;
+    if (!r.star_brute && sd.num_stars > 0)
+        for (uint32_t i = 0; i < n; ++i) binned = binned || stars_binned_for(r.u[i], sd.num_stars);
+    const size_t old_star = c.star_cd.bytes + c.star_rect.bytes + c.star_count.bytes + c.star_list.bytes + c.star_scan.bytes;
+    // Star lists: room for every (observer, star) in 8 tiles; tiles past the room sum every star.
+    const uint32_t list_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(8ull * n * sd.num_stars, 1u << 20), 1u << 30);
+    size_t scan_bytes = 0;
+    if (binned) {
+        const size_t pairs = (size_t)n * sd.num_stars;
+        const size_t tiles = sh.total_star_tiles;
+        cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)tiles, st);
+        if ((e = c.star_cd.ensure(pairs * sizeof(float4))) != cudaSuccess) return e;
+        if ((e = c.star_cu.ensure(pairs * sizeof(float4))) != cudaSuccess) return e;
+        if ((e = c.star_rect.ensure(pairs * sizeof(uint4))) != cudaSuccess) return e;
+        if ((e = c.star_count.ensure(tiles * 4)) != cudaSuccess) return e;
+        if ((e = c.star_offset.ensure(tiles * 4)) != cudaSuccess) return e;
+        if ((e = c.star_fill.ensure(tiles * 4)) != cudaSuccess) return e;
+        if ((e = c.star_list.ensure((size_t)list_cap * 4)) != cudaSuccess) return e;
+        if ((e = c.star_scan.ensure(scan_bytes)) != cudaSuccess) return e;
+    }
+    if (c.star_cd.bytes + c.star_rect.bytes + c.star_count.bytes + c.star_list.bytes + c.star_scan.bytes != old_star)
+        fast_release(c);
     if (!r.rgb && (e = c.rgb.ensure((size_t)sh.total_px * 4)) != cudaSuccess) return e;
     if ((e = c.hU.ensure(n * sizeof(SrGpuUniforms))) != cudaSuccess) return e;
     if ((e = c.hcam64.ensure(n * sizeof(SrCameraF64))) != cudaSuccess) return e;
@@ -884,14 +915,60 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
         sa.counters = counters;
         sa.work = work;
         sa.bb = bb;
+        sa.stars_binned = binned ? 1u : 0u;
         uint32_t gpx = (sh.total_px + 255) / 256;
         if (r.count_work) k_shade_batch<true><<<gpx, 256, 0, st>>>(sa);
         else k_shade_batch<false><<<gpx, 256, 0, st>>>(sa);
         if ((x = cudaGetLastError()) != cudaSuccess) return x;
-        if (timed) {
-            cudaEventRecord(r.ev[2], st);
-            cudaEventRecord(r.ev[3], st);
+        if (timed) cudaEventRecord(r.ev[2], st);
+        if (binned) {
+            const size_t tiles = sh.total_star_tiles;
+            if ((x = cudaMemsetAsync(c.star_count.p, 0, tiles * 4, st)) != cudaSuccess) return x;
+            if ((x = cudaMemsetAsync(c.star_fill.p, 0, tiles * 4, st)) != cudaSuccess) return x;
+            StarBinArgs ba;
+            ba.U = sa.U;
+            ba.cam = sa.cam;
+            ba.obs = sa.obs;
+            ba.stars = sd.stars;
+            ba.n = n;
+            ba.num_stars = sd.num_stars;
+            ba.cd = c.star_cd.as<float4>();
+            ba.cu = c.star_cu.as<float4>();
+            ba.rect = c.star_rect.as<uint4>();
+            ba.count = c.star_count.as<uint32_t>();
+            ba.offset = c.star_offset.as<uint32_t>();
+            ba.fill = c.star_fill.as<uint32_t>();
+            ba.list = c.star_list.as<uint32_t>();
+            ba.list_cap = list_cap;
+            const uint64_t pairs = (uint64_t)n * sd.num_stars;
+            const uint32_t gb = (uint32_t)((pairs + 255) / 256);
+            k_star_bin<<<gb, 256, 0, st>>>(ba);
+            size_t sb = scan_bytes;
+            if ((x = cub::DeviceScan::ExclusiveSum(c.star_scan.p, sb, ba.count, c.star_offset.as<uint32_t>(), (int)tiles, st)) !=
+                cudaSuccess)
+                return x;
+            k_star_fill<<<gb, 256, 0, st>>>(ba);
+            StarTileArgs ta2;
+            ta2.s = sd;
+            ta2.U = sa.U;
+            ta2.cam = sa.cam;
+            ta2.obs = sa.obs;
+            ta2.star_pre = tile_pre + (size_t)(SR_BLOOM_LEVELS + 2) * stride;
+            ta2.n = n;
+            ta2.hits = sa.hits;
+            ta2.slots = sa.slots;
+            ta2.cd = ba.cd;
+            ta2.cu = ba.cu;
+            ta2.count = ba.count;
+            ta2.offset = ba.offset;
+            ta2.list = ba.list;
+            ta2.list_cap = list_cap;
+            ta2.hdr = sa.hdr;
+            ta2.bb = bb;
+            k_star_tiles<<<(uint32_t)tiles, 256, STAR_SORT_CAP * 4, st>>>(ta2);
+            if ((x = cudaGetLastError()) != cudaSuccess) return x;
         }
+        if (timed) cudaEventRecord(r.ev[3], st);
         for (int k = 1; k <= SR_BLOOM_LEVELS; ++k) {
             const uint32_t* pre = tile_pre + (size_t)(1 + k) * stride;
             uint32_t tot = sh.pre[(size_t)(1 + k) * stride + n];
@@ -925,6 +1002,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
     key = mix(key, ((uint64_t)t.chunk_tiles << 40) | ((uint64_t)t.refill_lanes << 24) | ((uint64_t)t.leaf_batch << 8) |
                        t.leaf_coop);
     key = mix(key, t.home_pct);
+    key = mix(key, binned ? 0x5354ull : 0ull);
     for (auto& o : sh.obs) key = mix(key, ((uint64_t)o.width << 32) | o.height);
     auto it = c.graphs.find(key);
     if (it == c.graphs.end()) {

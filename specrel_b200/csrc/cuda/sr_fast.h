@@ -62,7 +62,7 @@ struct FastScene {
 // Per-observer description of a batch (device copy in BatchCtx::obs).
 struct ObsDev {
     uint32_t width, height, tiles_x, tile_base;
-    uint32_t pix_base, pyr_base, has_cam64, pad;
+    uint32_t pix_base, pyr_base, has_cam64, star_tile_base;  // star_tile_base: first 16x16 star tile
     uint32_t lw[SR_BLOOM_LEVELS + 1], lh[SR_BLOOM_LEVELS + 1];
     uint32_t loff[SR_BLOOM_LEVELS + 2];  // level offsets inside this observer's pyramid
 };
@@ -80,6 +80,9 @@ struct FastCtx {
     // shadow: one byte per pixel, the main light's shadow ray as traced (0 none, 1 clear, 2 occluded)
     // sched: the tile counters of the trace kernel, one per SM band then the shared pool's
     DevMem U, cam64, cam, obs, lvl_pre, hits, slots, shadow, hdr, rgb, sched;
+    // Star binning: per (observer, star) cone events and tile rectangles; per 16x16 tile a count,
+    // a list offset and a fill cursor; the lists; the prefix sum's scratch.
+    DevMem star_cd, star_cu, star_rect, star_count, star_offset, star_fill, star_list, star_scan;
     HostMem hU, hcam64, hobs, hlvl;
     uint32_t cap_obs = 0;
     std::map<uint64_t, GraphEntry> graphs;
@@ -106,7 +109,8 @@ struct BatchRequest {
     float* tau;                   // device, optional
     bool count_work;
     bool use_graph;
-    cudaEvent_t* ev;              // optional: 5 events, after camera, trace, shading, shading again, bloom
+    bool star_brute;              // sum every star per pixel (no binning), as the reference
+    cudaEvent_t* ev;              // optional: 5 events, after camera, trace, shading, stars, bloom
 };
 cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t, const SceneDev& sd,
                               const double anchor[4], const BBConst& bb, uint32_t* counters, const BatchRequest& r,

@@ -48,6 +48,17 @@ constexpr uint32_t ERR_BAD_INDEX = 4u;
 // (the two evaluate the same condition; a mismatch is an internal error).
 constexpr uint32_t ERR_SHADOW_MISMATCH = 8u;
 
+// Star binning of the fast path (sr_stars.cuh): tile side in pixels, and whether an observer's
+// stars are binned. The binning assumes a field of view within a 76-degree
+// half diagonal and pixels finer than 0.042 radians; other observers sum every star per pixel.
+constexpr uint32_t STAR_TILE = 16;
+__host__ __device__ inline bool stars_binned_for(const SrGpuUniforms& U, uint32_t num_stars) {
+    if (U.mode != 0u || num_stars == 0u || U.size[1] == 0u) return false;
+    const float hw = U.half_wh[0], hh = U.half_wh[1];
+    const float pitch = 2.0f * hh / (float)U.size[1];
+    return hw * hw + hh * hh <= 16.0f && 2.4f * pitch <= 0.1f;
+}
+
 // Pyramid geometry of bloom.rs:28-49 for one frame.
 struct Pyramid {
     uint32_t w[SR_BLOOM_LEVELS + 1], h[SR_BLOOM_LEVELS + 1], off[SR_BLOOM_LEVELS + 2];

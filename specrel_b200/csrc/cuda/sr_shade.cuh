@@ -127,15 +127,24 @@ __device__ __forceinline__ void camera_ray(const SrGpuUniforms& U, const Cam& c,
 }
 
 // The star term of a pixel, brute force over every star as star_light does (star.rs:240-286).
-static __device__ __noinline__ F3 stars_brute(const srk::SceneDev& s, const SrGpuUniforms& U, const Cam& cam, float4 o, float4 d,
-                                       float sx, float sy, float lambda_max, const srk::BBConst& bbc) {
+// The pixel's footprint quantities of star_light (star.rs:240-253): the ray's spatial direction n,
+// the footprint spread (RayFootprint::camera_pixel, star.rs:139-146) and the cone sign.
+__device__ __forceinline__ void star_ray(const SrGpuUniforms& U, const Cam& cam, float4 d, float sx, float sy, float4* n,
+                                         float* spread, float* cone) {
     float h = (float)U.size[1];
     float pitch = 2.0f * U.half_wh[1] / h;
     float inv_len = 1.0f / sqrtf(sx * sx + sy * sy + 1.0f);
-    float spread = pitch * inv_len * sqrtf(inv_len);
-    float cone = U.slice_mode == 0u ? -1.0f : (U.slice_mode == 2u ? 1.0f : 0.0f);
+    *spread = pitch * inv_len * sqrtf(inv_len);
+    *cone = U.slice_mode == 0u ? -1.0f : (U.slice_mode == 2u ? 1.0f : 0.0f);
+    *n = sub4(d, mul4(cam.e0, *cone));
+}
+
+static __device__ __noinline__ F3 stars_brute(const srk::SceneDev& s, const SrGpuUniforms& U, const Cam& cam, float4 o, float4 d,
+                                       float sx, float sy, float lambda_max, const srk::BBConst& bbc) {
+    float4 n;
+    float spread, cone;
+    star_ray(U, cam, d, sx, sy, &n, &spread, &cone);
     float4 e0 = cam.e0;
-    float4 n = sub4(d, mul4(e0, cone));
     BB bb{bbc.r5, bbc.g5, bbc.b5, bbc.wr, bbc.wg, bbc.wb};
     const float4* segs = s.stars + s.num_stars;
     F3 total{0.0f, 0.0f, 0.0f};
