@@ -246,6 +246,29 @@ sr_status sr_render_batch(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* 
                           uint32_t n_observers, uint32_t* rgb_out, uint64_t rgb_len, uint32_t flags,
                           SrTimings* timings);
 
+/* ---- Gradient with respect to the observer ------------------------------------------------
+ * New (the reference renders forward only). For one observer on the past light cone (mode 0,
+ * slice mode 0, no flashes, no haze) on the fast path:
+ *   loss = sum over pixels and r, g, b of (P(HDR) - P(target))^2 on the linear pre-bloom HDR
+ *          image, P = `level` (0..6) halvings by 2x2 box averages (0: the image itself; the
+ *          coarser levels widen the basin for a coarse-to-fine descent)
+ *   grad = d loss / d (rapidity x, y, z, event t, x, y, z) of the FP64 observer `cam`
+ * The forward frame's discrete outcomes (hit tetrahedra, shadow tests, textures, sky grid lines,
+ * star segments and footprint cuts) are held fixed; everything smooth is differentiated in
+ * forward mode in f32 with f64 accumulation. `target_hdr` is a device buffer of width*height*4
+ * floats (r, g, b, unused), the layout of SrOutputs.hdr. */
+typedef struct SrAdjointResult {
+    double loss;
+    double grad[7];
+    double primal_mismatch;  /* pixels whose recomputed value differs from the forward frame (0 expected) */
+    double star_terms;       /* (pixel, star) footprint terms differentiated */
+} SrAdjointResult;
+#define SR_ADJ_FROZEN 1u  /* only the loss at `cam`, under the discrete outcomes of the previous
+                             gradient call (same scene and frame size, no frame rendered in between):
+                             a smooth function of theta for checking the gradient by differences */
+sr_status sr_adjoint(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, const SrCameraF64* cam,
+                     const float* target_hdr, uint32_t level, uint32_t flags, SrAdjointResult* out);
+
 /* ---- Rendering without device allocation -------------------------------------------------
  * No counterpart in the reference: an entry point for callers that cannot call cudaMalloc while
  * they render, for instance an application whose own allocator owns all device memory under a fixed

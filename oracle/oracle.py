@@ -96,6 +96,12 @@ def lib():
         L.orc_tetrad.argtypes = [C.POINTER(Camera), C.c_int, C.POINTER(C.c_double)]
         L.orc_gamma_lut.argtypes = [C.c_void_p]
         L.orc_bloom_pack.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
+        L.orc_frozen_new.restype = C.c_void_p
+        L.orc_frozen_new.argtypes = [C.c_void_p, C.POINTER(Camera), C.POINTER(Config), C.c_int]
+        L.orc_frozen_free.argtypes = [C.c_void_p]
+        L.orc_frozen_loss.restype = C.c_double
+        L.orc_frozen_loss.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Camera), C.POINTER(Config), C.c_void_p,
+                                      C.c_uint32, C.c_int, C.c_void_p]
         _lib = L
     return _lib
 
@@ -309,3 +315,28 @@ def bloom_pack(hdr3: np.ndarray, w: int, h: int):
     bloomed = np.zeros(w * h * 3, np.float32)
     lib().orc_bloom_pack(src.ctypes.data, w, h, rgb.ctypes.data, bloomed.ctypes.data)
     return rgb, bloomed.reshape(-1, 3)
+
+
+class Frozen:
+    """The frame's discrete outcomes at one observer (hits, shadows, textures, sky grid lines, the
+    stars passing the footprint cut), for evaluating the image loss at nearby observers with them
+    held fixed: the FP64 reference for the engine's gradient (shaded, past light cone)."""
+
+    def __init__(self, scene: Scene, camera: Camera, cfg: Config, threads: int = 0):
+        self.scene, self.cfg = scene, cfg
+        self.h = lib().orc_frozen_new(scene.h, C.byref(camera), C.byref(cfg), threads or (os.cpu_count() or 1))
+        if not self.h:
+            raise RuntimeError("orc_frozen_new: only shaded past-light-cone frames")
+
+    def __del__(self):
+        if getattr(self, "h", None) and lib is not None:
+            lib().orc_frozen_free(self.h)
+            self.h = None
+
+    def loss(self, camera: Camera, target: np.ndarray, level: int = 0, threads: int = 0, hdr: bool = False):
+        """sum((P(HDR) - P(target))^2), P = `level` 2x2-box halvings; target: (w*h, 3) float64."""
+        t = np.ascontiguousarray(target, np.float64).reshape(-1)
+        out = np.zeros(t.size, np.float64) if hdr else None
+        L = lib().orc_frozen_loss(self.scene.h, self.h, C.byref(camera), C.byref(self.cfg), t.ctypes.data, level,
+                                  threads or (os.cpu_count() or 1), out.ctypes.data if hdr else None)
+        return (L, out.reshape(-1, 3)) if hdr else L

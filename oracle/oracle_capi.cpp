@@ -3,6 +3,7 @@
 #include <cstring>
 #include <memory>
 
+#include "oracle_grad.hpp"
 #include "oracle_scenes.hpp"
 
 using namespace orc;
@@ -353,6 +354,90 @@ int orc_bloom_pack(const float* hdr3, uint32_t w, uint32_t h, uint32_t* rgb, flo
         if (bloomed3) { bloomed3[3 * i] = img[i].x; bloomed3[3 * i + 1] = img[i].y; bloomed3[3 * i + 2] = img[i].z; }
     }
     return 0;
+}
+
+}  // extern "C"
+
+// ---- The frozen-outcome image loss (oracle_grad.hpp), FP64 reference of the engine's gradient ----
+namespace {
+template <class T> Camera4D<T> camera_of(const OrcCamera* c) {
+    Camera4D<T> cam;
+    cam.position = V4<T>((T)c->pos[0], (T)c->pos[1], (T)c->pos[2], (T)c->pos[3]);
+    cam.tetrad = make_tetrad<T>(*c);
+    cam.proper_time = (T)c->proper_time;
+    cam.fov_y_rad = (T)c->fov_deg * (C<T>::PI / T(180));
+    return cam;
+}
+RenderConfig config_of(const OrcConfig* cf) {
+    RenderConfig cfg;
+    cfg.width = cf->width;
+    cfg.height = cf->height;
+    cfg.mode = (RenderMode)cf->mode;
+    cfg.shadow_mode = (ShadowMode)cf->shadow_mode;
+    cfg.slice_mode = (ViewMode)cf->slice_mode;
+    cfg.prophecy_delta = cf->prophecy_delta;
+    return cfg;
+}
+struct FrozenBox {
+    bool fp64;
+    FrozenFrame<float> f;
+    FrozenFrame<double> d;
+};
+template <class T>
+double frozen_loss_t(const Scene<T>& scene, const FrozenFrame<T>& F, const OrcCamera* c, const OrcConfig* cf,
+                     const double* target, uint32_t level, unsigned threads, double* hdr_out) {
+    Camera4D<T> cam = camera_of<T>(c);
+    RenderConfig cfg = config_of(cf);
+    FrameDynamics<T> dyn;
+    Renderer<T> R{scene, cam, cfg, dyn};
+    std::vector<V3<T>> img = frozen_hdr(R, F, threads);
+    std::vector<V3<T>> tgt(img.size());
+    for (size_t i = 0; i < img.size(); ++i) tgt[i] = V3<T>((T)target[3 * i], (T)target[3 * i + 1], (T)target[3 * i + 2]);
+    if (hdr_out)
+        for (size_t i = 0; i < img.size(); ++i) {
+            hdr_out[3 * i] = (double)img[i].x;
+            hdr_out[3 * i + 1] = (double)img[i].y;
+            hdr_out[3 * i + 2] = (double)img[i].z;
+        }
+    return pyramid_loss(img, tgt, F.w, F.h, level);
+}
+}  // namespace
+
+extern "C" {
+
+// Records the discrete outcomes of the frame (shaded, past light cone, no flashes or haze).
+void* orc_frozen_new(void* s, const OrcCamera* c, const OrcConfig* cf, int threads) {
+    auto* b = (SceneBox*)s;
+    if (!cf || cf->mode != 0 || cf->slice_mode != 0 || cf->width == 0 || cf->height == 0) return nullptr;
+    auto* fb = new FrozenBox();
+    fb->fp64 = b->fp64;
+    RenderConfig cfg = config_of(cf);
+    unsigned th = threads <= 0 ? 1u : (unsigned)threads;
+    if (b->fp64) {
+        Camera4D<double> cam = camera_of<double>(c);
+        FrameDynamics<double> dyn;
+        Renderer<double> R{b->d->scene, cam, cfg, dyn};
+        fb->d = freeze(R, th);
+    } else {
+        Camera4D<float> cam = camera_of<float>(c);
+        FrameDynamics<float> dyn;
+        Renderer<float> R{b->f->scene, cam, cfg, dyn};
+        fb->f = freeze(R, th);
+    }
+    return fb;
+}
+
+void orc_frozen_free(void* f) { delete (FrozenBox*)f; }
+
+// sum((P(HDR) - P(target))^2) at camera `c` under the recorded outcomes; P: `level` 2x2-box
+// halvings; target: width*height*3 doubles; hdr_out (optional): the HDR image, width*height*3.
+double orc_frozen_loss(void* s, void* f, const OrcCamera* c, const OrcConfig* cf, const double* target, uint32_t level,
+                       int threads, double* hdr_out) {
+    auto* b = (SceneBox*)s;
+    auto* fb = (FrozenBox*)f;
+    unsigned th = threads <= 0 ? 1u : (unsigned)threads;
+    if (b->fp64) return frozen_loss_t(b->d->scene, fb->d, c, cf, target, level, th, hdr_out);
+    return frozen_loss_t(b->f->scene, fb->f, c, cf, target, level, th, hdr_out);
 }
 
 }  // extern "C"

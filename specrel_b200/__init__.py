@@ -350,6 +350,17 @@ class Engine:
                                       C.byref(t) if timing else None), self.h, "render_batch")
         return t
 
+    def adjoint(self, idx: int, u: GpuUniforms, cam: CameraF64, target_hdr_ptr: int, level: int = 0,
+                frozen: bool = False) -> _lib.AdjointResult:
+        """Loss sum((P(HDR) - P(target))^2) of the observer `cam` (P: `level` 2x2 box halvings) and
+        its gradient with respect to (rapidity x, y, z, event t, x, y, z); `target_hdr_ptr`: device,
+        width*height*4 floats. `frozen`: the loss only, under the previous call's discrete outcomes."""
+        r = _lib.AdjointResult()
+        flags = _lib.SR_ADJ_FROZEN if frozen else 0
+        _check(self.L.sr_adjoint(self.h, idx, C.byref(u), C.byref(cam), target_hdr_ptr, level, flags, C.byref(r)),
+               self.h, "adjoint")
+        return r
+
     def tuning(self, idx: int) -> _lib.Tuning:
         t = _lib.Tuning()
         _check(self.L.sr_get_tuning(self.h, idx, C.byref(t)), self.h, "get_tuning")

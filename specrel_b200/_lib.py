@@ -32,6 +32,7 @@ SR_FLAG_DEVICE_OUTPUT = 2
 SR_FLAG_STAR_BRUTE = 4
 SR_FLAG_COUNT_WORK = 8
 SR_NOALLOC_SCRATCH_BYTES = 8 << 20
+SR_ADJ_FROZEN = 1
 SR_NOALLOC_MAX_PIXELS = 1 << 18
 
 # ---- packed layouts (gpu.rs:44-144) ------------------------------------------------------------
@@ -93,6 +94,11 @@ class SceneStats(C.Structure):
     _fields_ = [("num_nodes", C.c_uint32), ("num_prims", C.c_uint32), ("num_stars", C.c_uint32),
                 ("bvh_depth", C.c_uint32), ("device_bytes", C.c_uint64), ("fast_nodes", C.c_uint32),
                 ("pad", C.c_uint32)]
+
+
+class AdjointResult(C.Structure):
+    _fields_ = [("loss", C.c_double), ("grad", C.c_double * 7), ("primal_mismatch", C.c_double),
+                ("star_terms", C.c_double)]
 
 
 class Tuning(C.Structure):
@@ -162,6 +168,8 @@ SIGNATURES = {
                                  C.POINTER(Outputs), C.POINTER(Timings)]),
     "sr_render_batch": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64),
                                     C.c_uint32, C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(Timings)]),
+    "sr_adjoint": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64), C.c_void_p,
+                               C.c_uint32, C.c_uint32, C.POINTER(AdjointResult)]),
     "sr_render_noalloc": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64), C.c_void_p]),
     "sr_get_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),
     "sr_set_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),

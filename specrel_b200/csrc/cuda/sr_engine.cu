@@ -601,6 +601,40 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
     return SR_OK;
 }
 
+sr_status sr_adjoint(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const SrCameraF64* cam, const float* target_hdr,
+                     uint32_t level, uint32_t flags, SrAdjointResult* out) {
+    if (!ctx || !u || !cam || !target_hdr || !out) return SR_ERR_INVALID_ARGUMENT;
+    if (level > SR_BLOOM_LEVELS) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "loss level must be 0..6");
+    if (idx >= ctx->scenes.size() || !ctx->scenes[idx] || !ctx->scenes[idx]->present)
+        return fail(ctx, SR_ERR_NO_SCENE, "scene " + std::to_string(idx) + " is not uploaded");
+    if (u->size[0] == 0 || u->size[1] == 0 || (uint64_t)u->size[0] * u->size[1] > (1ull << 28))
+        return fail(ctx, SR_ERR_INVALID_ARGUMENT, "frame size must be non-zero and at most 2^28 pixels");
+    if (u->mode != 0 || u->slice_mode != 0 || u->num_flashes != 0 || u->num_haze != 0 || u->shadow_mode > 2)
+        return fail(ctx, SR_ERR_UNSUPPORTED, "the gradient covers shaded past-light-cone frames without flashes or haze");
+    SceneSlot& s = *ctx->scenes[idx];
+    if (!s.fast.usable) return fail(ctx, SR_ERR_UNSUPPORTED, "the gradient needs a scene the fast path takes");
+    if (s.num_stars > 0 && !stars_binned_for(*u, s.num_stars))
+        return fail(ctx, SR_ERR_UNSUPPORTED, "the gradient needs binned stars (field of view and pixel size of stars_binned_for)");
+    CK(cudaSetDevice(ctx->device), "set device");
+    const bool frozen = (flags & SR_ADJ_FROZEN) != 0;
+    if (frozen && (!ctx->fast.adj_valid || ctx->fast.adj_w != u->size[0] || ctx->fast.adj_h != u->size[1] ||
+                   ctx->fast.adj_geoms != scene_dev(ctx, s).geoms))
+        return fail(ctx, SR_ERR_INVALID_ARGUMENT, "a frozen evaluation needs a gradient call on this scene and frame size just before");
+    double r[10];
+    CK(fast_adjoint(ctx->fast, s.fast, s.tuning, scene_dev(ctx, s), s.anchor, ctx->bb, ctx->counters.as<uint32_t>(), *u, *cam,
+                    target_hdr, level, frozen, r, ctx->stream),
+       "gradient");
+    uint32_t counters[4] = {0, 0, 0, 0};
+    CK(cudaMemcpy(counters, ctx->counters.p, 16, cudaMemcpyDeviceToHost), "counters");
+    if (counters[1] & ERR_TRAVERSAL_LIMIT) return fail(ctx, SR_ERR_TRAVERSAL_LIMIT, "a ray exceeded the traversal visit limit");
+    if (counters[1]) return fail(ctx, SR_ERR_BAD_SCENE, "device reported a bad index (flags " + std::to_string(counters[1]) + ")");
+    out->loss = r[0];
+    for (int k = 0; k < 7; ++k) out->grad[k] = r[1 + k];
+    out->primal_mismatch = r[8];
+    out->star_terms = r[9];
+    return SR_OK;
+}
+
 // ---------------------------------------------------------------------------------------------
 // sr_render_noalloc: the plain path with all of its scratch in one static device array.
 // ---------------------------------------------------------------------------------------------

@@ -708,6 +708,7 @@ __global__ void __launch_bounds__(256) k_shade_batch(ShadeBatchArgs a) {
 
 #include "sr_batch_bloom.cuh"
 #include "sr_stars.cuh"
+#include "sr_adjoint.cuh"
 
 namespace srk {
 
@@ -777,6 +778,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
                               const double anchor[4], const BBConst& bb, uint32_t* counters, const BatchRequest& r,
                               cudaStream_t st) {
     if (r.n == 0) return cudaSuccess;
+    c.adj_valid = false;  // the batch buffers the gradient's outcomes live in are about to change
     Shape sh = make_shape(r, t);
     const uint32_t n = r.n, stride = n + 1;
     if ((uint64_t)sh.total_tiles * 32 >= (1ull << 32)) return cudaErrorInvalidValue;
@@ -1024,6 +1026,133 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
         it = c.graphs.emplace(key, g).first;
     }
     return cudaGraphLaunch(it->second.exec, st);
+}
+
+// ---------------------------------------------------------------------------------------------
+// The gradient of the image loss (sr_adjoint.cuh).
+// ---------------------------------------------------------------------------------------------
+cudaError_t fast_adjoint(FastCtx& c, const FastScene& s, const SrTuning& t, const SceneDev& sd, const double anchor[4],
+                         const BBConst& bb, uint32_t* counters, const SrGpuUniforms& u, const SrCameraF64& cam,
+                         const float* target, uint32_t level, bool frozen, double out[10], cudaStream_t st) {
+    const uint32_t W = u.size[0], H = u.size[1];
+    cudaError_t e;
+    if (frozen) {
+        if (!c.adj_valid || c.adj_w != W || c.adj_h != H || c.adj_geoms != sd.geoms) return cudaErrorInvalidValue;
+    } else {
+        // The forward frame: hits, shadow results, star lists and the HDR image the loss compares.
+        BatchRequest br{};
+        br.n = 1;
+        br.u = &u;
+        br.cam64 = &cam;
+        br.use_graph = false;
+        c.adj_valid = false;
+        if ((e = fast_render_batch(c, s, t, sd, anchor, bb, counters, br, st)) != cudaSuccess) return e;
+    }
+    const uint32_t tx16 = (W + STAR_TILE - 1) / STAR_TILE, ty16 = (H + STAR_TILE - 1) / STAR_TILE;
+    const uint32_t tiles = tx16 * ty16;
+    const bool stars_on = sd.num_stars > 0 && stars_binned_for(u, sd.num_stars);
+    // Pyramid geometry of the loss levels 0..level.
+    uint32_t lw[8], lh[8];
+    size_t loff[9];
+    lw[0] = W;
+    lh[0] = H;
+    loff[0] = 0;
+    for (uint32_t k = 1; k <= level; ++k) {
+        lw[k] = (lw[k - 1] + 1) / 2;
+        lh[k] = (lh[k - 1] + 1) / 2;
+    }
+    for (uint32_t k = 0; k <= level; ++k) loff[k + 1] = loff[k] + (size_t)lw[k] * lh[k];
+    const size_t npx = (size_t)W * H;
+    const uint32_t rblocks = (uint32_t)((npx + 255) / 256);
+    const size_t list_cap = stars_on ? c.star_list.bytes / 4 : 0;
+    if ((e = c.adj_cam.ensure(sizeof(DCam))) != cudaSuccess) return e;
+    if ((e = c.adj_partials.ensure((size_t)std::max(tiles, rblocks) * ADJ_SLOTS * sizeof(double))) != cudaSuccess) return e;
+    if ((e = c.adj_out.ensure(2 * ADJ_SLOTS * sizeof(double))) != cudaSuccess) return e;
+    if ((e = c.adj_pyr.ensure(2 * loff[level + 1] * sizeof(float4))) != cudaSuccess) return e;
+    if ((e = c.adj_weight.ensure(2 * npx * 3 * sizeof(double))) != cudaSuccess) return e;
+    if ((e = c.adj_grid.ensure(npx)) != cudaSuccess) return e;
+    if ((e = c.adj_hdr.ensure(npx * sizeof(float4))) != cudaSuccess) return e;
+    if (stars_on && (e = c.adj_stars.ensure((size_t)sd.num_stars * sizeof(DF4))) != cudaSuccess) return e;
+    if (stars_on && (e = c.adj_pass.ensure(list_cap * 32)) != cudaSuccess) return e;
+    float4* pyr = c.adj_pyr.as<float4>();  // image levels 0..level
+    float4* tpyr = pyr + loff[level + 1];  // target levels 0..level
+    double* g0 = c.adj_weight.as<double>();
+    double* g1 = g0 + npx * 3;
+    const dim3 b2(16, 16);
+    // The loss at the chosen level of `image` against the target, and (gradient mode) its weights
+    // on the full image.
+    auto loss_pass = [&](const void* image) -> cudaError_t {
+        cudaError_t x;
+        if ((x = cudaMemcpyAsync(pyr, image, npx * sizeof(float4), cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return x;
+        if ((x = cudaMemcpyAsync(tpyr, target, npx * sizeof(float4), cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return x;
+        for (uint32_t k = 1; k <= level; ++k) {
+            const dim3 g2((lw[k] + 15) / 16, (lh[k] + 15) / 16);
+            k_adj_down<<<g2, b2, 0, st>>>(pyr + loff[k - 1], lw[k - 1], lh[k - 1], pyr + loff[k], lw[k], lh[k]);
+            k_adj_down<<<g2, b2, 0, st>>>(tpyr + loff[k - 1], lw[k - 1], lh[k - 1], tpyr + loff[k], lw[k], lh[k]);
+        }
+        const size_t nl = (size_t)lw[level] * lh[level];
+        double* gl = (level % 2 == 0) ? g0 : g1;  // ends in g0 after `level` transposes
+        const uint32_t lblocks = (uint32_t)((nl + 255) / 256);
+        k_adj_residual<<<lblocks, 256, 0, st>>>(pyr + loff[level], tpyr + loff[level], (uint32_t)nl, gl,
+                                                 c.adj_partials.as<double>());
+        k_adjoint_reduce<<<1, 256, 0, st>>>(c.adj_partials.as<double>(), lblocks, c.adj_out.as<double>() + ADJ_SLOTS);
+        for (uint32_t k = level; k >= 1; --k) {
+            double* src = (k % 2 == 0) ? g0 : g1;
+            double* dst = (k % 2 == 0) ? g1 : g0;
+            const dim3 g2((lw[k - 1] + 15) / 16, (lh[k - 1] + 15) / 16);
+            k_adj_up<<<g2, b2, 0, st>>>(src, lw[k], lh[k], dst, lw[k - 1], lh[k - 1]);
+        }
+        return cudaGetLastError();
+    };
+    if (!frozen) {
+        if ((e = loss_pass(c.hdr.p)) != cudaSuccess) return e;
+        if (stars_on && (e = cudaMemsetAsync(c.adj_pass.p, 0, list_cap * 32, st)) != cudaSuccess) return e;
+    }
+    // The duals of the camera and of the stars' cone events, then the pixels.
+    k_adjoint_camera<<<1, 1, 0, st>>>(cam, anchor[0], anchor[1], anchor[2], anchor[3], c.adj_cam.as<DCam>());
+    if (stars_on)
+        k_adjoint_stars<<<(sd.num_stars + 127) / 128, 128, 0, st>>>(sd.stars, sd.num_stars, c.adj_cam.as<DCam>(),
+                                                                  c.adj_stars.as<DF4>());
+    AdjointArgs a;
+    a.s = sd;
+    a.U = c.U.as<SrGpuUniforms>();
+    a.obs = c.obs.as<ObsDev>();
+    a.star_pre = nullptr;
+    a.dcam = c.adj_cam.as<DCam>();
+    a.hits = c.hits.as<float4>();
+    a.slots = c.slots.as<uint32_t>();
+    a.shadow = c.shadow.as<uint8_t>();
+    a.star_dcd = stars_on ? c.adj_stars.as<DF4>() : nullptr;
+    a.star_cu = stars_on ? c.star_cu.as<float4>() : nullptr;
+    a.count = stars_on ? c.star_count.as<uint32_t>() : nullptr;
+    a.offset = stars_on ? c.star_offset.as<uint32_t>() : nullptr;
+    a.list = stars_on ? c.star_list.as<uint32_t>() : nullptr;
+    a.list_cap = (uint32_t)list_cap;
+    a.stars_on = stars_on ? 1u : 0u;
+    a.hdr_fwd = c.hdr.as<float4>();
+    a.weight = g0;
+    a.partials = c.adj_partials.as<double>();
+    a.bb = bb;
+    a.grid = c.adj_grid.as<uint8_t>();
+    a.pass = stars_on ? c.adj_pass.as<uint32_t>() : nullptr;
+    a.frozen = frozen ? 1u : 0u;
+    a.hdr_out = c.adj_hdr.as<float4>();
+    k_adjoint_pixels<<<tiles, 256, STAR_SORT_CAP * 4, st>>>(a);
+    k_adjoint_reduce<<<1, 256, 0, st>>>(a.partials, tiles, c.adj_out.as<double>());
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (frozen && (e = loss_pass(c.adj_hdr.p)) != cudaSuccess) return e;
+    double both[2 * ADJ_SLOTS];
+    if ((e = cudaMemcpyAsync(both, c.adj_out.p, sizeof(both), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    for (int k = 0; k < ADJ_SLOTS; ++k) out[k] = frozen ? 0.0 : both[k];
+    out[0] = both[ADJ_SLOTS];  // the loss, from the residual pass
+    if (!frozen) {
+        c.adj_valid = true;
+        c.adj_w = W;
+        c.adj_h = H;
+        c.adj_geoms = sd.geoms;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace srk

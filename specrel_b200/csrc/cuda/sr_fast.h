@@ -83,6 +83,13 @@ struct FastCtx {
     // Star binning: per (observer, star) cone events and tile rectangles; per 16x16 tile a count,
     // a list offset and a fill cursor; the lists; the prefix sum's scratch.
     DevMem star_cd, star_cu, star_rect, star_count, star_offset, star_fill, star_list, star_scan;
+    // Gradient: the camera and the stars' cone events as duals, per-block partial sums, the result.
+    DevMem adj_cam, adj_stars, adj_partials, adj_out, adj_pyr, adj_weight, adj_grid, adj_pass, adj_hdr;
+    // The outcomes of the last gradient call (hits, shadows, star lists, grid lines, cut passes)
+    // stay valid for frozen evaluations while no other frame is rendered.
+    bool adj_valid = false;
+    uint32_t adj_w = 0, adj_h = 0;
+    const float4* adj_geoms = nullptr;
     HostMem hU, hcam64, hobs, hlvl;
     uint32_t cap_obs = 0;
     std::map<uint64_t, GraphEntry> graphs;
@@ -115,6 +122,14 @@ struct BatchRequest {
 cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t, const SceneDev& sd,
                               const double anchor[4], const BBConst& bb, uint32_t* counters, const BatchRequest& r,
                               cudaStream_t st);
+// The gradient of sum((P_level(HDR) - P_level(target))^2) with respect to (rapidity, event) of one
+// observer (see sr_adjoint.cuh). `target`: device, W*H*4 floats. out: loss, grad[7], primal
+// mismatches (pixels whose dual value differs from the forward frame, or whose star list was not
+// sortable), star terms. `frozen`: only the loss at `cam` under the last gradient call's discrete
+// outcomes (no forward frame; the finite-difference check of the gradient).
+cudaError_t fast_adjoint(FastCtx& c, const FastScene& s, const SrTuning& t, const SceneDev& sd, const double anchor[4],
+                         const BBConst& bb, uint32_t* counters, const SrGpuUniforms& u, const SrCameraF64& cam,
+                         const float* target, uint32_t level, bool frozen, double out[10], cudaStream_t st);
 // The device HDR image (level 0) of observer `i` of the last batch, for side outputs.
 float4* fast_batch_hdr(FastCtx& c, uint32_t pix_base_of_obs);
 
