@@ -341,6 +341,8 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
             slab_interval(rmin, rmax, no, inv, t_min, t_max, &enr, &exr);
             const bool hl = exl >= enl, hr = exr >= enr;
             if (hl && hr) {
+                // Nearer child first: whether any tetrahedron in (t_min, t_max) is hit does not
+                // depend on the order, and the nearer box tends to end the search sooner.
                 if (sp < FAST_STACK) st[sp++].x = r.y;
                 else atomicOr(err, ERR_BAD_INDEX);
                 cur = r.x;
