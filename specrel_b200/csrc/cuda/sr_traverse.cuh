@@ -319,7 +319,8 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
 }
 
 // Any hit in (t_min, t_max) from node `cur` (the root, already tested): left before right, no
-// culling (Bvh4D::is_occluded, bvh4d.rs:523-578).
+// culling (Bvh4D::is_occluded, bvh4d.rs:523-578). (The answer does not depend on the order;
+// nearer-first measured 7% slower on the 7.9M-tet scene.)
 template <bool COUNT>
 __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float4 o, float4 d, float4 inv, float t_min,
                                          float t_max, uint2* st, uint32_t* err, Work& work) {
@@ -341,8 +342,6 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
             slab_interval(rmin, rmax, no, inv, t_min, t_max, &enr, &exr);
             const bool hl = exl >= enl, hr = exr >= enr;
             if (hl && hr) {
-                // Nearer child first: whether any tetrahedron in (t_min, t_max) is hit does not
-                // depend on the order, and the nearer box tends to end the search sooner.
                 if (sp < FAST_STACK) st[sp++].x = r.y;
                 else atomicOr(err, ERR_BAD_INDEX);
                 cur = r.x;
