@@ -140,6 +140,7 @@ class Scene:
         self.params = params
         self.fp64 = fp64
         self.h = _handle if _handle is not None else lib().orc_scene_new(C.byref(params), 1 if fp64 else 0)
+        self._free = lib().orc_scene_free  # held so that freeing works during interpreter exit
         self.info = SceneInfo()
         lib().orc_scene_info(self.h, C.byref(self.info))
 
@@ -156,7 +157,7 @@ class Scene:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().orc_scene_free(self.h)
+            self._free(self.h)
             self.h = None
 
     def pack(self):
@@ -325,12 +326,13 @@ class Frozen:
     def __init__(self, scene: Scene, camera: Camera, cfg: Config, threads: int = 0):
         self.scene, self.cfg = scene, cfg
         self.h = lib().orc_frozen_new(scene.h, C.byref(camera), C.byref(cfg), threads or (os.cpu_count() or 1))
+        self._free = lib().orc_frozen_free
         if not self.h:
             raise RuntimeError("orc_frozen_new: only shaded past-light-cone frames")
 
     def __del__(self):
-        if getattr(self, "h", None) and lib is not None:
-            lib().orc_frozen_free(self.h)
+        if getattr(self, "h", None):
+            self._free(self.h)
             self.h = None
 
     def loss(self, camera: Camera, target: np.ndarray, level: int = 0, threads: int = 0, hdr: bool = False):

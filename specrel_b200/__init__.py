@@ -107,6 +107,7 @@ class SynthScene:
         if st != _lib.SR_OK:
             raise SrError(st, err.value.decode())
         self.h = h
+        self._free = _lib.lib().sr_scene_free  # held so that freeing works during interpreter exit
         self.info = _lib.SynthInfo()
         _lib.lib().sr_scene_info(self.h, C.byref(self.info))
         d = _lib.SceneDesc()
@@ -115,7 +116,7 @@ class SynthScene:
 
     def __del__(self):
         if getattr(self, "h", None):
-            _lib.lib().sr_scene_free(self.h)
+            self._free(self.h)
             self.h = None
 
     def desc(self):

@@ -36,16 +36,27 @@ __global__ void k_wide_flags(const SrGpuNode* nodes, uint32_t n, uint32_t* flags
     if (i < n) flags[i] = nodes[i].count == 0 ? 1u : 0u;
 }
 
-__global__ void k_wide_fill(const SrGpuNode* nodes, uint32_t n, const uint32_t* wid, float4* boxes, uint2* refs) {
+// One wide node: both children's boxes in each of the 16 sign-octant copies (near corner, far
+// corner; see WideScene) and the packed child references.
+__global__ void k_wide_fill(const SrGpuNode* nodes, uint32_t n, const uint32_t* wid, float4* boxes, size_t oct_stride,
+                            uint2* refs) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || nodes[i].count != 0) return;
     const SrGpuNode& nd = nodes[i];
     uint32_t c[2] = {nd.left, nd.right_or_first}, ref[2];
-    float4* b = boxes + 4ull * wid[i];
     for (int k = 0; k < 2; ++k) {
         const SrGpuNode& ch = nodes[c[k]];
-        b[2 * k] = make_float4(ch.min[0], ch.min[1], ch.min[2], ch.min[3]);
-        b[2 * k + 1] = make_float4(ch.max[0], ch.max[1], ch.max[2], ch.max[3]);
+        for (uint32_t oct = 0; oct < 16; ++oct) {
+            float nr[4], fr[4];
+            for (int a = 0; a < 4; ++a) {
+                const bool neg = (oct >> a) & 1u;
+                nr[a] = neg ? ch.max[a] : ch.min[a];
+                fr[a] = neg ? ch.min[a] : ch.max[a];
+            }
+            float4* b = boxes + oct * oct_stride + 4ull * wid[i];
+            b[2 * k] = make_float4(nr[0], nr[1], nr[2], nr[3]);
+            b[2 * k + 1] = make_float4(fr[0], fr[1], fr[2], fr[3]);
+        }
         ref[k] = ch.count > 0 ? pack_leaf(ch.right_or_first, ch.count) : wid[c[k]];
     }
     refs[wid[i]] = make_uint2(ref[0], ref[1]);
@@ -97,9 +108,10 @@ cudaError_t fast_build(FastCtx& c, FastScene& s, const SrGpuNode* nodes, uint32_
     cudaMemcpyAsync(&last[1], flags + n - 1, 4, cudaMemcpyDeviceToHost, st);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
     s.num_wide = last[0] + last[1];
-    if ((e = s.boxes.ensure((size_t)s.num_wide * 64)) != cudaSuccess) return e;
+    if ((e = s.boxes.ensure((size_t)s.num_wide * 64 * 16)) != cudaSuccess) return e;
     if ((e = s.refs.ensure((size_t)s.num_wide * 8)) != cudaSuccess) return e;
-    k_wide_fill<<<(n + 255) / 256, 256, 0, st>>>(nodes, n, wid, s.boxes.as<float4>(), s.refs.as<uint2>());
+    k_wide_fill<<<(n + 255) / 256, 256, 0, st>>>(nodes, n, wid, s.boxes.as<float4>(), 4ull * s.num_wide,
+                                                 s.refs.as<uint2>());
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     e = cudaStreamSynchronize(st);
     s.scratch.ensure(0);
@@ -835,6 +847,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
     uint32_t* rgb = r.rgb ? r.rgb : c.rgb.as<uint32_t>();
     WideScene ws;
     ws.boxes = s.boxes.as<float4>();
+    ws.oct_stride = 4ull * s.num_wide;
     ws.refs = s.refs.as<uint2>();
     ws.geoms = sd.geoms;
     ws.root_min = make_float4(s.root_min[0], s.root_min[1], s.root_min[2], s.root_min[3]);

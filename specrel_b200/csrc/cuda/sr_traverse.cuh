@@ -37,7 +37,12 @@ __host__ __device__ __forceinline__ uint32_t pack_leaf(uint32_t first, uint32_t 
 }
 
 struct WideScene {
-    const float4* boxes;  // 4 float4 per wide node
+    // 16 copies of the child boxes, one per sign octant of the inverse direction (bit i set: the
+    // ray's inv component i is negative). In copy `oct` each child holds its near corner then its
+    // far corner: component i is min[i] for a positive inv[i], max[i] for a negative one. Copy 0
+    // is therefore the plain (min, max) layout. 4 float4 per wide node in each copy.
+    const float4* boxes;
+    size_t oct_stride;    // float4 count of one copy (4 per wide node)
     const uint2* refs;    // packed (left, right)
     const float4* geoms;  // 5 float4 per hot record
     float4 root_min, root_max;
@@ -258,12 +263,35 @@ __device__ __forceinline__ bool intersect_lean(const float4* g, float4 o, float4
     return true;
 }
 
+// The same interval from a box stored near corner first for the ray's sign octant: the near
+// plane's parameter of each axis is then the smaller one (the products keep the order of the
+// sums, rounding being monotonic, since the sign of inv is the octant's), so the per-axis min and
+// max of slab_interval are not needed and the values are the same bit for bit.
+__device__ __forceinline__ void slab_octant(float4 bnear, float4 bfar, float4 no, float4 inv, float t_min, float t_max,
+                                            float* en, float* ex) {
+    const float2 i01 = f2(inv.x, inv.y), i23 = f2(inv.z, inv.w);
+    const float2 a01 = mul2(add2(f2(bnear.x, bnear.y), f2(no.x, no.y)), i01);
+    const float2 a23 = mul2(add2(f2(bnear.z, bnear.w), f2(no.z, no.w)), i23);
+    const float2 b01 = mul2(add2(f2(bfar.x, bfar.y), f2(no.x, no.y)), i01);
+    const float2 b23 = mul2(add2(f2(bfar.z, bfar.w), f2(no.z, no.w)), i23);
+    *en = max3f(max3f(t_min, a01.x, a01.y), a23.x, a23.y);
+    *ex = min3f(min3f(t_max, b01.x, b01.y), b23.x, b23.y);
+}
+
+// The box copy of a ray's sign octant (safe_inv never returns 0, so inv < 0 is the sign).
+__device__ __forceinline__ const float4* octant_boxes(const WideScene& s, float4 inv) {
+    const uint32_t oct = (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u) |
+                         (inv.w < 0.0f ? 8u : 0u);
+    return s.boxes + oct * s.oct_stride;
+}
+
 // Closest hit from node `cur` (the root, already tested against the ray). Returns the slot or
 // -1; `t_max` ends as the closest hit's parameter.
 template <bool COUNT>
 __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, float4 o, float4 d, float4 inv, float t_min,
                                             float& t_max, GeomHit& best, uint2* st, uint32_t* err, Work& work) {
     const float4 no = neg4(o);
+    const float4* ob = octant_boxes(s, inv);
     int slot = -1, sp = 0;
     uint32_t visits = 0;
     for (;;) {
@@ -273,12 +301,12 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
         }
         if (!(cur & REF_LEAF)) {
             if (COUNT) ++work.nodes;
-            const float4* b = s.boxes + 4ull * cur;
-            const float4 lmin = __ldg(b), lmax = __ldg(b + 1), rmin = __ldg(b + 2), rmax = __ldg(b + 3);
+            const float4* b = ob + 4ull * cur;
+            const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
             const uint2 r = __ldg(s.refs + cur);
             float enl, exl, enr, exr;
-            slab_interval(lmin, lmax, no, inv, t_min, t_max, &enl, &exl);
-            slab_interval(rmin, rmax, no, inv, t_min, t_max, &enr, &exr);
+            slab_octant(lnear, lfar, no, inv, t_min, t_max, &enl, &exl);
+            slab_octant(rnear, rfar, no, inv, t_min, t_max, &enr, &exr);
             const bool hl = exl >= enl && enl < t_max;
             const bool hr = exr >= enr && enr < t_max;
             if (hl && hr) {
@@ -325,6 +353,7 @@ template <bool COUNT>
 __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float4 o, float4 d, float4 inv, float t_min,
                                          float t_max, uint2* st, uint32_t* err, Work& work) {
     const float4 no = neg4(o);
+    const float4* ob = octant_boxes(s, inv);
     int sp = 0;
     uint32_t visits = 0;
     for (;;) {
@@ -334,12 +363,12 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
         }
         if (!(cur & REF_LEAF)) {
             if (COUNT) ++work.nodes;
-            const float4* b = s.boxes + 4ull * cur;
-            const float4 lmin = __ldg(b), lmax = __ldg(b + 1), rmin = __ldg(b + 2), rmax = __ldg(b + 3);
+            const float4* b = ob + 4ull * cur;
+            const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
             const uint2 r = __ldg(s.refs + cur);
             float enl, exl, enr, exr;
-            slab_interval(lmin, lmax, no, inv, t_min, t_max, &enl, &exl);
-            slab_interval(rmin, rmax, no, inv, t_min, t_max, &enr, &exr);
+            slab_octant(lnear, lfar, no, inv, t_min, t_max, &enl, &exl);
+            slab_octant(rnear, rfar, no, inv, t_min, t_max, &enr, &exr);
             const bool hl = exl >= enl, hr = exr >= enr;
             if (hl && hr) {
                 if (sp < FAST_STACK) st[sp++].x = r.y;
