@@ -287,6 +287,11 @@ __device__ __forceinline__ const float4* octant_boxes(const WideScene& s, float4
 
 // Closest hit from node `cur` (the root, already tested against the ray). Returns the slot or
 // -1; `t_max` ends as the closest hit's parameter.
+//
+// Loop shape: one iteration is one node visit or one tetrahedron test, so the lanes of a warp at
+// a node advance by a node for each tetrahedron the lanes at a leaf test, instead of waiting for
+// the longest leaf of the warp. Each ray's own sequence of node visits and tests, and so its
+// result, is the same.
 template <bool COUNT>
 __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, float4 o, float4 d, float4 inv, float t_min,
                                             float& t_max, GeomHit& best, uint2* st, uint32_t* err, Work& work) {
@@ -294,12 +299,32 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
     const float4* ob = octant_boxes(s, inv);
     int slot = -1, sp = 0;
     uint32_t visits = 0;
+    uint32_t lk = 0, lend = 0;  // the tetrahedra of the leaf being tested: [lk, lend)
+    // Moves to reference `ref`; a leaf's tetrahedra are tested from the next iteration on (leaves
+    // always hold at least one).
+    auto enter = [&](uint32_t ref) {
+        cur = ref;
+        if (ref & REF_LEAF) {
+            lk = ref & REF_FIRST_MASK;
+            lend = lk + ((ref >> REF_COUNT_SHIFT) & 63u);
+            if (COUNT) { ++work.leaves; work.tets += lend - lk; }
+        }
+    };
+    enter(cur);
     for (;;) {
         if (++visits > MAX_VISITS_FAST) {
             atomicOr(err, ERR_TRAVERSAL_LIMIT);
             break;
         }
-        if (!(cur & REF_LEAF)) {
+        if (lk < lend) {
+            GeomHit gh;
+            if (intersect_lean(s.geoms + 5u * lk, o, no, d, t_min, t_max, &gh)) {
+                t_max = gh.lambda;
+                best = gh;
+                slot = (int)lk;
+            }
+            if (++lk < lend) continue;
+        } else {
             if (COUNT) ++work.nodes;
             const float4* b = ob + 4ull * cur;
             const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
@@ -313,30 +338,19 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
                 const bool ln = enl <= enr;
                 if (sp < FAST_STACK) st[sp++] = ln ? make_uint2(r.y, __float_as_uint(enr)) : make_uint2(r.x, __float_as_uint(enl));
                 else atomicOr(err, ERR_BAD_INDEX);
-                cur = ln ? r.x : r.y;
+                enter(ln ? r.x : r.y);
                 continue;
             }
             if (hl || hr) {
-                cur = hl ? r.x : r.y;
+                enter(hl ? r.x : r.y);
                 continue;
-            }
-        } else {
-            const uint32_t first = cur & REF_FIRST_MASK, cnt = (cur >> REF_COUNT_SHIFT) & 63u;
-            if (COUNT) { ++work.leaves; work.tets += cnt; }
-            for (uint32_t k = first; k < first + cnt; ++k) {
-                GeomHit gh;
-                if (intersect_lean(s.geoms + 5u * k, o, no, d, t_min, t_max, &gh)) {
-                    t_max = gh.lambda;
-                    best = gh;
-                    slot = (int)k;
-                }
             }
         }
         bool found = false;
         while (sp > 0) {
             const uint2 e = st[--sp];
             if (__uint_as_float(e.y) < t_max) {
-                cur = e.x;
+                enter(e.x);
                 found = true;
                 break;
             }
@@ -356,12 +370,27 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
     const float4* ob = octant_boxes(s, inv);
     int sp = 0;
     uint32_t visits = 0;
+    uint32_t lk = 0, lend = 0;  // the tetrahedra of the leaf being tested: [lk, lend)
+    auto enter = [&](uint32_t ref) {
+        cur = ref;
+        if (ref & REF_LEAF) {
+            lk = ref & REF_FIRST_MASK;
+            lend = lk + ((ref >> REF_COUNT_SHIFT) & 63u);
+            if (COUNT) ++work.leaves;
+        }
+    };
+    enter(cur);
     for (;;) {
         if (++visits > MAX_VISITS_FAST) {
             atomicOr(err, ERR_TRAVERSAL_LIMIT);
             return false;
         }
-        if (!(cur & REF_LEAF)) {
+        if (lk < lend) {
+            if (COUNT) ++work.tets;
+            GeomHit gh;
+            if (intersect_lean(s.geoms + 5u * lk, o, no, d, t_min, t_max, &gh)) return true;
+            if (++lk < lend) continue;
+        } else {
             if (COUNT) ++work.nodes;
             const float4* b = ob + 4ull * cur;
             const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
@@ -373,24 +402,16 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
             if (hl && hr) {
                 if (sp < FAST_STACK) st[sp++].x = r.y;
                 else atomicOr(err, ERR_BAD_INDEX);
-                cur = r.x;
+                enter(r.x);
                 continue;
             }
             if (hl || hr) {
-                cur = hl ? r.x : r.y;
+                enter(hl ? r.x : r.y);
                 continue;
-            }
-        } else {
-            const uint32_t first = cur & REF_FIRST_MASK, cnt = (cur >> REF_COUNT_SHIFT) & 63u;
-            if (COUNT) ++work.leaves;
-            for (uint32_t k = first; k < first + cnt; ++k) {
-                if (COUNT) ++work.tets;
-                GeomHit gh;
-                if (intersect_lean(s.geoms + 5u * k, o, no, d, t_min, t_max, &gh)) return true;
             }
         }
         if (sp == 0) return false;
-        cur = st[--sp].x;
+        enter(st[--sp].x);
     }
 }
 
