@@ -26,6 +26,10 @@ using namespace srd;
 constexpr uint32_t REF_LEAF = 0x80000000u;
 constexpr uint32_t REF_COUNT_SHIFT = 25;
 constexpr uint32_t REF_FIRST_MASK = (1u << REF_COUNT_SHIFT) - 1u;
+constexpr uint32_t REF_COUNT_MASK = 63u << REF_COUNT_SHIFT;
+// Adding this to a leaf reference moves it past its first primitive: first + 1, count - 1 (first
+// + count never reaches 2^25, so the fields do not carry into each other).
+constexpr uint32_t REF_NEXT_PRIM = 1u - (1u << REF_COUNT_SHIFT);
 constexpr uint32_t MAX_LEAF_PRIMS = 63;
 constexpr uint32_t MAX_PACKED_PRIMS = 1u << REF_COUNT_SHIFT;
 constexpr uint32_t FAST_MAX_DEPTH = 60;
@@ -290,7 +294,8 @@ __device__ __forceinline__ const float4* octant_boxes(const WideScene& s, float4
 //
 // Loop shape: one iteration is one node visit or one tetrahedron test, so the lanes of a warp at
 // a node advance by a node for each tetrahedron the lanes at a leaf test, instead of waiting for
-// the longest leaf of the warp. Each ray's own sequence of node visits and tests, and so its
+// the longest leaf of the warp. A leaf in progress is its packed reference with the tested
+// primitives taken off the front. Each ray's own sequence of node visits and tests, and so its
 // result, is the same.
 template <bool COUNT>
 __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, float4 o, float4 d, float4 inv, float t_min,
@@ -299,31 +304,23 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
     const float4* ob = octant_boxes(s, inv);
     int slot = -1, sp = 0;
     uint32_t visits = 0;
-    uint32_t lk = 0, lend = 0;  // the tetrahedra of the leaf being tested: [lk, lend)
-    // Moves to reference `ref`; a leaf's tetrahedra are tested from the next iteration on (leaves
-    // always hold at least one).
-    auto enter = [&](uint32_t ref) {
-        cur = ref;
-        if (ref & REF_LEAF) {
-            lk = ref & REF_FIRST_MASK;
-            lend = lk + ((ref >> REF_COUNT_SHIFT) & 63u);
-            if (COUNT) { ++work.leaves; work.tets += lend - lk; }
-        }
-    };
-    enter(cur);
+    if (COUNT && (cur & REF_LEAF)) ++work.leaves;
     for (;;) {
         if (++visits > MAX_VISITS_FAST) {
             atomicOr(err, ERR_TRAVERSAL_LIMIT);
             break;
         }
-        if (lk < lend) {
+        if (cur & REF_LEAF) {
+            const uint32_t k = cur & REF_FIRST_MASK;
+            if (COUNT) ++work.tets;
             GeomHit gh;
-            if (intersect_lean(s.geoms + 5u * lk, o, no, d, t_min, t_max, &gh)) {
+            if (intersect_lean(s.geoms + 5u * k, o, no, d, t_min, t_max, &gh)) {
                 t_max = gh.lambda;
                 best = gh;
-                slot = (int)lk;
+                slot = (int)k;
             }
-            if (++lk < lend) continue;
+            cur += REF_NEXT_PRIM;
+            if (cur & REF_COUNT_MASK) continue;
         } else {
             if (COUNT) ++work.nodes;
             const float4* b = ob + 4ull * cur;
@@ -338,11 +335,13 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
                 const bool ln = enl <= enr;
                 if (sp < FAST_STACK) st[sp++] = ln ? make_uint2(r.y, __float_as_uint(enr)) : make_uint2(r.x, __float_as_uint(enl));
                 else atomicOr(err, ERR_BAD_INDEX);
-                enter(ln ? r.x : r.y);
+                cur = ln ? r.x : r.y;
+                if (COUNT && (cur & REF_LEAF)) ++work.leaves;
                 continue;
             }
             if (hl || hr) {
-                enter(hl ? r.x : r.y);
+                cur = hl ? r.x : r.y;
+                if (COUNT && (cur & REF_LEAF)) ++work.leaves;
                 continue;
             }
         }
@@ -350,7 +349,8 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
         while (sp > 0) {
             const uint2 e = st[--sp];
             if (__uint_as_float(e.y) < t_max) {
-                enter(e.x);
+                cur = e.x;
+                if (COUNT && (cur & REF_LEAF)) ++work.leaves;
                 found = true;
                 break;
             }
@@ -370,26 +370,18 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
     const float4* ob = octant_boxes(s, inv);
     int sp = 0;
     uint32_t visits = 0;
-    uint32_t lk = 0, lend = 0;  // the tetrahedra of the leaf being tested: [lk, lend)
-    auto enter = [&](uint32_t ref) {
-        cur = ref;
-        if (ref & REF_LEAF) {
-            lk = ref & REF_FIRST_MASK;
-            lend = lk + ((ref >> REF_COUNT_SHIFT) & 63u);
-            if (COUNT) ++work.leaves;
-        }
-    };
-    enter(cur);
+    if (COUNT && (cur & REF_LEAF)) ++work.leaves;
     for (;;) {
         if (++visits > MAX_VISITS_FAST) {
             atomicOr(err, ERR_TRAVERSAL_LIMIT);
             return false;
         }
-        if (lk < lend) {
+        if (cur & REF_LEAF) {
             if (COUNT) ++work.tets;
             GeomHit gh;
-            if (intersect_lean(s.geoms + 5u * lk, o, no, d, t_min, t_max, &gh)) return true;
-            if (++lk < lend) continue;
+            if (intersect_lean(s.geoms + 5u * (cur & REF_FIRST_MASK), o, no, d, t_min, t_max, &gh)) return true;
+            cur += REF_NEXT_PRIM;
+            if (cur & REF_COUNT_MASK) continue;
         } else {
             if (COUNT) ++work.nodes;
             const float4* b = ob + 4ull * cur;
@@ -402,16 +394,19 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
             if (hl && hr) {
                 if (sp < FAST_STACK) st[sp++].x = r.y;
                 else atomicOr(err, ERR_BAD_INDEX);
-                enter(r.x);
+                cur = r.x;
+                if (COUNT && (cur & REF_LEAF)) ++work.leaves;
                 continue;
             }
             if (hl || hr) {
-                enter(hl ? r.x : r.y);
+                cur = hl ? r.x : r.y;
+                if (COUNT && (cur & REF_LEAF)) ++work.leaves;
                 continue;
             }
         }
         if (sp == 0) return false;
-        enter(st[--sp].x);
+        cur = st[--sp].x;
+        if (COUNT && (cur & REF_LEAF)) ++work.leaves;
     }
 }
 
