@@ -304,6 +304,10 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
     const float4* ob = octant_boxes(s, inv);
     int slot = -1, sp = 0;
     uint32_t visits = 0;
+    // The largest float below t_max (t_max > t_min > 0): with it as the exit bound, exit >= entry
+    // holds exactly when exit >= entry and entry < t_max do with t_max, so a child's hit test is
+    // one comparison.
+    float t_below = __uint_as_float(__float_as_uint(t_max) - 1u);
     if (COUNT && (cur & REF_LEAF)) ++work.leaves;
     for (;;) {
         if (++visits > MAX_VISITS_FAST) {
@@ -316,6 +320,7 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
             GeomHit gh;
             if (intersect_lean(s.geoms + 5u * k, o, no, d, t_min, t_max, &gh)) {
                 t_max = gh.lambda;
+                t_below = __uint_as_float(__float_as_uint(t_max) - 1u);
                 best = gh;
                 slot = (int)k;
             }
@@ -327,10 +332,10 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
             const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
             const uint2 r = __ldg(s.refs + cur);
             float enl, exl, enr, exr;
-            slab_octant(lnear, lfar, no, inv, t_min, t_max, &enl, &exl);
-            slab_octant(rnear, rfar, no, inv, t_min, t_max, &enr, &exr);
-            const bool hl = exl >= enl && enl < t_max;
-            const bool hr = exr >= enr && enr < t_max;
+            slab_octant(lnear, lfar, no, inv, t_min, t_below, &enl, &exl);
+            slab_octant(rnear, rfar, no, inv, t_min, t_below, &enr, &exr);
+            const bool hl = exl >= enl;  // and enl < t_max
+            const bool hr = exr >= enr;
             if (hl && hr) {
                 const bool ln = enl <= enr;
                 if (sp < FAST_STACK) st[sp++] = ln ? make_uint2(r.y, __float_as_uint(enr)) : make_uint2(r.x, __float_as_uint(enl));
