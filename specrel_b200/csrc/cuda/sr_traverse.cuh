@@ -309,11 +309,9 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
     // one comparison.
     float t_below = __uint_as_float(__float_as_uint(t_max) - 1u);
     if (COUNT && (cur & REF_LEAF)) ++work.leaves;
+    // Only node visits are counted against the bound: a leaf's tests end with its count, leaves
+    // are entered from node visits or from stack entries, and entries are pushed by node visits.
     for (;;) {
-        if (++visits > MAX_VISITS_FAST) {
-            atomicOr(err, ERR_TRAVERSAL_LIMIT);
-            break;
-        }
         if (cur & REF_LEAF) {
             const uint32_t k = cur & REF_FIRST_MASK;
             if (COUNT) ++work.tets;
@@ -327,6 +325,10 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
             cur += REF_NEXT_PRIM;
             if (cur & REF_COUNT_MASK) continue;
         } else {
+            if (++visits > MAX_VISITS_FAST) {
+                atomicOr(err, ERR_TRAVERSAL_LIMIT);
+                break;
+            }
             if (COUNT) ++work.nodes;
             const float4* b = ob + 4ull * cur;
             const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
@@ -376,11 +378,7 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
     int sp = 0;
     uint32_t visits = 0;
     if (COUNT && (cur & REF_LEAF)) ++work.leaves;
-    for (;;) {
-        if (++visits > MAX_VISITS_FAST) {
-            atomicOr(err, ERR_TRAVERSAL_LIMIT);
-            return false;
-        }
+    for (;;) {  // node visits are counted against the bound (see closest_lean)
         if (cur & REF_LEAF) {
             if (COUNT) ++work.tets;
             GeomHit gh;
@@ -388,6 +386,10 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
             cur += REF_NEXT_PRIM;
             if (cur & REF_COUNT_MASK) continue;
         } else {
+            if (++visits > MAX_VISITS_FAST) {
+                atomicOr(err, ERR_TRAVERSAL_LIMIT);
+                return false;
+            }
             if (COUNT) ++work.nodes;
             const float4* b = ob + 4ull * cur;
             const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
