@@ -10,14 +10,30 @@
 //   src/bvh4d.rs:8-13,123-141,287-427  box_measure, build, split (8-bin SAH over 4 axes)
 //   src/bvh4d.rs:430-578   safe_inv_dir, trace, is_occluded
 #pragma once
+#include <atomic>
 #include <functional>
+#include <future>
 #include <numeric>
+#include <thread>
 #include <utility>
 #include <vector>
 
 #include "oracle_math.hpp"
 
 namespace orc {
+
+// fn(i) for i in [0, n) on the host's threads (work items taken from a shared counter).
+template <class F> void parallel_for(uint32_t n, F&& fn) {
+    const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), n));
+    std::atomic<uint32_t> next{0};
+    auto work = [&] {
+        for (uint32_t i; (i = next.fetch_add(1)) < n;) fn(i);
+    };
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+}
 
 constexpr float DECIDED_AT_STATIC = -1.0e9f;  // mesh4d.rs:5
 
@@ -478,7 +494,11 @@ template <class T> struct Bvh {
     }
     const Simplex<T>& leaf_simplex(size_t i) const { return simplices[order[i]]; }
 
-    static uint32_t build_recursive(std::vector<BvhNode<T>>& nodes, Ref* refs, size_t count, size_t first) {
+    // Large subtrees are built on a second thread into their own arrays and spliced in depth-
+    // first order (left subtree, then right), which gives the serial build's array exactly: the
+    // two subtrees own disjoint ranges of `refs`.
+    static uint32_t build_recursive(std::vector<BvhNode<T>>& nodes, Ref* refs, size_t count, size_t first,
+                                    int spawn_depth = 6) {
         uint32_t node_idx = (uint32_t)nodes.size();
         Aabb<T> bounds;
         size_t mid;
@@ -495,8 +515,27 @@ template <class T> struct Bvh {
         nd.aabb = bounds;
         nd.left = node_idx + 1;
         nodes.push_back(nd);
-        build_recursive(nodes, refs, mid, first);
-        uint32_t right_idx = build_recursive(nodes, refs + mid, count - mid, first + mid);
+        if (spawn_depth > 0 && count >= 65536) {
+            std::vector<BvhNode<T>> ln, rn;
+            auto fl = std::async(std::launch::async, [&] { build_recursive(ln, refs, mid, first, spawn_depth - 1); });
+            build_recursive(rn, refs + mid, count - mid, first + mid, spawn_depth - 1);
+            fl.get();
+            const uint32_t lbase = node_idx + 1, rbase = lbase + (uint32_t)ln.size();
+            for (auto* part : {&ln, &rn}) {
+                const uint32_t base = part == &ln ? lbase : rbase;
+                for (BvhNode<T> x : *part) {
+                    if (x.count == 0) {
+                        x.left += base;
+                        x.right_or_first += base;
+                    }
+                    nodes.push_back(x);
+                }
+            }
+            nodes[node_idx].right_or_first = rbase;
+            return node_idx;
+        }
+        build_recursive(nodes, refs, mid, first, 0);
+        uint32_t right_idx = build_recursive(nodes, refs + mid, count - mid, first + mid, 0);
         nodes[node_idx].right_or_first = right_idx;
         return node_idx;
     }

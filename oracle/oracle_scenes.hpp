@@ -202,6 +202,10 @@ template <class T> SynthOut<T> synth_scene(const SynthParams& p) {
     sc.light_pos = V3<T>(T(0), T(50), T(0));
     if (p.config == 2) {
         const uint32_t mats[6] = {6, 7, 8, 1, 6, 5};
+        // The bodies are drawn in order (the draws alone use the generator), then extruded on
+        // worker threads and concatenated in body order: the same simplices as one serial loop.
+        struct Body { double c[3], d[3], r, a_eff; };
+        std::vector<Body> bodies(p.n_bodies);
         for (uint32_t i = 0; i < p.n_bodies; ++i) {
             double c[3], r, a, d[3], a_eff;
             // A body that would enclose or graze the observer at the origin during t in [-5, 0]
@@ -222,12 +226,30 @@ template <class T> SynthOut<T> synth_scene(const SynthParams& p) {
                 if (attempt >= 1000 || clear_of_observer(probe, r + OBSERVER_CLEARANCE)) break;
             }
             if (a_eff < a) out.clamped_accel++;
-            HyperbolicPath path(c, d, a_eff, ACCEL_START_T, ACCEL_PROPER_TIME);
-            bool sl = false;
-            auto samples = sample_accelerated_worldline<T>(path, T(-100), T(0), p.steps, &sl);
-            out.superluminal |= sl;
-            Mesh3D<T> mesh = icosphere<T>(r, (int)p.subdiv);
-            out.rindler_ok &= extend_worldtube_simplices<T>(simplices, mesh, samples, (const T*)nullptr, mats[i % 6]);
+            Body& b = bodies[i];
+            for (int k = 0; k < 3; ++k) { b.c[k] = c[k]; b.d[k] = d[k]; }
+            b.r = r;
+            b.a_eff = a_eff;
+        }
+        std::vector<std::vector<Simplex<T>>> parts(p.n_bodies);
+        std::vector<char> sl(p.n_bodies, 0), ok(p.n_bodies, 1);
+        parallel_for(p.n_bodies, [&](uint32_t i) {
+            Body& b = bodies[i];
+            HyperbolicPath path(b.c, b.d, b.a_eff, ACCEL_START_T, ACCEL_PROPER_TIME);
+            bool s_l = false;
+            auto samples = sample_accelerated_worldline<T>(path, T(-100), T(0), p.steps, &s_l);
+            sl[i] = s_l;
+            Mesh3D<T> mesh = icosphere<T>(b.r, (int)p.subdiv);
+            ok[i] = extend_worldtube_simplices<T>(parts[i], mesh, samples, (const T*)nullptr, mats[i % 6]);
+        });
+        size_t total = 0;
+        for (auto& v : parts) total += v.size();
+        simplices.reserve(total);
+        for (uint32_t i = 0; i < p.n_bodies; ++i) {
+            out.superluminal |= sl[i] != 0;
+            out.rindler_ok &= ok[i] != 0;
+            simplices.insert(simplices.end(), parts[i].begin(), parts[i].end());
+            std::vector<Simplex<T>>().swap(parts[i]);
         }
         double ph[3];
         rng.ball(ph);
