@@ -243,13 +243,15 @@ static __device__ __noinline__ bool sample_digital_tau(float u, float v, float t
     return ((__ldg(tables + SR_GAMMA_LUT_SIZE + g * 7u + (uint32_t)row) >> (4u - cc)) & 1u) != 0u;
 }
 
-static __device__ __noinline__ F3 corner_mini_clock(float mdx, float mdy, float mr, float tau, const Mat& m) {
-    if (mr > 0.080f) return mul(m.base, 1.15f);  // renderer.rs:880-927
+// The out-of-line helpers below take scalars by value: a struct passed by reference to a call
+// would have to be stored to per-thread local memory first.
+static __device__ __noinline__ F3 corner_mini_clock(float mdx, float mdy, float mr, float tau, F3 base) {
+    if (mr > 0.080f) return mul(base, 1.15f);  // renderer.rs:880-927
     float ang = rem_e(atan2f(mdx, mdy), TAU_F);
     float fast = rem_e((tau / 1.0f) * TAU_F, TAU_F);
     float main = rem_e((tau / 10.0f) * TAU_F, TAU_F);
     F3 col{0.04f, 0.06f, 0.10f};
-    if (ang <= fast && mr < 0.066f) col = add(col, mul(m.base, 0.25f));
+    if (ang <= fast && mr < 0.066f) col = add(col, mul(base, 0.25f));
     if (mr >= 0.062f && mr <= 0.078f) {
         float sector = ang / (TAU_F / 10.0f);
         float dist = fabsf(sector - roundf(sector));
@@ -264,28 +266,29 @@ static __device__ __noinline__ F3 corner_mini_clock(float mdx, float mdy, float 
     return col;
 }
 
-static __device__ __noinline__ F3 clock_face(const Hit& h, const Mat& m, const uint32_t* tables) {
-    float grid = fmaxf(m.grid, 1e-4f);  // renderer.rs:737-874
+static __device__ __noinline__ F3 clock_face(float uv_u, float uv_v, float tau, float grad_u, float grad_v, float uvs_u,
+                                             float uvs_v, float m_grid, F3 base, F3 checker, const uint32_t* tables) {
+    float grid = fmaxf(m_grid, 1e-4f);  // renderer.rs:737-874
     float inv_grid = 1.0f / grid;
-    float u = rem_e(h.uv_u * grid, 1.0f);
-    float v = rem_e(h.uv_v * grid, 1.0f);
+    float u = rem_e(uv_u * grid, 1.0f);
+    float v = rem_e(uv_v * grid, 1.0f);
     // clock_tile_central_proper_time (renderer.rs:704-715)
     float ig2 = 1.0f / fmaxf(grid, 1e-4f);
-    float central = h.tau - (((u - 0.5f) * ig2) * h.grad_u + ((v - 0.5f) * ig2) * h.grad_v);
+    float central = tau - (((u - 0.5f) * ig2) * grad_u + ((v - 0.5f) * ig2) * grad_v);
     const float CX[4] = {0.135f, 0.865f, 0.135f, 0.865f}, CY[4] = {0.865f, 0.865f, 0.135f, 0.135f};
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         float mdx = u - CX[i], mdy = v - CY[i];
         float mr = sqrtf(mdx * mdx + mdy * mdy);
         if (mr <= 0.095f) {
-            float osc = central + ((CX[i] - 0.5f) * inv_grid) * h.grad_u + ((CY[i] - 0.5f) * inv_grid) * h.grad_v;
-            float px = (mdx * inv_grid) * h.uvs_u, py = (mdy * inv_grid) * h.uvs_v;
+            float osc = central + ((CX[i] - 0.5f) * inv_grid) * grad_u + ((CY[i] - 0.5f) * inv_grid) * grad_v;
+            float px = (mdx * inv_grid) * uvs_u, py = (mdy * inv_grid) * uvs_v;
             float mrp = sqrtf(px * px + py * py);
-            return corner_mini_clock(mdx, mdy, mr, osc - mrp, m);
+            return corner_mini_clock(mdx, mdy, mr, osc - mrp, base);
         }
     }
     if (v >= 0.035f && v <= 0.205f && u >= 0.25f && u <= 0.75f) {
-        if (!(v >= 0.050f && v <= 0.190f) || !(u >= 0.265f && u <= 0.735f)) return mul(m.base, 0.9f);
+        if (!(v >= 0.050f && v <= 0.190f) || !(u >= 0.265f && u <= 0.735f)) return mul(base, 0.9f);
         if (v >= 0.06f && v <= 0.18f && u >= 0.28f && u <= 0.72f && sample_digital_tau(u, v, central, tables))
             return F3{1.0f, 0.96f, 0.30f};
         return F3{0.03f, 0.04f, 0.07f};
@@ -295,16 +298,16 @@ static __device__ __noinline__ F3 clock_face(const Hit& h, const Mat& m, const u
     if (r > 0.330f) {
         int gu = (int)floorf(u * 4.0f), gv = (int)floorf(v * 4.0f);
         int s = (int)((unsigned)gu + (unsigned)gv);
-        return ((s % 2 + 2) % 2) == 0 ? mul(m.base, 0.78f) : mul(m.checker, 0.78f);
+        return ((s % 2 + 2) % 2) == 0 ? mul(base, 0.78f) : mul(checker, 0.78f);
     }
-    if (r > 0.292f) return mul(m.base, 1.15f);
-    float dxp = (dx * inv_grid) * h.uvs_u, dyp = (dy * inv_grid) * h.uvs_v;
+    if (r > 0.292f) return mul(base, 1.15f);
+    float dxp = (dx * inv_grid) * uvs_u, dyp = (dy * inv_grid) * uvs_v;
     float rp = sqrtf(dxp * dxp + dyp * dyp);
     float dial = central - rp;
     float ang = rem_e(atan2f(dx, dy), TAU_F);
     float main = rem_e((dial / 10.0f) * TAU_F, TAU_F);
     F3 dc{0.04f, 0.06f, 0.10f};
-    if (ang <= main && r < 0.236f) dc = add(dc, mul(m.base, 0.22f));
+    if (ang <= main && r < 0.236f) dc = add(dc, mul(base, 0.22f));
     if (r >= 0.220f && r <= 0.286f) {
         float sector = ang / (TAU_F / 10.0f);
         float dist = fabsf(sector - roundf(sector));
@@ -328,13 +331,13 @@ static __device__ __noinline__ F3 clock_face(const Hit& h, const Mat& m, const u
     return dc;
 }
 
-static __device__ __noinline__ F3 light_clock(float uv_u, float uv_v, float tau, const Mat& m) {
-    float u = rem_e(uv_u * m.grid, 1.0f);  // renderer.rs:988-1052
-    float v = rem_e(uv_v * m.grid, 1.0f);
-    if (!(u >= 0.12f && u <= 0.88f)) return mul(m.base, 0.65f);
+static __device__ __noinline__ F3 light_clock(float uv_u, float uv_v, float tau, float m_grid, float m_cavity, F3 base) {
+    float u = rem_e(uv_u * m_grid, 1.0f);  // renderer.rs:988-1052
+    float v = rem_e(uv_v * m_grid, 1.0f);
+    if (!(u >= 0.12f && u <= 0.88f)) return mul(base, 0.65f);
     if ((v >= 0.04f && v <= 0.10f) || (v >= 0.90f && v <= 0.96f)) return F3{0.75f, 0.90f, 0.98f};
     if (!(v >= 0.10f && v <= 0.90f)) return F3{0.08f, 0.12f, 0.16f};
-    float period = fmaxf(2.0f * m.cavity, 1e-4f);
+    float period = fmaxf(2.0f * m_cavity, 1e-4f);
     float cycle = rem_e(tau / period, 1.0f);
     float bounce = cycle < 0.5f ? cycle * 2.0f : (1.0f - cycle) * 2.0f;
     float pv = 0.10f + 0.80f * bounce;
@@ -346,7 +349,7 @@ static __device__ __noinline__ F3 light_clock(float uv_u, float uv_v, float tau,
     if (du < 0.015f) col = add(col, F3{0.06f, 0.16f, 0.16f});
     if (dv < 0.032f) {
         float k = 1.0f - dv / 0.032f;
-        col = add(col, mul(m.base, 0.9f * (k * k)));
+        col = add(col, mul(base, 0.9f * (k * k)));
     }
     if (dist < 0.11f) {
         float k = 1.0f - dist / 0.11f;
@@ -368,9 +371,9 @@ __device__ __forceinline__ F3 surface_albedo(const Hit& h, const Mat& m, const u
         }
         a = col;
     } else if (m.pattern == 1u) {
-        a = clock_face(h, m, tables);
+        a = clock_face(h.uv_u, h.uv_v, h.tau, h.grad_u, h.grad_v, h.uvs_u, h.uvs_v, m.grid, m.base, m.checker, tables);
     } else {
-        a = light_clock(h.uv_u, h.uv_v, h.tau, m);
+        a = light_clock(h.uv_u, h.uv_v, h.tau, m.grid, m.cavity, m.base);
     }
     if (m.pattern != 0u) {
         float ut = rem_e(h.uv_u * m.grid, 1.0f), vt = rem_e(h.uv_v * m.grid, 1.0f);

@@ -676,7 +676,7 @@ struct FrameOccluder {
 };
 
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_shade_batch(ShadeBatchArgs a) {
+__global__ void __launch_bounds__(256, 3) k_shade_batch(const __grid_constant__ ShadeBatchArgs a) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.total_px) return;
     uint32_t o = find_obs(a.pix_pre, a.n, p);

@@ -117,7 +117,7 @@ struct RefOccluder {
     __device__ bool operator()(float4 o, float4 d, float t0, float t1) { return occluded_ref(*s, o, d, t0, t1, err); }
 };
 
-__global__ void __launch_bounds__(64) k_render_plain(SceneDev s, SrGpuUniforms U, const float4* cam_dev, FrameDev f,
+__global__ void __launch_bounds__(64, 16) k_render_plain(SceneDev s, SrGpuUniforms U, const float4* cam_dev, FrameDev f,
                                                      BBConst bb) {
     uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t py = blockIdx.y * blockDim.y + threadIdx.y;

@@ -30,24 +30,25 @@ __device__ __forceinline__ float illumination(const SrGpuUniforms& U, const Cam&
 
 // compute_flash_illumination with the uniform block's premultiplied colours (gpu.rs:160-167).
 template <class Occ>
-static __device__ __noinline__ F3 flash_illumination(const SrGpuUniforms& U, const Hit& h, Occ& occ, uint32_t* shadow_rays) {
+static __device__ __noinline__ F3 flash_illumination(const SrGpuUniforms& U, float4 event, float4 normal, float4 four_vel,
+                                                     Occ& occ, uint32_t* shadow_rays) {
     F3 total{0.0f, 0.0f, 0.0f};
     for (uint32_t i = 0; i < U.num_flashes; ++i) {
         float4 at = v4(U.flash_at[i][0], U.flash_at[i][1], U.flash_at[i][2], U.flash_at[i][3]);
-        float dt = h.event.x - at.x;
+        float dt = event.x - at.x;
         if (dt <= 0.0f) continue;
-        float dist = fmaxf(len3(sub(spatial(at), spatial(h.event))), 1e-4f);
+        float dist = fmaxf(len3(sub(spatial(at), spatial(event))), 1e-4f);
         float err = fabsf(dt - dist);
         float hw = fmaxf(0.5f * U.flash_col_width[i][3], 1e-3f);
         if (err >= hw) continue;
         float k = 1.0f - err / hw;
         float pulse = k * k;
-        float4 tf = mul4(sub4(at, h.event), 1.0f / dist);
-        float cf = fmaxf(rest_frame_cos(tf, h.normal, h.four_vel), 0.0f);
+        float4 tf = mul4(sub4(at, event), 1.0f / dist);
+        float cf = fmaxf(rest_frame_cos(tf, normal, four_vel), 0.0f);
         bool in_shadow = false;
         if (cf > 0.0f && U.shadow_mode != 0u) {
             ++*shadow_rays;
-            in_shadow = occ(h.event, tf, 2e-3f, dist - 2e-3f);
+            in_shadow = occ(event, tf, 2e-3f, dist - 2e-3f);
         }
         float sf = in_shadow ? 0.25f : 1.0f;
         float atten = 1.0f / (1.0f + 0.015f * dist * dist);
@@ -67,7 +68,7 @@ __device__ __forceinline__ F3 shade_hit(const srk::SceneDev& s, const SrGpuUnifo
         float lighting = illumination(U, cam, dir, h, m, occ, shadow_rays);
         F3 lit = mul(albedo, lighting);
         if (U.num_flashes > 0u) {
-            F3 fr = flash_illumination(U, h, occ, shadow_rays);
+            F3 fr = flash_illumination(U, h.event, h.normal, h.four_vel, occ, shadow_rays);
             lit = add(lit, mulv(add(mul(albedo, 0.65f), F3{0.35f, 0.35f, 0.35f}), fr));
         }
         return apply_fog(lit, dir, h.lambda);
