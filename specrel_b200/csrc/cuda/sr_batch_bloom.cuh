@@ -65,13 +65,9 @@ __global__ void k_bloom_up_batch(float4* hdr, const ObsDev* obs, const uint32_t*
     *dst = make_float4(v.x + up.x, v.y + up.y, v.z + up.z, 0.0f);
 }
 
-__global__ void __launch_bounds__(256) k_bloom_composite_batch(const float4* hdr, const ObsDev* obs, const uint32_t* pre,
-                                                               uint32_t n, uint32_t* rgb, const uint32_t* tables) {
-    __shared__ uint8_t lut[SR_GAMMA_LUT_SIZE];
-    for (uint32_t i = threadIdx.x; i < SR_GAMMA_LUT_SIZE; i += blockDim.x) lut[i] = (uint8_t)__ldg(tables + i);
-    __syncthreads();
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= __ldg(pre + n)) return;
+// One pixel of the composite (bloom.rs:93-125 with pack_rgb_with_lut, renderer.rs:1116-1129).
+__device__ __forceinline__ void composite_pixel(const float4* hdr, const ObsDev* obs, const uint32_t* pre, uint32_t n,
+                                                uint32_t* rgb, const uint8_t* lut, uint32_t i) {
     uint32_t o = find_obs(pre, n, i);
     const ObsDev& od = obs[o];
     uint32_t l = i - __ldg(pre + o);
@@ -90,6 +86,18 @@ __global__ void __launch_bounds__(256) k_bloom_composite_batch(const float4* hdr
     float fx = mx * scale, fy = my * scale, fz = mz * scale;
     uint32_t ix = fx > 0.0f ? (uint32_t)fx : 0u, iy = fy > 0.0f ? (uint32_t)fy : 0u, iz = fz > 0.0f ? (uint32_t)fz : 0u;
     rgb[i] = ((uint32_t)lut[ix] << 16) | ((uint32_t)lut[iy] << 8) | (uint32_t)lut[iz];
+}
+
+// Grid-stride over the batch's pixels: a block stages the gamma LUT in shared memory once and
+// composites many pixels with it (the grid is a few blocks per SM, not one block per 256 pixels).
+__global__ void __launch_bounds__(256) k_bloom_composite_batch(const float4* hdr, const ObsDev* obs, const uint32_t* pre,
+                                                               uint32_t n, uint32_t* rgb, const uint32_t* tables) {
+    __shared__ uint8_t lut[SR_GAMMA_LUT_SIZE];
+    for (uint32_t i = threadIdx.x; i < SR_GAMMA_LUT_SIZE; i += blockDim.x) lut[i] = (uint8_t)__ldg(tables + i);
+    __syncthreads();
+    const uint32_t total = __ldg(pre + n);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+        composite_pixel(hdr, obs, pre, n, rgb, lut, i);
 }
 
 }  // namespace srk
