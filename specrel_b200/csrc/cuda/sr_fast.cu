@@ -597,15 +597,16 @@ __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
         float4 o, d;
         float sx, sy;
         camera_ray(U, cam, px, py, &o, &d, &sx, &sy);
+        const float4 no = neg4(o);  // the traversal and the hit event use the negated origin only
         const float4 inv = v4(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z), safe_inv(d.w));
         float t_max = 180.0f;
         GeomHit best{0.0f, 0.0f, 0.0f, 0.0f};
         int slot = -1;
         if (!a.ws.empty) {
             float en, ex;
-            slab_interval(a.ws.root_min, a.ws.root_max, neg4(o), inv, 1e-3f, t_max, &en, &ex);
+            slab_interval(a.ws.root_min, a.ws.root_max, no, inv, 1e-3f, t_max, &en, &ex);
             if (ex >= en && en < t_max)  // else the ray misses the scene's box (bvh4d.rs:451)
-                slot = closest_lean<COUNT>(a.ws, a.ws.root_ref, o, d, inv, 1e-3f, t_max, best, st, a.err, wp);
+                slot = closest_lean<COUNT>(a.ws, a.ws.root_ref, no, d, inv, 1e-3f, t_max, best, st, a.err, wp);
         }
         a.hits[pix] = make_float4(best.lambda, best.u, best.v, best.w);
         a.slots[pix] = slot < 0 ? 0xFFFFFFFFu : (uint32_t)slot;
@@ -615,10 +616,11 @@ __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
             const float4* at = a.attrs + 12u * (uint32_t)slot;
             const uint32_t mat = __float_as_uint(__ldg(at + 10).z);
             if (__float_as_uint(__ldg(a.mats + 3u * mat + 2u).y) == 0u) {
-                const float4 ev = add4(o, mul4(d, best.lambda));
+                const float4 ev = sub4(mul4(d, best.lambda), no);  // o + d * lambda
                 float4 tl;
                 float dist;
-                light_ray(U, cam, ev, &tl, &dist);
+                // The camera is read again here rather than kept in registers across the traversal.
+                light_ray(U, cam_of(a.cam, obs), ev, &tl, &dist);
                 if (fmaxf(rest_frame_cos(tl, __ldg(at + 8), __ldg(at + 9)), 0.0f) > 0.0f) {
                     // Bvh4D::is_occluded(hit.event, to_light, 2e-3, dist - 2e-3) (renderer.rs:636-641).
                     sh = 1;
@@ -626,7 +628,7 @@ __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
                     const float s0 = 2e-3f, s1 = dist - 2e-3f;
                     float en, ex;
                     slab_interval(a.ws.root_min, a.ws.root_max, neg4(ev), sinv, s0, s1, &en, &ex);
-                    if (ex >= en && any_lean<COUNT>(a.ws, a.ws.root_ref, ev, tl, sinv, s0, s1, st, a.err, wsh)) sh = 2;
+                    if (ex >= en && any_lean<COUNT>(a.ws, a.ws.root_ref, neg4(ev), tl, sinv, s0, s1, st, a.err, wsh)) sh = 2;
                 }
             }
         }

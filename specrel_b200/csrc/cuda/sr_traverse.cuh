@@ -239,7 +239,7 @@ __device__ __forceinline__ void slab_interval(float4 bmin, float4 bmax, float4 n
 
 // SimplexGeom4D::intersect_fast (mesh4d.rs:175-211) in paired arithmetic, for a ray with origin
 // o = -no: the values of intersect_geom bit for bit.
-__device__ __forceinline__ bool intersect_lean(const float4* g, float4 o, float4 no, float4 d, float t_min, float t_max,
+__device__ __forceinline__ bool intersect_lean(const float4* g, float4 no, float4 d, float t_min, float t_max,
                                                GeomHit* h) {
     const float4 n = __ldg(g + 1);
     const float denom = edot_p(n, d);
@@ -250,7 +250,7 @@ __device__ __forceinline__ bool intersect_lean(const float4* g, float4 o, float4
     if (lambda <= t_min || lambda >= t_max) return false;
     // The event o + d * lambda in scalar arithmetic: ptxas fuses a paired product followed by a
     // paired sum into one fused multiply-add (one rounding), whatever the rounding modifiers say.
-    const float4 ev = add4(o, mul4(d, lambda));
+    const float4 ev = sub4(mul4(d, lambda), no);  // o + d * lambda: negation is exact, a - b is a + (-b)
     const float2 q01 = add2(f2(ev.x, ev.y), f2(-v0.x, -v0.y)), q23 = add2(f2(ev.z, ev.w), f2(-v0.z, -v0.w));
     const float4 q = make_float4(q01.x, q01.y, q23.x, q23.y);
     const float eps = -1e-5f;
@@ -298,9 +298,8 @@ __device__ __forceinline__ const float4* octant_boxes(const WideScene& s, float4
 // primitives taken off the front. Each ray's own sequence of node visits and tests, and so its
 // result, is the same.
 template <bool COUNT>
-__device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, float4 o, float4 d, float4 inv, float t_min,
+__device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, float4 no, float4 d, float4 inv, float t_min,
                                             float& t_max, GeomHit& best, uint2* st, uint32_t* err, Work& work) {
-    const float4 no = neg4(o);
     const float4* ob = octant_boxes(s, inv);
     int slot = -1, sp = 0;
     uint32_t visits = 0;
@@ -316,7 +315,7 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
             const uint32_t k = cur & REF_FIRST_MASK;
             if (COUNT) ++work.tets;
             GeomHit gh;
-            if (intersect_lean(s.geoms + 5u * k, o, no, d, t_min, t_max, &gh)) {
+            if (intersect_lean(s.geoms + 5u * k, no, d, t_min, t_max, &gh)) {
                 t_max = gh.lambda;
                 t_below = __uint_as_float(__float_as_uint(t_max) - 1u);
                 best = gh;
@@ -371,9 +370,8 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
 // culling (Bvh4D::is_occluded, bvh4d.rs:523-578). (The answer does not depend on the order;
 // nearer-first measured 7% slower on the 7.9M-tet scene.)
 template <bool COUNT>
-__device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float4 o, float4 d, float4 inv, float t_min,
+__device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float4 no, float4 d, float4 inv, float t_min,
                                          float t_max, uint2* st, uint32_t* err, Work& work) {
-    const float4 no = neg4(o);
     const float4* ob = octant_boxes(s, inv);
     int sp = 0;
     uint32_t visits = 0;
@@ -382,7 +380,7 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
         if (cur & REF_LEAF) {
             if (COUNT) ++work.tets;
             GeomHit gh;
-            if (intersect_lean(s.geoms + 5u * (cur & REF_FIRST_MASK), o, no, d, t_min, t_max, &gh)) return true;
+            if (intersect_lean(s.geoms + 5u * (cur & REF_FIRST_MASK), no, d, t_min, t_max, &gh)) return true;
             cur += REF_NEXT_PRIM;
             if (cur & REF_COUNT_MASK) continue;
         } else {
