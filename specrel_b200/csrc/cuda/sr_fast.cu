@@ -662,8 +662,9 @@ struct ShadeBatchArgs {
 };
 
 // The shadow queries of a pixel's shading: the main light's was traced by the trace kernel (its
-// state must say so); with flashes in the frame every query is traced here.
-template <bool COUNT>
+// state must say so); with flashes in the frame every query is traced here. The SIMPLE kernel
+// (no flashes in the batch) carries no traversal code.
+template <bool COUNT, bool SIMPLE>
 struct FrameOccluder {
     const WideScene* s;
     uint32_t* err;
@@ -671,14 +672,16 @@ struct FrameOccluder {
     uint8_t state;
     bool trace_here;
     __device__ bool operator()(float4 o, float4 d, float t0, float t1) {
-        if (trace_here) return occluded_wide<COUNT>(*s, o, d, t0, t1, err, work);
+        if (!SIMPLE && trace_here) return occluded_wide<COUNT>(*s, o, d, t0, t1, err, work);
         if (state == 0) atomicOr(err, ERR_SHADOW_MISMATCH);
         return state == 2;
     }
 };
 
-template <bool COUNT>
-__global__ void __launch_bounds__(256, 3) k_shade_batch(const __grid_constant__ ShadeBatchArgs a) {
+// SIMPLE: every observer of the batch is flash-free and gets its stars (if any) from the binned
+// pass, so the kernel has neither shadow traversal nor the per-pixel star sum.
+template <bool COUNT, bool SIMPLE>
+__global__ void __launch_bounds__(256, SIMPLE ? 4 : 3) k_shade_batch(const __grid_constant__ ShadeBatchArgs a) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.total_px) return;
     uint32_t o = find_obs(a.pix_pre, a.n, p);
@@ -701,13 +704,13 @@ __global__ void __launch_bounds__(256, 3) k_shade_batch(const __grid_constant__ 
         float4 hr = a.hits[p];
         GeomHit gh{hr.x, hr.y, hr.z, hr.w};
         interpolate(a.s.attrs + 12u * slot, ro, rd, gh, &h);
-        FrameOccluder<COUNT> occ{&a.ws, a.counters + 1, &work, a.shadow[p], U.num_flashes != 0u};
+        FrameOccluder<COUNT, SIMPLE> occ{&a.ws, a.counters + 1, &work, a.shadow[p], U.num_flashes != 0u};
         color = shade_hit(a.s, U, cam, rd, h, occ, &shadow_rays);
         if (U.num_haze > 0u) color = apply_haze(color, h.event, U);
     } else {
         color = shade_sky(rd);
     }
-    if (U.mode == 0u && a.s.num_stars > 0u && !(a.stars_binned && stars_binned_for(U, a.s.num_stars)))
+    if (!SIMPLE && U.mode == 0u && a.s.num_stars > 0u && !(a.stars_binned && stars_binned_for(U, a.s.num_stars)))
         color = add(color, stars_brute(a.s, U, cam, ro, rd, sx, sy, slot != 0xFFFFFFFFu ? h.lambda : INFINITY, a.bb));
     a.hdr[(size_t)od.pyr_base + l] = make_float4(color.x, color.y, color.z, 0.0f);
     if (a.hit_id)
@@ -812,6 +815,14 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
     bool binned = false;
     if (!r.star_brute && sd.num_stars > 0)
         for (uint32_t i = 0; i < n; ++i) binned = binned || stars_binned_for(r.u[i], sd.num_stars);
+    // A flash-free batch whose stars all come from the binned pass shades with the SIMPLE kernel.
+    bool simple = true;
+    for (uint32_t i = 0; i < n; ++i) {
+        const SrGpuUniforms& ui = r.u[i];
+        if (ui.num_flashes != 0u ||
+            (ui.mode == 0u && sd.num_stars > 0u && !(binned && stars_binned_for(ui, sd.num_stars))))
+            simple = false;
+    }
     const size_t old_star = c.star_cd.bytes + c.star_rect.bytes + c.star_count.bytes + c.star_list.bytes + c.star_scan.bytes;
     // Star lists: room for every (observer, star) in 8 tiles; tiles past the room sum every star.
     const uint32_t list_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(8ull * n * sd.num_stars, 1u << 20), 1u << 30);
@@ -934,8 +945,13 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
         sa.bb = bb;
         sa.stars_binned = binned ? 1u : 0u;
         uint32_t gpx = (sh.total_px + 255) / 256;
-        if (r.count_work) k_shade_batch<true><<<gpx, 256, 0, st>>>(sa);
-        else k_shade_batch<false><<<gpx, 256, 0, st>>>(sa);
+        if (r.count_work) {
+            if (simple) k_shade_batch<true, true><<<gpx, 256, 0, st>>>(sa);
+            else k_shade_batch<true, false><<<gpx, 256, 0, st>>>(sa);
+        } else {
+            if (simple) k_shade_batch<false, true><<<gpx, 256, 0, st>>>(sa);
+            else k_shade_batch<false, false><<<gpx, 256, 0, st>>>(sa);
+        }
         if ((x = cudaGetLastError()) != cudaSuccess) return x;
         if (timed) cudaEventRecord(r.ev[2], st);
         if (binned) {
@@ -1021,6 +1037,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
                        t.leaf_coop);
     key = mix(key, t.home_pct);
     key = mix(key, binned ? 0x5354ull : 0ull);
+    key = mix(key, simple ? 0x51ull : 0ull);
     for (auto& o : sh.obs) key = mix(key, ((uint64_t)o.width << 32) | o.height);
     auto it = c.graphs.find(key);
     if (it == c.graphs.end()) {
