@@ -65,39 +65,55 @@ __global__ void k_bloom_up_batch(float4* hdr, const ObsDev* obs, const uint32_t*
     *dst = make_float4(v.x + up.x, v.y + up.y, v.z + up.z, 0.0f);
 }
 
-// One pixel of the composite (bloom.rs:93-125 with pack_rgb_with_lut, renderer.rs:1116-1129).
-__device__ __forceinline__ void composite_pixel(const float4* hdr, const ObsDev* obs, const uint32_t* pre, uint32_t n,
-                                                uint32_t* rgb, const uint8_t* lut, uint32_t i) {
-    uint32_t o = find_obs(pre, n, i);
-    const ObsDev& od = obs[o];
-    uint32_t l = i - __ldg(pre + o);
-    uint32_t w = od.lw[0], x = l % w, y = l / w;
-    const float strength = 0.04f;
-    const float keep = 1.0f - strength;
-    const float halo = strength / (float)SR_BLOOM_LEVELS;
-    float4 up = upsample_b(hdr + od.pyr_base + od.loff[1], od.lw[1], od.lh[1], x, y);
-    float4 c = hdr[od.pyr_base + l];
-    float cx = c.x * keep + up.x * halo, cy = c.y * keep + up.y * halo, cz = c.z * keep + up.z * halo;
-    float mx = cx / (1.0f + cx * 0.35f), my = cy / (1.0f + cy * 0.35f), mz = cz / (1.0f + cz * 0.35f);
-    mx = mx < 0.0f ? 0.0f : (mx > 1.0f ? 1.0f : mx);
-    my = my < 0.0f ? 0.0f : (my > 1.0f ? 1.0f : my);
-    mz = mz < 0.0f ? 0.0f : (mz > 1.0f ? 1.0f : mz);
-    const float scale = (float)(SR_GAMMA_LUT_SIZE - 1);
-    float fx = mx * scale, fy = my * scale, fz = mz * scale;
-    uint32_t ix = fx > 0.0f ? (uint32_t)fx : 0u, iy = fy > 0.0f ? (uint32_t)fy : 0u, iz = fz > 0.0f ? (uint32_t)fz : 0u;
-    rgb[i] = ((uint32_t)lut[ix] << 16) | ((uint32_t)lut[iy] << 8) | (uint32_t)lut[iz];
-}
-
-// Grid-stride over the batch's pixels: a block stages the gamma LUT in shared memory once and
-// composites many pixels with it (the grid is a few blocks per SM, not one block per 256 pixels).
-__global__ void __launch_bounds__(256) k_bloom_composite_batch(const float4* hdr, const ObsDev* obs, const uint32_t* pre,
-                                                               uint32_t n, uint32_t* rgb, const uint32_t* tables) {
+// The composite (bloom.rs:93-125) and pack_rgb_with_lut (renderer.rs:1116-1129) of every pixel of
+// the batch. A block takes a contiguous run of 256-pixel segments, so a thread's pixels increase
+// and it keeps its observer's pyramid fields in registers, looking them up again only when it
+// crosses into the next observer; per pixel only the independent HDR loads remain. The block
+// stages the gamma LUT in shared memory once (the grid is a few blocks per SM).
+__global__ void __launch_bounds__(256) k_bloom_composite_batch(const float4* __restrict__ hdr,
+                                                               const ObsDev* __restrict__ obs,
+                                                               const uint32_t* __restrict__ pre, uint32_t n,
+                                                               uint32_t* __restrict__ rgb, const uint32_t* tables) {
     __shared__ uint8_t lut[SR_GAMMA_LUT_SIZE];
     for (uint32_t i = threadIdx.x; i < SR_GAMMA_LUT_SIZE; i += blockDim.x) lut[i] = (uint8_t)__ldg(tables + i);
     __syncthreads();
     const uint32_t total = __ldg(pre + n);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
-        composite_pixel(hdr, obs, pre, n, rgb, lut, i);
+    const uint32_t segs = (total + blockDim.x - 1) / blockDim.x;
+    const uint32_t per = (segs + gridDim.x - 1) / gridDim.x;
+    const uint32_t s0 = blockIdx.x * per, s1 = min(segs, s0 + per);
+    uint32_t lo = 0, hi = 0, w = 1, w1 = 1, h1 = 1;
+    const float4* base0 = hdr;
+    const float4* base1 = hdr;
+    const float strength = 0.04f;
+    const float keep = 1.0f - strength;
+    const float halo = strength / (float)SR_BLOOM_LEVELS;
+    const float scale = (float)(SR_GAMMA_LUT_SIZE - 1);
+    for (uint32_t sg = s0; sg < s1; ++sg) {
+        const uint32_t i = sg * blockDim.x + threadIdx.x;
+        if (i >= total) break;
+        if (i >= hi) {  // the next observer of this thread's run
+            const uint32_t o = find_obs(pre, n, i);
+            const ObsDev& od = obs[o];
+            lo = __ldg(pre + o);
+            hi = __ldg(pre + o + 1);
+            w = od.lw[0];
+            w1 = od.lw[1];
+            h1 = od.lh[1];
+            base0 = hdr + od.pyr_base;
+            base1 = hdr + od.pyr_base + od.loff[1];
+        }
+        const uint32_t l = i - lo, x = l % w, y = l / w;
+        const float4 up = upsample_b(base1, w1, h1, x, y);
+        const float4 c = base0[l];
+        float cx = c.x * keep + up.x * halo, cy = c.y * keep + up.y * halo, cz = c.z * keep + up.z * halo;
+        float mx = cx / (1.0f + cx * 0.35f), my = cy / (1.0f + cy * 0.35f), mz = cz / (1.0f + cz * 0.35f);
+        mx = mx < 0.0f ? 0.0f : (mx > 1.0f ? 1.0f : mx);
+        my = my < 0.0f ? 0.0f : (my > 1.0f ? 1.0f : my);
+        mz = mz < 0.0f ? 0.0f : (mz > 1.0f ? 1.0f : mz);
+        float fx = mx * scale, fy = my * scale, fz = mz * scale;
+        uint32_t ix = fx > 0.0f ? (uint32_t)fx : 0u, iy = fy > 0.0f ? (uint32_t)fy : 0u, iz = fz > 0.0f ? (uint32_t)fz : 0u;
+        rgb[i] = ((uint32_t)lut[ix] << 16) | ((uint32_t)lut[iy] << 8) | (uint32_t)lut[iz];
+    }
 }
 
 }  // namespace srk

@@ -1012,7 +1012,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
             uint32_t tot = sh.pre[(size_t)(1 + k) * stride + n];
             k_bloom_up_batch<<<(tot + 255) / 256, 256, 0, st>>>(sa.hdr, sa.obs, pre, n, k);
         }
-        const uint32_t gcomp = std::min<uint32_t>(gpx, (uint32_t)c.num_sms * 8u);
+        const uint32_t gcomp = std::min<uint32_t>(gpx, (uint32_t)c.num_sms * 6u);
         k_bloom_composite_batch<<<gcomp, 256, 0, st>>>(sa.hdr, sa.obs, pix_pre, n, rgb, sd.tables);
         if ((x = cudaGetLastError()) != cudaSuccess) return x;
         if (timed) cudaEventRecord(r.ev[4], st);
