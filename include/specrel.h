@@ -215,6 +215,34 @@ sr_status sr_scene_validate(const SrSceneDesc* desc, uint32_t* depth, char* err,
 sr_status sr_update_scene(sr_ctx* ctx, uint32_t scene_idx, const SrSceneDesc* desc, const SrRange* node_ranges,
                           uint32_t n_node_ranges, const SrRange* prim_ranges, uint32_t n_prim_ranges);
 
+/* The simplices of a scene in build order, for the build on the device. */
+typedef struct SrBuildDesc {
+    const float* boxes;               /* num_prims x 8: box min (t, x, y, z), then max (t, x, y, z) */
+    const SrGpuGeom* geoms;           /* num_prims, build order */
+    const SrGpuAttr* attrs;           /* num_prims, build order */
+    uint32_t num_prims;
+    const SrGpuMaterial* materials;
+    uint32_t num_materials;
+    uint32_t num_stars;
+    const float* stars;               /* as SrSceneDesc */
+    uint64_t num_star_vec4;
+    float light_pos[4];
+    const double* anchor;             /* optional, as SrSceneDesc */
+} SrBuildDesc;
+/* Bvh4D::build (bvh4d.rs:123-141, 287-427) and the leaf-order packing of
+ * PackedSceneGpuData::from_scene (gpu.rs:247-289) run on the device: the tree over the simplices'
+ * boxes (8-bin SAH over the four axes, the reference's partition order), the hot and cold records
+ * gathered into leaf order, then the B200 node layout. The node array and leaf order are those of
+ * the host build. Hit ids are reported in build order (the tree's leaf order is kept as
+ * leaf_to_orig). A split that leaves one side empty, where the reference selects by median,
+ * returns SR_ERR_UNSUPPORTED (build such a scene on the host and use sr_upload_scene). */
+sr_status sr_build_scene(sr_ctx* ctx, uint32_t scene_idx, const SrBuildDesc* desc);
+/* The device scene's node array and leaf order (leaf slot -> build index) read back. Either buffer
+ * may be NULL; `num_nodes` receives the node count. No counterpart in the reference (its tree
+ * lives on the host). */
+sr_status sr_scene_tree(sr_ctx* ctx, uint32_t scene_idx, SrGpuNode* nodes, uint32_t nodes_cap, uint32_t* order,
+                        uint32_t order_cap, uint32_t* num_nodes);
+
 typedef struct SrSceneStats {
     uint32_t num_nodes, num_prims, num_stars, bvh_depth;
     uint64_t device_bytes;

@@ -52,6 +52,9 @@ void sr_scene_free(sr_scene* s);
 /* Pointers into the scene's packed arrays (valid until sr_scene_free). */
 sr_status sr_scene_desc(const sr_scene* s, SrSceneDesc* out);
 sr_status sr_scene_info(const sr_scene* s, SrSynthInfo* out);
+/* The simplices' padded boxes in build order (8 floats each: min, max, (t, x, y, z)), the input of
+ * sr_build_scene; the packed arrays' leaf_to_orig maps leaf slots to this order. */
+sr_status sr_scene_boxes(const sr_scene* s, const float** boxes);
 
 /* One observer of the batched workload (configuration 4). */
 typedef struct SrObserverDraw {

@@ -138,6 +138,20 @@ class SynthScene:
     def light_pos(self):
         return tuple(self._desc.light_pos[k] for k in range(4))
 
+    def build_inputs(self):
+        """The simplices in build order, the input of Engine.build: boxes (n x 8 float32), hot and cold
+        records (from the packed leaf-order arrays through leaf_to_orig)."""
+        p = self.packed()
+        bp = C.c_void_p()
+        _check(_lib.lib().sr_scene_boxes(self.h, C.byref(bp)), what="scene_boxes")
+        n = len(p.geoms)
+        boxes = np.frombuffer((C.c_float * (8 * n)).from_address(bp.value), np.float32).reshape(n, 8).copy()
+        geoms = np.empty_like(p.geoms)
+        attrs = np.empty_like(p.attrs)
+        geoms[p.leaf_to_orig] = p.geoms
+        attrs[p.leaf_to_orig] = p.attrs
+        return boxes, geoms, attrs, p
+
     def packed(self) -> PackedScene:
         """Copies of the packed arrays as numpy (for comparisons in tests)."""
         d = self._desc
@@ -279,6 +293,41 @@ class Engine:
         d, keep = scene.desc()
         _check(self.L.sr_upload_scene(self.h, idx, C.byref(d)), self.h, "upload_scene")
         self.scenes[idx] = scene
+
+    def build(self, idx: int, boxes: np.ndarray, geoms: np.ndarray, attrs: np.ndarray, materials: np.ndarray,
+              stars: np.ndarray | None = None, num_stars: int = 0, light_pos=(0.0, 0.0, 50.0, 0.0), anchor=None) -> None:
+        """sr_build_scene: the tree and leaf order built on the device from simplices in build order."""
+        keep = [np.ascontiguousarray(boxes, np.float32), np.ascontiguousarray(geoms), np.ascontiguousarray(attrs),
+                np.ascontiguousarray(materials)]
+        d = _lib.BuildDesc()
+        d.boxes, d.geoms, d.attrs, d.materials = (a.ctypes.data for a in keep)
+        d.num_prims = len(geoms)
+        d.num_materials = len(materials)
+        if num_stars:
+            st = np.ascontiguousarray(stars, np.float32)
+            keep.append(st)
+            d.stars = st.ctypes.data
+            d.num_star_vec4 = st.size // 4
+            d.num_stars = num_stars
+        for k in range(4):
+            d.light_pos[k] = light_pos[k]
+        if anchor is not None:
+            an = np.asarray(anchor, np.float64)
+            keep.append(an)
+            d.anchor = an.ctypes.data
+        _check(self.L.sr_build_scene(self.h, idx, C.byref(d)), self.h, "build_scene")
+        self.scenes[idx] = keep
+
+    def tree(self, idx: int):
+        """The device scene's node array and leaf order (leaf slot -> build index)."""
+        nn = C.c_uint32()
+        _check(self.L.sr_scene_tree(self.h, idx, None, 0, None, 0, C.byref(nn)), self.h, "scene_tree")
+        nodes = np.zeros(nn.value, NODE_DTYPE)
+        n = self.stats(idx).num_prims
+        order = np.zeros(n, np.uint32)
+        _check(self.L.sr_scene_tree(self.h, idx, nodes.ctypes.data, nn.value, order.ctypes.data, n, C.byref(nn)),
+               self.h, "scene_tree")
+        return nodes, order
 
     def update(self, idx: int, scene, node_ranges=(), prim_ranges=()) -> None:
         d, keep = scene.desc()

@@ -62,6 +62,13 @@ class SceneDesc(C.Structure):
                 ("anchor", C.c_void_p)]
 
 
+class BuildDesc(C.Structure):
+    _fields_ = [("boxes", C.c_void_p), ("geoms", C.c_void_p), ("attrs", C.c_void_p), ("num_prims", C.c_uint32),
+                ("materials", C.c_void_p), ("num_materials", C.c_uint32), ("num_stars", C.c_uint32),
+                ("stars", C.c_void_p), ("num_star_vec4", C.c_uint64), ("light_pos", C.c_float * 4),
+                ("anchor", C.c_void_p)]
+
+
 class Range(C.Structure):
     _fields_ = [("start", C.c_uint64), ("end", C.c_uint64)]
 
@@ -159,6 +166,10 @@ SIGNATURES = {
     "sr_synchronize": (C.c_int32, [C.c_void_p]),
     "sr_scene_validate": (C.c_int32, [C.POINTER(SceneDesc), C.POINTER(C.c_uint32), C.c_char_p, C.c_size_t]),
     "sr_upload_scene": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(SceneDesc)]),
+    "sr_build_scene": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(BuildDesc)]),
+    "sr_scene_tree": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                  C.POINTER(C.c_uint32)]),
+    "sr_scene_boxes": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "sr_update_scene": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(SceneDesc), C.POINTER(Range), C.c_uint32,
                                     C.POINTER(Range), C.c_uint32]),
     "sr_scene_stats": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(SceneStats)]),

@@ -1,0 +1,26 @@
+// BVH build on the GPU (sr_build.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../../include/specrel.h"
+
+namespace srk {
+
+struct GpuBuildInfo {
+    uint32_t num_nodes, depth, max_leaf;
+    uint32_t unsupported;  // a split left one side empty (the reference selects by median there)
+};
+
+// Builds the reference's tree over n simplex boxes (device, build order; box i is box[2i] = min,
+// box[2i + 1] = max, (t, x, y, z)): nodes (device, room for 2n) in depth-first order, order[i] =
+// the build index of leaf slot i.
+cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint32_t* order, GpuBuildInfo* info,
+                          cudaStream_t st);
+
+// Hot and cold records from build order into leaf order (out[i] = in[order[i]]).
+cudaError_t gpu_gather_records(const uint32_t* order, uint32_t n, const SrGpuGeom* gin, const SrGpuAttr* ain,
+                               SrGpuGeom* gout, SrGpuAttr* aout, cudaStream_t st);
+
+}  // namespace srk

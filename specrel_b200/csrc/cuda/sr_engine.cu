@@ -15,6 +15,7 @@
 
 #include "../../../include/specrel.h"
 #include "../../../include/specrel_scene.h"
+#include "sr_build.h"
 #include "sr_fast.h"
 #include "sr_kernels.h"
 
@@ -300,6 +301,98 @@ sr_status sr_update_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d, const
                   ctx->stream),
        "rebuild node layout");
     CK(cudaStreamSynchronize(ctx->stream), "update sync");
+    return SR_OK;
+}
+
+sr_status sr_build_scene(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d) {
+    if (!ctx || !d) return SR_ERR_INVALID_ARGUMENT;
+    if (idx > 4096) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "scene index too large");
+    const uint32_t n = d->num_prims;
+    if (n == 0 || !d->boxes || !d->geoms || !d->attrs) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "no simplices to build");
+    // Materials and star segments are checked as sr_upload_scene checks them (no tree yet).
+    SrSceneDesc v{};
+    v.num_prims = n;
+    v.geoms = d->geoms;
+    v.attrs = d->attrs;
+    v.materials = d->materials;
+    v.num_materials = d->num_materials;
+    v.num_stars = d->num_stars;
+    v.stars = d->stars;
+    v.num_star_vec4 = d->num_star_vec4;
+    uint32_t unused_depth = 0;
+    char why[256] = {0};
+    if (sr_scene_validate(&v, &unused_depth, why, sizeof(why)) != SR_OK)
+        return fail(ctx, SR_ERR_BAD_SCENE, std::string("invalid scene: ") + why);
+    CK(cudaSetDevice(ctx->device), "set device");
+    if (ctx->scenes.size() <= idx) ctx->scenes.resize(idx + 1);
+    auto slot = std::make_unique<SceneSlot>();
+    SceneSlot& s = *slot;
+    cudaStream_t st = ctx->stream;
+    {
+        DevBuf box, gin, ain;
+        CK(box.ensure((size_t)n * 32), "alloc boxes");
+        CK(gin.ensure((size_t)n * sizeof(SrGpuGeom)), "alloc geoms");
+        CK(ain.ensure((size_t)n * sizeof(SrGpuAttr)), "alloc attrs");
+        CK(cudaMemcpyAsync(box.p, d->boxes, (size_t)n * 32, cudaMemcpyHostToDevice, st), "upload boxes");
+        CK(cudaMemcpyAsync(gin.p, d->geoms, (size_t)n * sizeof(SrGpuGeom), cudaMemcpyHostToDevice, st), "upload geoms");
+        CK(cudaMemcpyAsync(ain.p, d->attrs, (size_t)n * sizeof(SrGpuAttr), cudaMemcpyHostToDevice, st), "upload attrs");
+        CK(s.nodes.ensure((size_t)2 * n * sizeof(SrGpuNode)), "alloc nodes");
+        CK(s.l2o.ensure((size_t)n * 4), "alloc order");
+        GpuBuildInfo info{};
+        CK(gpu_bvh_build(box.as<float4>(), n, s.nodes.as<SrGpuNode>(), s.l2o.as<uint32_t>(), &info, st), "build tree");
+        if (info.unsupported)
+            return fail(ctx, SR_ERR_UNSUPPORTED,
+                        "a split left one side empty: the reference selects by median there; build this scene on the host");
+        CK(s.geoms.ensure((size_t)n * sizeof(SrGpuGeom)), "alloc geoms");
+        CK(s.attrs.ensure((size_t)n * sizeof(SrGpuAttr)), "alloc attrs");
+        CK(gpu_gather_records(s.l2o.as<uint32_t>(), n, gin.as<SrGpuGeom>(), ain.as<SrGpuAttr>(), s.geoms.as<SrGpuGeom>(),
+                              s.attrs.as<SrGpuAttr>(), st),
+           "leaf order");
+        CK(cudaStreamSynchronize(st), "build sync");
+        s.num_nodes = info.num_nodes;
+        s.depth = info.depth;
+        s.has_l2o = true;
+        s.num_prims = n;
+        CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, s.depth, n, info.max_leaf, st),
+           "build node layout");
+    }
+    auto up = [&](DevBuf& b, const void* src, size_t bytes) -> cudaError_t {
+        cudaError_t e = b.ensure(std::max<size_t>(bytes, 16));
+        if (e != cudaSuccess || !bytes) return e;
+        return cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice);
+    };
+    CK(up(s.mats, d->materials, (size_t)d->num_materials * sizeof(SrGpuMaterial)), "upload materials");
+    CK(up(s.stars, d->stars, (size_t)d->num_star_vec4 * 16), "upload stars");
+    s.num_mats = d->num_materials;
+    s.num_stars = d->num_stars;
+    s.num_star_vec4 = d->num_star_vec4;
+    for (int k = 0; k < 4; ++k) {
+        s.light_pos[k] = d->light_pos[k];
+        s.anchor[k] = d->anchor ? d->anchor[k] : 0.0;
+    }
+    s.tuning = fast_default_tuning(ctx->fast);
+    CK(cudaStreamSynchronize(st), "build sync");
+    s.present = true;
+    ctx->scenes[idx] = std::move(slot);
+    return SR_OK;
+}
+
+sr_status sr_scene_tree(sr_ctx* ctx, uint32_t idx, SrGpuNode* nodes, uint32_t nodes_cap, uint32_t* order,
+                        uint32_t order_cap, uint32_t* num_nodes) {
+    if (!ctx || !num_nodes) return SR_ERR_INVALID_ARGUMENT;
+    if (idx >= ctx->scenes.size() || !ctx->scenes[idx] || !ctx->scenes[idx]->present)
+        return fail(ctx, SR_ERR_NO_SCENE, "no scene at this index");
+    SceneSlot& s = *ctx->scenes[idx];
+    *num_nodes = s.num_nodes;
+    if (nodes) {
+        if (nodes_cap < s.num_nodes) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "node buffer too small");
+        CK(cudaMemcpy(nodes, s.nodes.p, (size_t)s.num_nodes * sizeof(SrGpuNode), cudaMemcpyDeviceToHost), "read nodes");
+    }
+    if (order) {
+        if (order_cap < s.num_prims) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "order buffer too small");
+        if (s.has_l2o) CK(cudaMemcpy(order, s.l2o.p, (size_t)s.num_prims * 4, cudaMemcpyDeviceToHost), "read order");
+        else for (uint32_t i = 0; i < s.num_prims; ++i) order[i] = i;
+    }
     return SR_OK;
 }
 

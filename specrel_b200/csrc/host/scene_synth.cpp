@@ -477,6 +477,7 @@ struct sr_scene {
     std::vector<SrGpuMaterial> mats;
     std::vector<float> stars;
     std::vector<uint32_t> order;
+    std::vector<float> boxes;  // build order: min (t, x, y, z), max (t, x, y, z) per simplex
     uint32_t num_stars = 0;
     double anchor[4] = {0, 0, 0, 0};
     SrSynthInfo info{};
@@ -664,6 +665,11 @@ extern "C" sr_status sr_scene_synth(const SrSynthParams* p, sr_scene** out, char
     tets.reserve(n);
     for (auto& v : per_body) { tets.insert(tets.end(), v.begin(), v.end()); std::vector<Tet>().swap(v); }
 
+    sc->boxes.resize(8 * n);
+    for (size_t i = 0; i < n; ++i) {
+        put4(&sc->boxes[8 * i], tets[i].box.lo);
+        put4(&sc->boxes[8 * i + 4], tets[i].box.hi);
+    }
     // BVH.
     std::vector<Ref> refs(n);
     for (size_t i = 0; i < n; ++i) refs[i] = {tets[i].box, (tets[i].box.lo + tets[i].box.hi) * 0.5f, (uint32_t)i};
@@ -730,6 +736,12 @@ extern "C" sr_status sr_scene_desc(const sr_scene* s, SrSceneDesc* d) {
     d->light_pos[3] = 0.0f;
     d->leaf_to_orig = s->order.data();
     d->anchor = s->anchor;
+    return SR_OK;
+}
+
+extern "C" sr_status sr_scene_boxes(const sr_scene* s, const float** boxes) {
+    if (!s || !boxes) return SR_ERR_INVALID_ARGUMENT;
+    *boxes = s->boxes.empty() ? nullptr : s->boxes.data();
     return SR_OK;
 }
 

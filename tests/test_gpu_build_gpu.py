@@ -1,0 +1,63 @@
+"""The scene build on the device (sr_build_scene): Bvh4D::build and the leaf-order packing run on
+the GPU from the simplices in build order. The node array and the leaf order must equal the host
+build's byte for byte (the host builder is itself bit-exact with the oracle's restatement of the
+reference's build), and frames rendered from the device-built scene must equal frames from the
+uploaded one."""
+import os
+import time
+
+import numpy as np
+import pytest
+
+import specrel_b200 as sr
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    dict(config=1, seed=1),
+    dict(config=1, seed=2),
+    dict(config=2, seed=4, n_bodies=24, steps=24),
+    dict(config=5, seed=1, n_stars=2000),
+]
+
+
+def _build_and_compare(engine, idx, scene):
+    boxes, geoms, attrs, p = scene.build_inputs()
+    t0 = time.perf_counter()
+    engine.build(idx, boxes, geoms, attrs, p.materials, p.stars, p.num_stars, p.light_pos, p.anchor)
+    t_gpu = time.perf_counter() - t0
+    nodes, order = engine.tree(idx)
+    assert len(nodes) == len(p.nodes)
+    assert nodes.tobytes() == p.nodes.tobytes()
+    assert (order == p.leaf_to_orig).all()
+    return t_gpu
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
+def test_device_build_equals_host_build(engine, case):
+    scene = sr.synth_scene(**case)
+    t_gpu = _build_and_compare(engine, 21, scene)
+    print(case, "prims", scene.num_prims, "nodes", scene.num_nodes, f"host build {scene.info.build_seconds:.3f} s,"
+          f" device build (with uploads) {t_gpu:.3f} s")
+    # Frames from the device-built scene equal frames from the uploaded scene.
+    engine.upload(22, scene)
+    u = sr.uniforms(sr.camera(rapidity=tuple(scene.info.cam_rapidity)), 320, 200, 0, 1, 0,
+                    num_nodes=scene.num_nodes, num_stars=scene.num_stars)
+    for path in (sr.SR_PATH_FAST, sr.SR_PATH_PLAIN):
+        a = engine.render(21, u, path=path, aux=True)
+        b = engine.render(22, u, path=path, aux=True)
+        assert (a.rgb == b.rgb).all() and (a.hit_id == b.hit_id).all() and (a.lam == b.lam).all()
+
+
+def test_device_build_full_size(engine):
+    """configs[1] at full size: 7.9M simplices."""
+    scene = sr.synth_scene(2, 1, threads=os.cpu_count())
+    t_gpu = _build_and_compare(engine, 21, scene)
+    print("7.9M tets: host build", f"{scene.info.build_seconds:.2f} s (synthesis, extrusion and tree),",
+          f"device build {t_gpu:.3f} s (uploads, tree, leaf order and node layout)")
+
+
+def test_device_build_rejects_empty(engine):
+    with pytest.raises(sr.SrError):
+        engine.build(21, np.zeros((0, 8), np.float32), np.zeros(0, sr.GEOM_DTYPE), np.zeros(0, sr.ATTR_DTYPE),
+                     sr.synth_scene(1, 1).packed().materials)
