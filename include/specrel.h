@@ -237,11 +237,44 @@ typedef struct SrBuildDesc {
  * leaf_to_orig). A split that leaves one side empty, where the reference selects by median,
  * returns SR_ERR_UNSUPPORTED (build such a scene on the host and use sr_upload_scene). */
 sr_status sr_build_scene(sr_ctx* ctx, uint32_t scene_idx, const SrBuildDesc* desc);
+/* Worldtubes for the build on the device: a body's mesh swept along its sampled worldline
+ * (extend_worldtube_simplices, mesh4d.rs:721-854; static geometry). */
+typedef struct SrTubeTriangle {       /* Triangle3D (mesh4d.rs:438-443) */
+    uint32_t idx[3];
+    float uv[3][2];
+    float normal[3];                  /* (x, y, z) */
+} SrTubeTriangle;
+typedef struct SrTubeSample {         /* WorldlineSample (mesh4d.rs:615-630) */
+    float center[4];                  /* (t, x, y, z) */
+    float tetrad[4][4];               /* e0..e3, each (t, x, y, z) */
+    float proper_time;
+    float phi[3];                     /* proper-time gradient in the body frame */
+    float accel[3];                   /* proper acceleration in the body frame */
+    float pad;
+} SrTubeSample;
+typedef struct SrTube {
+    const float* vertices;            /* num_vertices x (x, y, z), body frame */
+    uint32_t num_vertices;
+    uint32_t num_triangles;
+    const SrTubeTriangle* triangles;
+    const SrTubeSample* samples;
+    uint32_t num_samples;
+    uint32_t material;
+} SrTube;
+/* The whole scene build on the device: the worldtubes' simplices (Simplex4D::new, mesh4d.rs:312-371,
+ * the Dompierre split of each triangle between consecutive samples, degenerate tetrahedra skipped)
+ * in tube order, then the tree and packing of sr_build_scene. `rest` supplies materials, stars,
+ * light_pos and anchor (its boxes, geoms and attrs are not used). The records equal the host
+ * builder's bit for bit. */
+sr_status sr_build_scene_tubes(sr_ctx* ctx, uint32_t scene_idx, const SrTube* tubes, uint32_t num_tubes,
+                               const SrBuildDesc* rest);
 /* The device scene's node array and leaf order (leaf slot -> build index) read back. Either buffer
  * may be NULL; `num_nodes` receives the node count. No counterpart in the reference (its tree
  * lives on the host). */
 sr_status sr_scene_tree(sr_ctx* ctx, uint32_t scene_idx, SrGpuNode* nodes, uint32_t nodes_cap, uint32_t* order,
                         uint32_t order_cap, uint32_t* num_nodes);
+/* The device scene's hot and cold records (leaf order) read back; either buffer may be NULL. */
+sr_status sr_scene_records(sr_ctx* ctx, uint32_t scene_idx, SrGpuGeom* geoms, SrGpuAttr* attrs, uint32_t cap);
 
 typedef struct SrSceneStats {
     uint32_t num_nodes, num_prims, num_stars, bvh_depth;

@@ -55,6 +55,9 @@ sr_status sr_scene_info(const sr_scene* s, SrSynthInfo* out);
 /* The simplices' padded boxes in build order (8 floats each: min, max, (t, x, y, z)), the input of
  * sr_build_scene; the packed arrays' leaf_to_orig maps leaf slots to this order. */
 sr_status sr_scene_boxes(const sr_scene* s, const float** boxes);
+/* The scene's worldtubes (meshes, samples and materials of its bodies, in build order), the input
+ * of sr_build_scene_tubes (valid until sr_scene_free). */
+sr_status sr_scene_tubes(const sr_scene* s, const SrTube** tubes, uint32_t* num_tubes);
 
 /* One observer of the batched workload (configuration 4). */
 typedef struct SrObserverDraw {

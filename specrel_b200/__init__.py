@@ -318,6 +318,32 @@ class Engine:
         _check(self.L.sr_build_scene(self.h, idx, C.byref(d)), self.h, "build_scene")
         self.scenes[idx] = keep
 
+    def build_tubes(self, idx: int, scene: "SynthScene") -> None:
+        """sr_build_scene_tubes: the synthetic scene's worldtubes extruded, built and packed on the device."""
+        tp = C.c_void_p()
+        nt = C.c_uint32()
+        _check(_lib.lib().sr_scene_tubes(scene.h, C.byref(tp), C.byref(nt)), what="scene_tubes")
+        sd = scene._desc  # the scene's own arrays: materials, stars, light and anchor
+        d = _lib.BuildDesc()
+        d.materials = sd.materials
+        d.num_materials = sd.num_materials
+        d.stars = sd.stars
+        d.num_star_vec4 = sd.num_star_vec4
+        d.num_stars = sd.num_stars
+        for k in range(4):
+            d.light_pos[k] = sd.light_pos[k]
+        d.anchor = sd.anchor
+        _check(self.L.sr_build_scene_tubes(self.h, idx, tp, nt.value, C.byref(d)), self.h, "build_scene_tubes")
+        self.scenes[idx] = scene
+
+    def records(self, idx: int):
+        """The device scene's hot and cold records (leaf order)."""
+        n = self.stats(idx).num_prims
+        g = np.zeros(n, GEOM_DTYPE)
+        a = np.zeros(n, ATTR_DTYPE)
+        _check(self.L.sr_scene_records(self.h, idx, g.ctypes.data, a.ctypes.data, n), self.h, "scene_records")
+        return g, a
+
     def tree(self, idx: int):
         """The device scene's node array and leaf order (leaf slot -> build index)."""
         nn = C.c_uint32()

@@ -170,6 +170,9 @@ SIGNATURES = {
     "sr_scene_tree": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
                                   C.POINTER(C.c_uint32)]),
     "sr_scene_boxes": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "sr_scene_tubes": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint32)]),
+    "sr_build_scene_tubes": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.POINTER(BuildDesc)]),
+    "sr_scene_records": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32]),
     "sr_update_scene": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(SceneDesc), C.POINTER(Range), C.c_uint32,
                                     C.POINTER(Range), C.c_uint32]),
     "sr_scene_stats": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(SceneStats)]),

@@ -19,6 +19,16 @@ struct GpuBuildInfo {
 cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint32_t* order, GpuBuildInfo* info,
                           cudaStream_t st);
 
+// The simplices of worldtubes (build order) extruded on the device: records and boxes in device
+// buffers the caller frees (cudaFree), num_prims of them.
+struct ExtrudeOut {
+    SrGpuGeom* geoms;
+    SrGpuAttr* attrs;
+    float4* boxes;
+    uint32_t num_prims;
+};
+cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out, cudaStream_t st);
+
 // Hot and cold records from build order into leaf order (out[i] = in[order[i]]).
 cudaError_t gpu_gather_records(const uint32_t* order, uint32_t n, const SrGpuGeom* gin, const SrGpuAttr* ain,
                                SrGpuGeom* gout, SrGpuAttr* aout, cudaStream_t st);

@@ -304,58 +304,33 @@ sr_status sr_update_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d, const
     return SR_OK;
 }
 
-sr_status sr_build_scene(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d) {
-    if (!ctx || !d) return SR_ERR_INVALID_ARGUMENT;
-    if (idx > 4096) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "scene index too large");
-    const uint32_t n = d->num_prims;
-    if (n == 0 || !d->boxes || !d->geoms || !d->attrs) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "no simplices to build");
-    // Materials and star segments are checked as sr_upload_scene checks them (no tree yet).
-    SrSceneDesc v{};
-    v.num_prims = n;
-    v.geoms = d->geoms;
-    v.attrs = d->attrs;
-    v.materials = d->materials;
-    v.num_materials = d->num_materials;
-    v.num_stars = d->num_stars;
-    v.stars = d->stars;
-    v.num_star_vec4 = d->num_star_vec4;
-    uint32_t unused_depth = 0;
-    char why[256] = {0};
-    if (sr_scene_validate(&v, &unused_depth, why, sizeof(why)) != SR_OK)
-        return fail(ctx, SR_ERR_BAD_SCENE, std::string("invalid scene: ") + why);
-    CK(cudaSetDevice(ctx->device), "set device");
-    if (ctx->scenes.size() <= idx) ctx->scenes.resize(idx + 1);
-    auto slot = std::make_unique<SceneSlot>();
+// The tree, leaf order and node layout of a scene whose simplices (build order) are on the device.
+static sr_status finish_build(sr_ctx* ctx, SceneSlot& s, const float4* box, const SrGpuGeom* gin, const SrGpuAttr* ain,
+                              uint32_t n, cudaStream_t st) {
+    CK(s.nodes.ensure((size_t)2 * n * sizeof(SrGpuNode)), "alloc nodes");
+    CK(s.l2o.ensure((size_t)n * 4), "alloc order");
+    GpuBuildInfo info{};
+    CK(gpu_bvh_build(box, n, s.nodes.as<SrGpuNode>(), s.l2o.as<uint32_t>(), &info, st), "build tree");
+    if (info.unsupported)
+        return fail(ctx, SR_ERR_UNSUPPORTED,
+                    "a split left one side empty: the reference selects by median there; build this scene on the host");
+    CK(s.geoms.ensure((size_t)n * sizeof(SrGpuGeom)), "alloc geoms");
+    CK(s.attrs.ensure((size_t)n * sizeof(SrGpuAttr)), "alloc attrs");
+    CK(gpu_gather_records(s.l2o.as<uint32_t>(), n, gin, ain, s.geoms.as<SrGpuGeom>(), s.attrs.as<SrGpuAttr>(), st),
+       "leaf order");
+    CK(cudaStreamSynchronize(st), "build sync");
+    s.num_nodes = info.num_nodes;
+    s.depth = info.depth;
+    s.has_l2o = true;
+    s.num_prims = n;
+    CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, s.depth, n, info.max_leaf, st),
+       "build node layout");
+    return SR_OK;
+}
+
+// Materials, stars, light and anchor of a built scene; the slot goes live at `idx`.
+static sr_status finish_scene(sr_ctx* ctx, uint32_t idx, std::unique_ptr<SceneSlot> slot, const SrBuildDesc* d) {
     SceneSlot& s = *slot;
-    cudaStream_t st = ctx->stream;
-    {
-        DevBuf box, gin, ain;
-        CK(box.ensure((size_t)n * 32), "alloc boxes");
-        CK(gin.ensure((size_t)n * sizeof(SrGpuGeom)), "alloc geoms");
-        CK(ain.ensure((size_t)n * sizeof(SrGpuAttr)), "alloc attrs");
-        CK(cudaMemcpyAsync(box.p, d->boxes, (size_t)n * 32, cudaMemcpyHostToDevice, st), "upload boxes");
-        CK(cudaMemcpyAsync(gin.p, d->geoms, (size_t)n * sizeof(SrGpuGeom), cudaMemcpyHostToDevice, st), "upload geoms");
-        CK(cudaMemcpyAsync(ain.p, d->attrs, (size_t)n * sizeof(SrGpuAttr), cudaMemcpyHostToDevice, st), "upload attrs");
-        CK(s.nodes.ensure((size_t)2 * n * sizeof(SrGpuNode)), "alloc nodes");
-        CK(s.l2o.ensure((size_t)n * 4), "alloc order");
-        GpuBuildInfo info{};
-        CK(gpu_bvh_build(box.as<float4>(), n, s.nodes.as<SrGpuNode>(), s.l2o.as<uint32_t>(), &info, st), "build tree");
-        if (info.unsupported)
-            return fail(ctx, SR_ERR_UNSUPPORTED,
-                        "a split left one side empty: the reference selects by median there; build this scene on the host");
-        CK(s.geoms.ensure((size_t)n * sizeof(SrGpuGeom)), "alloc geoms");
-        CK(s.attrs.ensure((size_t)n * sizeof(SrGpuAttr)), "alloc attrs");
-        CK(gpu_gather_records(s.l2o.as<uint32_t>(), n, gin.as<SrGpuGeom>(), ain.as<SrGpuAttr>(), s.geoms.as<SrGpuGeom>(),
-                              s.attrs.as<SrGpuAttr>(), st),
-           "leaf order");
-        CK(cudaStreamSynchronize(st), "build sync");
-        s.num_nodes = info.num_nodes;
-        s.depth = info.depth;
-        s.has_l2o = true;
-        s.num_prims = n;
-        CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, s.depth, n, info.max_leaf, st),
-           "build node layout");
-    }
     auto up = [&](DevBuf& b, const void* src, size_t bytes) -> cudaError_t {
         cudaError_t e = b.ensure(std::max<size_t>(bytes, 16));
         if (e != cudaSuccess || !bytes) return e;
@@ -371,9 +346,97 @@ sr_status sr_build_scene(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d) {
         s.anchor[k] = d->anchor ? d->anchor[k] : 0.0;
     }
     s.tuning = fast_default_tuning(ctx->fast);
-    CK(cudaStreamSynchronize(st), "build sync");
+    CK(cudaStreamSynchronize(ctx->stream), "build sync");
     s.present = true;
+    if (ctx->scenes.size() <= idx) ctx->scenes.resize(idx + 1);
     ctx->scenes[idx] = std::move(slot);
+    return SR_OK;
+}
+
+// Materials and star segments checked as sr_upload_scene checks them (no tree yet).
+static sr_status check_build_desc(sr_ctx* ctx, const SrBuildDesc* d, const SrGpuAttr* host_attrs, uint32_t n) {
+    SrSceneDesc v{};
+    v.num_prims = host_attrs ? n : 0;
+    v.attrs = host_attrs;
+    v.geoms = host_attrs ? d->geoms : nullptr;
+    v.materials = d->materials;
+    v.num_materials = d->num_materials;
+    v.num_stars = d->num_stars;
+    v.stars = d->stars;
+    v.num_star_vec4 = d->num_star_vec4;
+    uint32_t unused_depth = 0;
+    char why[256] = {0};
+    if (sr_scene_validate(&v, &unused_depth, why, sizeof(why)) != SR_OK)
+        return fail(ctx, SR_ERR_BAD_SCENE, std::string("invalid scene: ") + why);
+    return SR_OK;
+}
+
+sr_status sr_build_scene(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d) {
+    if (!ctx || !d) return SR_ERR_INVALID_ARGUMENT;
+    if (idx > 4096) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "scene index too large");
+    const uint32_t n = d->num_prims;
+    if (n == 0 || !d->boxes || !d->geoms || !d->attrs) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "no simplices to build");
+    sr_status r = check_build_desc(ctx, d, d->attrs, n);
+    if (r != SR_OK) return r;
+    CK(cudaSetDevice(ctx->device), "set device");
+    auto slot = std::make_unique<SceneSlot>();
+    cudaStream_t st = ctx->stream;
+    {
+        DevBuf box, gin, ain;
+        CK(box.ensure((size_t)n * 32), "alloc boxes");
+        CK(gin.ensure((size_t)n * sizeof(SrGpuGeom)), "alloc geoms");
+        CK(ain.ensure((size_t)n * sizeof(SrGpuAttr)), "alloc attrs");
+        CK(cudaMemcpyAsync(box.p, d->boxes, (size_t)n * 32, cudaMemcpyHostToDevice, st), "upload boxes");
+        CK(cudaMemcpyAsync(gin.p, d->geoms, (size_t)n * sizeof(SrGpuGeom), cudaMemcpyHostToDevice, st), "upload geoms");
+        CK(cudaMemcpyAsync(ain.p, d->attrs, (size_t)n * sizeof(SrGpuAttr), cudaMemcpyHostToDevice, st), "upload attrs");
+        r = finish_build(ctx, *slot, box.as<float4>(), gin.as<SrGpuGeom>(), ain.as<SrGpuAttr>(), n, st);
+        if (r != SR_OK) return r;
+    }
+    return finish_scene(ctx, idx, std::move(slot), d);
+}
+
+sr_status sr_build_scene_tubes(sr_ctx* ctx, uint32_t idx, const SrTube* tubes, uint32_t num_tubes, const SrBuildDesc* d) {
+    if (!ctx || !d || (!tubes && num_tubes)) return SR_ERR_INVALID_ARGUMENT;
+    if (idx > 4096) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "scene index too large");
+    for (uint32_t b = 0; b < num_tubes; ++b) {
+        const SrTube& t = tubes[b];
+        if ((t.num_vertices && !t.vertices) || (t.num_triangles && !t.triangles) || (t.num_samples && !t.samples))
+            return fail(ctx, SR_ERR_INVALID_ARGUMENT, "tube " + std::to_string(b) + ": null array");
+        if (t.material >= d->num_materials)
+            return fail(ctx, SR_ERR_BAD_SCENE, "tube " + std::to_string(b) + ": material id out of range");
+        for (uint32_t i = 0; i < t.num_triangles; ++i)
+            for (int k = 0; k < 3; ++k)
+                if (t.triangles[i].idx[k] >= t.num_vertices)
+                    return fail(ctx, SR_ERR_BAD_SCENE, "tube " + std::to_string(b) + ": vertex index out of range");
+        if ((uint64_t)t.num_samples * t.num_vertices > 0xFFFFFFFFull || (uint64_t)t.num_samples * t.num_triangles > 0x3FFFFFFFull)
+            return fail(ctx, SR_ERR_INVALID_ARGUMENT, "tube " + std::to_string(b) + ": too many samples");
+    }
+    sr_status r = check_build_desc(ctx, d, nullptr, 0);
+    if (r != SR_OK) return r;
+    CK(cudaSetDevice(ctx->device), "set device");
+    auto slot = std::make_unique<SceneSlot>();
+    cudaStream_t st = ctx->stream;
+    ExtrudeOut ex{};
+    cudaError_t e = gpu_extrude(tubes, num_tubes, &ex, st);
+    struct Free {
+        ExtrudeOut* x;
+        ~Free() { if (x->geoms) cudaFree(x->geoms); if (x->attrs) cudaFree(x->attrs); if (x->boxes) cudaFree(x->boxes); }
+    } free_ex{&ex};
+    CK(e, "extrude");
+    if (ex.num_prims == 0) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "the tubes hold no simplices");
+    r = finish_build(ctx, *slot, ex.boxes, ex.geoms, ex.attrs, ex.num_prims, st);
+    if (r != SR_OK) return r;
+    return finish_scene(ctx, idx, std::move(slot), d);
+}
+
+sr_status sr_scene_records(sr_ctx* ctx, uint32_t idx, SrGpuGeom* geoms, SrGpuAttr* attrs, uint32_t cap) {
+    if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+    if (idx >= ctx->scenes.size() || !ctx->scenes[idx] || !ctx->scenes[idx]->present)
+        return fail(ctx, SR_ERR_NO_SCENE, "no scene at this index");
+    SceneSlot& s = *ctx->scenes[idx];
+    if (cap < s.num_prims) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "record buffer too small");
+    if (geoms) CK(cudaMemcpy(geoms, s.geoms.p, (size_t)s.num_prims * sizeof(SrGpuGeom), cudaMemcpyDeviceToHost), "read geoms");
+    if (attrs) CK(cudaMemcpy(attrs, s.attrs.p, (size_t)s.num_prims * sizeof(SrGpuAttr), cudaMemcpyDeviceToHost), "read attrs");
     return SR_OK;
 }
 

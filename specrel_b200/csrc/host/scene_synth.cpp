@@ -23,10 +23,9 @@
 
 #include "../../../include/specrel_scene.h"
 #include "sr_math.hpp"
+#include "tube_build.hpp"
 
 using namespace srh;
-using V3f = V3<float>;
-using V4f = V4<float>;
 
 namespace {
 
@@ -192,128 +191,42 @@ std::vector<Sample> accelerated_worldline(const std::function<P3(double)>& pos, 
     return out;
 }
 
-struct Box { V4f lo{INFINITY, INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY, -INFINITY}; };
-inline void grow(Box& b, const V4f& p) { b.lo = b.lo.vmin(p); b.hi = b.hi.vmax(p); }
-inline Box unite(const Box& a, const Box& b) { return {a.lo.vmin(b.lo), a.hi.vmax(b.hi)}; }
-
-struct Tet { SrGpuGeom g; SrGpuAttr a; Box box; };
-
-inline void put4(float* d, const V4f& v) { d[0] = v.t; d[1] = v.x; d[2] = v.y; d[3] = v.z; }
-inline float fbits(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
-
-// Simplex4D::new (mesh4d.rs:312-371) writing the hot record, the transposed cold record and the
-// padded box directly. Returns false for a degenerate tetrahedron.
-bool make_tet(const V4f* v, const float (*uv)[2], const V3f* tb, const float* tau, const float (*gr)[2], float uvs_u,
-              float uvs_v, const V4f& nrm, const V4f& u, uint32_t mat, float dec0, float dec1, const int* dec_sel, Tet* out) {
-    V4f e1 = v[1] - v[0], e2 = v[2] - v[0], e3 = v[3] - v[0];
-    V4f n = cross4(e1, e2, e3);
-    float nl2 = n.edot(n);
-    if (nl2 < 1e-16f) return false;
-    V4f un = n * (1.0f / std::sqrt(nl2));
-    V4f r1 = cross4(e2, e3, un), r2 = cross4(e3, e1, un), r3 = cross4(e1, e2, un);
-    float d1 = r1.edot(e1), d2 = r2.edot(e2), d3 = r3.edot(e3);
-    if (std::fabs(d1) < 1e-12f || std::fabs(d2) < 1e-12f || std::fabs(d3) < 1e-12f) return false;
-    put4(out->g.v0, v[0]);
-    put4(out->g.n, un);
-    put4(out->g.b1, r1 * (1.0f / d1));
-    put4(out->g.b2, r2 * (1.0f / d2));
-    put4(out->g.b3, r3 * (1.0f / d3));
-    SrGpuAttr& a = out->a;
-    for (int k = 0; k < 4; ++k) {
-        a.uv_u[k] = uv[k][0]; a.uv_v[k] = uv[k][1];
-        a.tb_x[k] = tb[k].x; a.tb_y[k] = tb[k].y; a.tb_z[k] = tb[k].z;
-        a.tau[k] = tau[k]; a.grad_u[k] = gr[k][0]; a.grad_v[k] = gr[k][1];
-        a.decided_at[k] = dec_sel[k] ? dec1 : dec0;
-    }
-    put4(a.normal, nrm);
-    put4(a.four_vel, u);
-    a.misc[0] = uvs_u; a.misc[1] = uvs_v; a.misc[2] = fbits(mat); a.misc[3] = 0;
-    Box b;
-    for (int k = 0; k < 4; ++k) grow(b, v[k]);
-    V4f eps(1e-4f, 1e-4f, 1e-4f, 1e-4f);
-    b.lo -= eps;
-    b.hi += eps;
-    out->box = b;
-    return true;
+// extend_worldtube_simplices (mesh4d.rs:721-854), static geometry (decided_at = -1e9): the
+// worldtube's events at every sample, then the three tetrahedra of each triangle between
+// consecutive samples (tube_segment, shared with the device build).
+TubeSample tube_sample(const Sample& smp) {
+    TubeSample t;
+    t.center = smp.center;
+    t.tau = smp.tau;
+    t.phi = smp.phi;
+    t.accel = smp.accel;
+    for (int k = 0; k < 4; ++k) t.e[k] = smp.tet.e[k];
+    return t;
 }
 
-// extend_worldtube_simplices (mesh4d.rs:721-854), static geometry (decided_at = -1e9).
 bool extrude(std::vector<Tet>& out, const Mesh& mesh, const std::vector<Sample>& s, uint32_t mat) {
-    const float DEC = -1.0e9f;
     size_t nv = mesh.v.size();
     bool rindler_ok = true;
+    std::vector<TubeSample> ts;
+    for (auto& smp : s) ts.push_back(tube_sample(smp));
     std::vector<V4f> ev;
     ev.reserve(s.size() * nv);
-    for (auto& smp : s)
+    for (auto& smp : ts)
         for (auto& p : mesh.v) {
             if (!(1.0f + smp.accel.dot(p) > 0.0f)) rindler_ok = false;
-            ev.push_back(smp.center + smp.tet.local_spatial_to_world(p));
+            ev.push_back(smp.center + to_world(smp, p));
         }
-    struct TT { uint32_t idx[3]; V3f p[3]; float uv[3][2]; V3f bary[3]; V3f tu, tv, normal; };
-    std::vector<TT> tt;
-    for (auto& tr : mesh.tris) {  // TubeTriangle::new (mesh4d.rs:678-717)
-        TT t;
-        int perm[3] = {0, 1, 2};
-        std::stable_sort(perm, perm + 3, [&](int a, int b) { return tr.idx[a] < tr.idx[b]; });
-        const V3f sb[3] = {V3f(1, 0, 0), V3f(0, 1, 0), V3f(0, 0, 1)};
-        for (int k = 0; k < 3; ++k) {
-            t.idx[k] = tr.idx[perm[k]];
-            t.p[k] = mesh.v[t.idx[k]];
-            t.uv[k][0] = tr.uv[perm[k]][0];
-            t.uv[k][1] = tr.uv[perm[k]][1];
-            t.bary[k] = sb[perm[k]];
-        }
-        V3f dp1 = t.p[1] - t.p[0], dp2 = t.p[2] - t.p[0];
-        float du1 = t.uv[1][0] - t.uv[0][0], dv1 = t.uv[1][1] - t.uv[0][1];
-        float du2 = t.uv[2][0] - t.uv[0][0], dv2 = t.uv[2][1] - t.uv[0][1];
-        float det = du1 * dv2 - dv1 * du2;
-        if (std::fabs(det) > 1e-10f) {
-            float inv = 1.0f / det;
-            t.tu = (dp1 * dv2 - dp2 * dv1) * inv;
-            t.tv = (dp2 * du1 - dp1 * du2) * inv;
-        }
-        t.normal = tr.normal;
-        tt.push_back(t);
-    }
+    std::vector<TubeTri> tt;
+    for (auto& tr : mesh.tris) tt.push_back(make_tube_tri(mesh.v.data(), tr.idx, tr.uv, tr.normal));
     out.reserve(out.size() + (s.size() - 1) * 3 * tt.size());
-    for (size_t st = 0; st + 1 < s.size(); ++st) {
-        const V4f* vc = &ev[st * nv];
-        const V4f* vn = &ev[(st + 1) * nv];
-        const Sample &sc = s[st], &sn = s[st + 1];
-        V4f ur = sc.tet.e[0] + sn.tet.e[0];
-        V4f u = ur * (1.0f / std::sqrt(mx(-ur.mdot(ur), 1e-12f)));
+    for (size_t st = 0; st + 1 < s.size(); ++st)
         for (auto& t : tt) {
-            V4f a0 = vc[t.idx[0]], b0 = vc[t.idx[1]], c0 = vc[t.idx[2]];
-            V4f a1 = vn[t.idx[0]], b1 = vn[t.idx[1]], c1 = vn[t.idx[2]];
-            float ta0 = sc.tau + t.p[0].dot(sc.phi), tb0 = sc.tau + t.p[1].dot(sc.phi), tc0 = sc.tau + t.p[2].dot(sc.phi);
-            float ta1 = sn.tau + t.p[0].dot(sn.phi), tb1 = sn.tau + t.p[1].dot(sn.phi), tc1 = sn.tau + t.p[2].dot(sn.phi);
-            float uvs_u = t.tu.length(), uvs_v = t.tv.length();
-            float g0[2] = {t.tu.dot(sc.phi), t.tv.dot(sc.phi)}, g1[2] = {t.tu.dot(sn.phi), t.tv.dot(sn.phi)};
-            V4f nr = sc.tet.local_spatial_to_world(t.normal) + sn.tet.local_spatial_to_world(t.normal);
-            V4f nrm = nr * (1.0f / std::sqrt(mx(nr.mdot(nr), 1e-12f)));
-            const float* UA = t.uv[0]; const float* UB = t.uv[1]; const float* UC = t.uv[2];
-            // The Dompierre split (mesh4d.rs:801-830): (A0,B0,C0,C1), (A0,B0,B1,C1), (A0,A1,B1,C1).
-            const V4f V[3][4] = {{a0, b0, c0, c1}, {a0, b0, b1, c1}, {a0, a1, b1, c1}};
-            const float* UVp[3][4] = {{UA, UB, UC, UC}, {UA, UB, UB, UC}, {UA, UA, UB, UC}};
-            const V3f TB[3][4] = {{t.bary[0], t.bary[1], t.bary[2], t.bary[2]},
-                                  {t.bary[0], t.bary[1], t.bary[1], t.bary[2]},
-                                  {t.bary[0], t.bary[0], t.bary[1], t.bary[2]}};
-            const float TAU[3][4] = {{ta0, tb0, tc0, tc1}, {ta0, tb0, tb1, tc1}, {ta0, ta1, tb1, tc1}};
-            const int SEL[3][4] = {{0, 0, 0, 1}, {0, 0, 1, 1}, {0, 1, 1, 1}};
-            for (int k = 0; k < 3; ++k) {
-                float uv[4][2], gr[4][2];
-                for (int j = 0; j < 4; ++j) {
-                    uv[j][0] = UVp[k][j][0];
-                    uv[j][1] = UVp[k][j][1];
-                    const float* g = SEL[k][j] ? g1 : g0;
-                    gr[j][0] = g[0];
-                    gr[j][1] = g[1];
-                }
-                Tet tet;
-                if (make_tet(V[k], uv, TB[k], TAU[k], gr, uvs_u, uvs_v, nrm, u, mat, DEC, DEC, SEL[k], &tet)) out.push_back(tet);
-            }
+            Tet tet[3];
+            bool ok[3];
+            tube_segment(t, &ev[st * nv], &ev[(st + 1) * nv], ts[st], ts[st + 1], mat, tet, ok);
+            for (int k = 0; k < 3; ++k)
+                if (ok[k]) out.push_back(tet[k]);
         }
-    }
     return rindler_ok;
 }
 
@@ -478,6 +391,14 @@ struct sr_scene {
     std::vector<float> stars;
     std::vector<uint32_t> order;
     std::vector<float> boxes;  // build order: min (t, x, y, z), max (t, x, y, z) per simplex
+    struct TubeRec {
+        std::vector<float> verts;
+        std::vector<SrTubeTriangle> tris;
+        std::vector<SrTubeSample> samples;
+        uint32_t mat = 0;
+    };
+    std::vector<TubeRec> tube_recs;  // the bodies' worldtubes (sr_scene_tubes)
+    std::vector<SrTube> tubes;
     uint32_t num_stars = 0;
     double anchor[4] = {0, 0, 0, 0};
     SrSynthInfo info{};
@@ -544,7 +465,28 @@ extern "C" sr_status sr_scene_synth(const SrSynthParams* p, sr_scene** out, char
     auto sc = std::make_unique<sr_scene>();
     Rng rng{p->seed};
     std::vector<std::vector<Tet>> per_body(p->n_bodies);
-    std::vector<std::function<bool(std::vector<Tet>&)>> jobs;
+    using TubeRec = sr_scene::TubeRec;
+    // A body's worldtube as recorded for sr_scene_tubes.
+    auto record = [](TubeRec& rec, const Mesh& m, const std::vector<Sample>& smp, uint32_t mat) {
+        for (auto& v : m.v) { rec.verts.push_back(v.x); rec.verts.push_back(v.y); rec.verts.push_back(v.z); }
+        for (auto& t : m.tris) {
+            SrTubeTriangle x{};
+            for (int k = 0; k < 3; ++k) { x.idx[k] = t.idx[k]; x.uv[k][0] = t.uv[k][0]; x.uv[k][1] = t.uv[k][1]; }
+            x.normal[0] = t.normal.x; x.normal[1] = t.normal.y; x.normal[2] = t.normal.z;
+            rec.tris.push_back(x);
+        }
+        for (auto& q : smp) {
+            SrTubeSample x{};
+            put4(x.center, q.center);
+            for (int k = 0; k < 4; ++k) put4(x.tetrad[k], q.tet.e[k]);
+            x.proper_time = q.tau;
+            x.phi[0] = q.phi.x; x.phi[1] = q.phi.y; x.phi[2] = q.phi.z;
+            x.accel[0] = q.accel.x; x.accel[1] = q.accel.y; x.accel[2] = q.accel.z;
+            rec.samples.push_back(x);
+        }
+        rec.mat = mat;
+    };
+    std::vector<std::function<bool(std::vector<Tet>&, TubeRec&)>> jobs;
     // A body that would enclose or graze the observer standing at the spatial origin (within its
     // radius + 1 of it at the lab times -5, -4.9, ..., 0) is drawn again.
     auto clear_of_observer = [](const std::function<P3(double)>& pos, double dist) {
@@ -592,8 +534,11 @@ extern "C" sr_status sr_scene_synth(const SrSynthParams* p, sr_scene** out, char
             if (ae < a) sc->info.clamped_accel++;
             auto pos = path_of(c, d);
             uint32_t mat = mats[i % 6], steps = p->steps, subdiv = p->subdiv;
-            jobs.push_back([=](std::vector<Tet>& o) {
-                return extrude(o, icosphere_mesh(r, (int)subdiv), accelerated_worldline(pos, -100.0f, 0.0f, steps), mat);
+            jobs.push_back([=](std::vector<Tet>& o, TubeRec& rec) {
+                Mesh m = icosphere_mesh(r, (int)subdiv);
+                std::vector<Sample> smp = accelerated_worldline(pos, -100.0f, 0.0f, steps);
+                record(rec, m, smp, mat);
+                return extrude(o, m, smp, mat);
             });
         }
         double ph[3];
@@ -615,8 +560,11 @@ extern "C" sr_status sr_scene_synth(const SrSynthParams* p, sr_scene** out, char
             V3f pos((float)c[0], (float)c[1], (float)c[2]);
             V3f beta((float)(0.9 * b[0]), (float)(0.9 * b[1]), (float)(0.9 * b[2]));
             uint32_t mat = mats[i % 3], steps = p->steps;
-            jobs.push_back([=](std::vector<Tet>& o) {
-                return extrude(o, cube_mesh(0.5f), inertial_worldline(pos, beta, -100.0f, 0.0f, steps), mat);
+            jobs.push_back([=](std::vector<Tet>& o, TubeRec& rec) {
+                Mesh m = cube_mesh(0.5f);
+                std::vector<Sample> smp = inertial_worldline(pos, beta, -100.0f, 0.0f, steps);
+                record(rec, m, smp, mat);
+                return extrude(o, m, smp, mat);
             });
         }
         // Configuration 3: the same f32 scene, whose coordinates are relative to the FP64 anchor.
@@ -648,15 +596,19 @@ extern "C" sr_status sr_scene_synth(const SrSynthParams* p, sr_scene** out, char
     }
     // Extrude on worker threads; bodies are concatenated in order afterwards.
     std::vector<char> rok(jobs.size(), 1);
+    sc->tube_recs.resize(jobs.size());
     {
         std::atomic<size_t> next{0};
         std::vector<std::thread> pool;
         for (unsigned t = 0; t < std::min<size_t>(threads, jobs.size()); ++t)
             pool.emplace_back([&] {
-                for (size_t j; (j = next.fetch_add(1)) < jobs.size();) rok[j] = jobs[j](per_body[j]) ? 1 : 0;
+                for (size_t j; (j = next.fetch_add(1)) < jobs.size();) rok[j] = jobs[j](per_body[j], sc->tube_recs[j]) ? 1 : 0;
             });
         for (auto& th : pool) th.join();
     }
+    for (auto& rec : sc->tube_recs)
+        sc->tubes.push_back(SrTube{rec.verts.data(), (uint32_t)(rec.verts.size() / 3), (uint32_t)rec.tris.size(),
+                                   rec.tris.data(), rec.samples.data(), (uint32_t)rec.samples.size(), rec.mat});
     sc->info.rindler_ok = 1;
     for (char c : rok) if (!c) sc->info.rindler_ok = 0;
     size_t n = 0;
@@ -742,6 +694,13 @@ extern "C" sr_status sr_scene_desc(const sr_scene* s, SrSceneDesc* d) {
 extern "C" sr_status sr_scene_boxes(const sr_scene* s, const float** boxes) {
     if (!s || !boxes) return SR_ERR_INVALID_ARGUMENT;
     *boxes = s->boxes.empty() ? nullptr : s->boxes.data();
+    return SR_OK;
+}
+
+extern "C" sr_status sr_scene_tubes(const sr_scene* s, const SrTube** tubes, uint32_t* num_tubes) {
+    if (!s || !tubes || !num_tubes) return SR_ERR_INVALID_ARGUMENT;
+    *tubes = s->tubes.empty() ? nullptr : s->tubes.data();
+    *num_tubes = (uint32_t)s->tubes.size();
     return SR_OK;
 }
 

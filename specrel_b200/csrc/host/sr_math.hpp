@@ -7,48 +7,55 @@
 #include <cmath>
 #include <cstdint>
 
+// Also compiled for the device (the scene build kernels): the vector algebra is marked for both.
+#ifdef __CUDACC__
+#define SRH_HD __host__ __device__
+#else
+#define SRH_HD
+#endif
+
 namespace srh {
 
-template <class T> inline T mn(T a, T b) { return std::fmin(a, b); }
-template <class T> inline T mx(T a, T b) { return std::fmax(a, b); }
+template <class T> SRH_HD inline T mn(T a, T b) { return std::fmin(a, b); }
+template <class T> SRH_HD inline T mx(T a, T b) { return std::fmax(a, b); }
 
 template <class T> struct V3 {
     T x = 0, y = 0, z = 0;
     V3() = default;
-    V3(T a, T b, T c) : x(a), y(b), z(c) {}
-    T dot(const V3& o) const { return x * o.x + y * o.y + z * o.z; }
-    T length() const { return std::sqrt(dot(*this)); }
-    V3 normalized() const {
+    SRH_HD V3(T a, T b, T c) : x(a), y(b), z(c) {}
+    SRH_HD T dot(const V3& o) const { return x * o.x + y * o.y + z * o.z; }
+    SRH_HD T length() const { return std::sqrt(dot(*this)); }
+    SRH_HD V3 normalized() const {
         T l = length();
         return l > T(1e-12) ? (*this) * (T(1) / l) : V3();
     }
-    V3 operator+(const V3& o) const { return V3(x + o.x, y + o.y, z + o.z); }
-    V3 operator-(const V3& o) const { return V3(x - o.x, y - o.y, z - o.z); }
-    V3 operator*(T s) const { return V3(x * s, y * s, z * s); }
-    V3 operator/(T s) const { return (*this) * (T(1) / s); }
-    V3& operator+=(const V3& o) { x += o.x; y += o.y; z += o.z; return *this; }
+    SRH_HD V3 operator+(const V3& o) const { return V3(x + o.x, y + o.y, z + o.z); }
+    SRH_HD V3 operator-(const V3& o) const { return V3(x - o.x, y - o.y, z - o.z); }
+    SRH_HD V3 operator*(T s) const { return V3(x * s, y * s, z * s); }
+    SRH_HD V3 operator/(T s) const { return (*this) * (T(1) / s); }
+    SRH_HD V3& operator+=(const V3& o) { x += o.x; y += o.y; z += o.z; return *this; }
 };
 
 template <class T> struct V4 {
     T t = 0, x = 0, y = 0, z = 0;
     V4() = default;
-    V4(T a, T b, T c, T d) : t(a), x(b), y(c), z(d) {}
-    V3<T> sp() const { return V3<T>(x, y, z); }
-    T mdot(const V4& o) const { return -t * o.t + x * o.x + y * o.y + z * o.z; }
-    T edot(const V4& o) const { return t * o.t + x * o.x + y * o.y + z * o.z; }
-    T ax(int i) const { return i == 0 ? t : i == 1 ? x : i == 2 ? y : z; }
-    V4 vmin(const V4& o) const { return V4(mn(t, o.t), mn(x, o.x), mn(y, o.y), mn(z, o.z)); }
-    V4 vmax(const V4& o) const { return V4(mx(t, o.t), mx(x, o.x), mx(y, o.y), mx(z, o.z)); }
-    V4 operator+(const V4& o) const { return V4(t + o.t, x + o.x, y + o.y, z + o.z); }
-    V4 operator-(const V4& o) const { return V4(t - o.t, x - o.x, y - o.y, z - o.z); }
-    V4 operator*(T s) const { return V4(t * s, x * s, y * s, z * s); }
-    V4 operator-() const { return V4(-t, -x, -y, -z); }
-    V4& operator+=(const V4& o) { t += o.t; x += o.x; y += o.y; z += o.z; return *this; }
-    V4& operator-=(const V4& o) { t -= o.t; x -= o.x; y -= o.y; z -= o.z; return *this; }
+    SRH_HD V4(T a, T b, T c, T d) : t(a), x(b), y(c), z(d) {}
+    SRH_HD V3<T> sp() const { return V3<T>(x, y, z); }
+    SRH_HD T mdot(const V4& o) const { return -t * o.t + x * o.x + y * o.y + z * o.z; }
+    SRH_HD T edot(const V4& o) const { return t * o.t + x * o.x + y * o.y + z * o.z; }
+    SRH_HD T ax(int i) const { return i == 0 ? t : i == 1 ? x : i == 2 ? y : z; }
+    SRH_HD V4 vmin(const V4& o) const { return V4(mn(t, o.t), mn(x, o.x), mn(y, o.y), mn(z, o.z)); }
+    SRH_HD V4 vmax(const V4& o) const { return V4(mx(t, o.t), mx(x, o.x), mx(y, o.y), mx(z, o.z)); }
+    SRH_HD V4 operator+(const V4& o) const { return V4(t + o.t, x + o.x, y + o.y, z + o.z); }
+    SRH_HD V4 operator-(const V4& o) const { return V4(t - o.t, x - o.x, y - o.y, z - o.z); }
+    SRH_HD V4 operator*(T s) const { return V4(t * s, x * s, y * s, z * s); }
+    SRH_HD V4 operator-() const { return V4(-t, -x, -y, -z); }
+    SRH_HD V4& operator+=(const V4& o) { t += o.t; x += o.x; y += o.y; z += o.z; return *this; }
+    SRH_HD V4& operator-=(const V4& o) { t -= o.t; x -= o.x; y -= o.y; z -= o.z; return *this; }
 };
 
 // minkowski.rs:247-262.
-template <class T> inline V4<T> cross4(const V4<T>& u, const V4<T>& v, const V4<T>& w) {
+template <class T> SRH_HD inline V4<T> cross4(const V4<T>& u, const V4<T>& v, const V4<T>& w) {
     T m_xy = v.x * w.y - v.y * w.x, m_xz = v.x * w.z - v.z * w.x, m_yz = v.y * w.z - v.z * w.y;
     T m_tx = v.t * w.x - v.x * w.t, m_ty = v.t * w.y - v.y * w.t, m_tz = v.t * w.z - v.z * w.t;
     return V4<T>(u.x * m_yz - u.y * m_xz + u.z * m_xy, -(u.t * m_yz - u.y * m_tz + u.z * m_ty),

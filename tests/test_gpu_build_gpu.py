@@ -1,8 +1,8 @@
-"""The scene build on the device (sr_build_scene): Bvh4D::build and the leaf-order packing run on
-the GPU from the simplices in build order. The node array and the leaf order must equal the host
-build's byte for byte (the host builder is itself bit-exact with the oracle's restatement of the
-reference's build), and frames rendered from the device-built scene must equal frames from the
-uploaded one."""
+"""The scene build on the device. sr_build_scene: Bvh4D::build and the leaf-order packing run on the
+GPU from the simplices in build order; sr_build_scene_tubes: the worldtubes' simplices extruded on
+the GPU too. The node array, the leaf order and the records must equal the host build's byte for
+byte (the host builder is itself bit-exact with the oracle's restatement of the reference's build),
+and frames rendered from the device-built scene must equal frames from the uploaded one."""
 import os
 import time
 
@@ -49,12 +49,40 @@ def test_device_build_equals_host_build(engine, case):
         assert (a.rgb == b.rgb).all() and (a.hit_id == b.hit_id).all() and (a.lam == b.lam).all()
 
 
+def _tubes_and_compare(engine, idx, scene):
+    p = scene.packed()
+    t0 = time.perf_counter()
+    engine.build_tubes(idx, scene)
+    t_gpu = time.perf_counter() - t0
+    nodes, order = engine.tree(idx)
+    g, a = engine.records(idx)
+    assert nodes.tobytes() == p.nodes.tobytes()
+    assert (order == p.leaf_to_orig).all()
+    assert g.tobytes() == p.geoms.tobytes() and a.tobytes() == p.attrs.tobytes()
+    return t_gpu
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
+def test_device_extrusion_and_build_equal_host_build(engine, case):
+    scene = sr.synth_scene(**case)
+    t_gpu = _tubes_and_compare(engine, 23, scene)
+    print(case, f"tubes built on the device in {t_gpu:.3f} s")
+    engine.upload(22, scene)
+    u = sr.uniforms(sr.camera(rapidity=tuple(scene.info.cam_rapidity)), 320, 200, 0, 1, 0,
+                    num_nodes=scene.num_nodes, num_stars=scene.num_stars)
+    a = engine.render(23, u, path=sr.SR_PATH_FAST, aux=True)
+    b = engine.render(22, u, path=sr.SR_PATH_FAST, aux=True)
+    assert (a.rgb == b.rgb).all() and (a.hit_id == b.hit_id).all()
+
+
 def test_device_build_full_size(engine):
-    """configs[1] at full size: 7.9M simplices."""
+    """configs[1] at full size: 7.9M simplices, from build-order simplices and from worldtubes."""
     scene = sr.synth_scene(2, 1, threads=os.cpu_count())
     t_gpu = _build_and_compare(engine, 21, scene)
-    print("7.9M tets: host build", f"{scene.info.build_seconds:.2f} s (synthesis, extrusion and tree),",
-          f"device build {t_gpu:.3f} s (uploads, tree, leaf order and node layout)")
+    t_tubes = _tubes_and_compare(engine, 23, scene)
+    print("7.9M tets: host build", f"{scene.info.build_seconds:.2f} s (synthesis, extrusion and tree, host threads),",
+          f"device build {t_gpu:.3f} s from simplices (uploads, tree, leaf order, node layout),",
+          f"{t_tubes:.3f} s from worldtubes (extrusion included)")
 
 
 def test_device_build_rejects_empty(engine):
