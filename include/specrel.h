@@ -379,6 +379,8 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, u
 static_assert(sizeof(SrGpuNode) == 48, "GpuNode is 48 bytes (gpu.rs:44-51)");
 static_assert(sizeof(SrGpuGeom) == 80, "GpuGeom is 80 bytes (gpu.rs:68-74)");
 static_assert(sizeof(SrGpuAttr) == 192, "GpuAttr is 192 bytes (gpu.rs:79-92)");
+static_assert(sizeof(SrTubeTriangle) == 48, "SrTubeTriangle is 48 bytes");
+static_assert(sizeof(SrTubeSample) == 112, "SrTubeSample is 112 bytes");
 static_assert(sizeof(SrGpuMaterial) == 48, "GpuMaterial is 48 bytes (gpu.rs:96-100)");
 static_assert(sizeof(SrGpuUniforms) == 768, "GpuUniforms is 768 bytes (gpu.rs:122-144)");
 static_assert(sizeof(SrTuning) == 48, "SrTuning is 12 words");
