@@ -89,3 +89,27 @@ def test_device_build_rejects_empty(engine):
     with pytest.raises(sr.SrError):
         engine.build(21, np.zeros((0, 8), np.float32), np.zeros(0, sr.GEOM_DTYPE), np.zeros(0, sr.ATTR_DTYPE),
                      sr.synth_scene(1, 1).packed().materials)
+
+
+def test_dynamic_scale_update_and_rebuild(engine):
+    """The per-frame scene cost of the reference's dynamic mode, at its quoted size (about 12.5k
+    simplices): a dirty-range update of every array (sr_update_scene) and a full rebuild from the
+    worldtubes on the device (sr_build_scene_tubes), each timed on the host around the call; both
+    render as a fresh upload does."""
+    scene = sr.synth_scene(1, 3, n_bodies=16, steps=22)
+    p = scene.packed()
+    engine.upload(24, scene)
+    u = sr.uniforms(sr.camera(rapidity=tuple(scene.info.cam_rapidity)), 320, 200, 0, 1, 0, num_nodes=scene.num_nodes)
+    ref = engine.render(24, u, path=sr.SR_PATH_FAST).rgb
+    ts_up, ts_build = [], []
+    for _ in range(10):
+        t0 = time.perf_counter()
+        engine.update(24, scene, node_ranges=[(0, len(p.nodes))], prim_ranges=[(0, len(p.geoms))])
+        ts_up.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        engine.build_tubes(25, scene)
+        ts_build.append(time.perf_counter() - t0)
+    assert (engine.render(24, u, path=sr.SR_PATH_FAST).rgb == ref).all()
+    assert (engine.render(25, u, path=sr.SR_PATH_FAST).rgb == ref).all()
+    print(f"{scene.num_prims} simplices: dirty-range update {np.median(ts_up) * 1e3:.2f} ms, "
+          f"rebuild from worldtubes on the device {np.median(ts_build) * 1e3:.2f} ms (medians of 10)")
