@@ -235,7 +235,9 @@ typedef struct SrBuildDesc {
  * gathered into leaf order, then the B200 node layout. The node array and leaf order are those of
  * the host build. Hit ids are reported in build order (the tree's leaf order is kept as
  * leaf_to_orig). A split that leaves one side empty, where the reference selects by median,
- * returns SR_ERR_UNSUPPORTED (build such a scene on the host and use sr_upload_scene). */
+ * returns SR_ERR_UNSUPPORTED (build such a scene on the host and use sr_upload_scene). A scene
+ * already at the index is replaced, its device buffers reused when large enough (a scene rebuilt
+ * every frame allocates nothing once warm); after a failed build the index holds no scene. */
 sr_status sr_build_scene(sr_ctx* ctx, uint32_t scene_idx, const SrBuildDesc* desc);
 /* Worldtubes for the build on the device: a body's mesh swept along its sampled worldline
  * (extend_worldtube_simplices, mesh4d.rs:721-854; static geometry). */

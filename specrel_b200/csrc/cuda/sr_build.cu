@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "sr_build.h"
@@ -303,7 +304,7 @@ __global__ void k_large_events(const Chunk* chunks, const LTask* tasks, const ui
 }
 
 // One round of pointer jumping over the enqueue list (reads a, writes b).
-__global__ void k_jump(const int* item_a, const int* ref_a, int* item_b, int* ref_b, uint32_t len, uint32_t* pending) {
+__global__ void k_jump(const int* item_a, const int* ref_a, int* item_b, int* ref_b, uint32_t len) {
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= len) return;
     int it = item_a[j], rf = ref_a[j];
@@ -314,7 +315,6 @@ __global__ void k_jump(const int* item_a, const int* ref_a, int* item_b, int* re
             rf = -1;
         } else {
             rf = ref_a[rf];
-            atomicAdd(pending, 1u);
         }
     }
     item_b[j] = it;
@@ -540,14 +540,38 @@ __global__ void k_place_large(const SrGpuNode* src, const uint32_t* at, uint32_t
     if (j < cnt) nodes[at[j]] = src[j];
 }
 
+// Build scratch from the stream-ordered pool (freed in stream order when the buffer goes out of
+// scope), so that small scenes rebuilt every frame do not pay cudaMalloc / cudaFree each time.
 template <class T>
 struct Buf {
     T* p = nullptr;
-    ~Buf() { if (p) cudaFree(p); }
-    cudaError_t alloc(size_t n) { return cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)); }
+    cudaStream_t st = nullptr;
+    ~Buf() { if (p) cudaFreeAsync(p, st); }
+    cudaError_t alloc(size_t n, cudaStream_t s) {
+        st = s;
+        return cudaMallocAsync(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T), s);
+    }
 };
 
 }  // namespace
+
+// Keeps the device's stream-ordered pool from returning memory at every synchronisation (once
+// per device), so that repeated builds reuse it.
+cudaError_t keep_build_pool() {
+    static std::mutex mu;
+    static std::vector<int> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return cudaSuccess;
+    cudaMemPool_t pool;
+    if ((e = cudaDeviceGetDefaultMemPool(&pool, dev)) != cudaSuccess) return e;
+    uint64_t keep = UINT64_MAX;
+    if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+    done.push_back(dev);
+    return cudaSuccess;
+}
 
 // Hot (5 float4) and cold (12 float4) records from build order into leaf order.
 __global__ void k_gather_records(const uint32_t* order, uint32_t n, const float4* gin, const float4* ain, float4* gout,
@@ -577,17 +601,17 @@ cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint3
                           GpuBuildInfo* info, cudaStream_t st) {
     *info = GpuBuildInfo{};
     if (n == 0) return cudaSuccess;
-    cudaError_t e;
+    cudaError_t e = keep_build_pool();
+    if (e != cudaSuccess) return e;
 #define BK(x) do { if ((e = (x)) != cudaSuccess) return e; } while (0)
     Buf<float4> cen;
-    Buf<uint32_t> perm, perm2, flag, key, lb, svc, sb, pending;
+    Buf<uint32_t> perm, perm2, flag, key, lb, svc, sb;
     Buf<int> ei[2], er[2];
     Buf<SrGpuNode> tmp;
-    BK(cen.alloc(n));
-    BK(perm.alloc(n));
-    BK(perm2.alloc(n));
-    BK(tmp.alloc(2ull * n));
-    BK(pending.alloc(1));
+    BK(cen.alloc(n, st));
+    BK(perm.alloc(n, st));
+    BK(perm2.alloc(n, st));
+    BK(tmp.alloc(2ull * n, st));
     k_init_build<<<(n + 255) / 256, 256, 0, st>>>(box, n, cen.p, perm.p);
     BK(cudaGetLastError());
 
@@ -620,13 +644,13 @@ cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint3
     size_t scan_bytes = 0;
     cub::DeviceScan::ExclusiveSumByKey(nullptr, scan_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)n);
     Buf<unsigned char> scan_tmp;
-    BK(scan_tmp.alloc(scan_bytes));
-    BK(flag.alloc(n));
-    BK(key.alloc(n));
-    BK(lb.alloc(n));
-    BK(svc.alloc(n));
-    BK(sb.alloc(n));
-    for (int k = 0; k < 2; ++k) { BK(ei[k].alloc(2ull * n)); BK(er[k].alloc(2ull * n)); }
+    BK(scan_tmp.alloc(scan_bytes, st));
+    BK(flag.alloc(n, st));
+    BK(key.alloc(n, st));
+    BK(lb.alloc(n, st));
+    BK(svc.alloc(n, st));
+    BK(sb.alloc(n, st));
+    for (int k = 0; k < 2; ++k) { BK(ei[k].alloc(2ull * n, st)); BK(er[k].alloc(2ull * n, st)); }
     while (!level.empty()) {
         const uint32_t nt = (uint32_t)level.size();
         std::vector<LTask> tasks(nt);
@@ -643,10 +667,10 @@ cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint3
         Buf<Chunk> dc;
         Buf<LHead> dh;
         Buf<LBins> db;
-        BK(dt.alloc(nt));
-        BK(dc.alloc(nch));
-        BK(dh.alloc(nt));
-        BK(db.alloc(nt));
+        BK(dt.alloc(nt, st));
+        BK(dc.alloc(nch, st));
+        BK(dh.alloc(nt, st));
+        BK(db.alloc(nt, st));
         BK(cudaMemcpyAsync(dt.p, tasks.data(), nt * sizeof(LTask), cudaMemcpyHostToDevice, st));
         BK(cudaMemcpyAsync(dc.p, chunks.data(), nch * sizeof(Chunk), cudaMemcpyHostToDevice, st));
         k_init_heads<<<nt, 128, 0, st>>>(dh.p, db.p, nt);
@@ -662,17 +686,18 @@ cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint3
         BK(cudaMemsetAsync(er[0].p, 0xFF, 2ull * total * sizeof(int), st));
         k_large_events<<<nch, 256, 0, st>>>(dc.p, dt.p, perm.p, flag.p, lb.p, svc.p, sb.p, ei[0].p, er[0].p, dh.p);
         BK(cudaGetLastError());
+        // A chain of references in a node's enqueue list is shorter than the list (at most twice
+        // the node's size), and every round halves it: log2 of that many rounds resolve all.
         int cur = 0;
         const uint32_t len = 2u * total;
-        for (int round = 0; round < 64; ++round) {
-            BK(cudaMemsetAsync(pending.p, 0, 4, st));
-            k_jump<<<(len + 255) / 256, 256, 0, st>>>(ei[cur].p, er[cur].p, ei[1 - cur].p, er[1 - cur].p, len, pending.p);
+        uint32_t maxc = 0;
+        for (const LTask& tk : tasks) maxc = std::max(maxc, tk.count);
+        int rounds = 1;
+        while ((1ull << rounds) < 2ull * maxc + 2) ++rounds;
+        for (int round = 0; round <= rounds; ++round) {
+            k_jump<<<(len + 255) / 256, 256, 0, st>>>(ei[cur].p, er[cur].p, ei[1 - cur].p, er[1 - cur].p, len);
             BK(cudaGetLastError());
             cur = 1 - cur;
-            uint32_t pend = 0;
-            BK(cudaMemcpyAsync(&pend, pending.p, 4, cudaMemcpyDeviceToHost, st));
-            BK(cudaStreamSynchronize(st));
-            if (pend == 0) break;
         }
         k_large_scatter<<<nch, 256, 0, st>>>(dc.p, dt.p, dh.p, perm.p, flag.p, lb.p, ei[cur].p, perm2.p);
         k_copy_range<<<nch, 256, 0, st>>>(dc.p, dt.p, perm2.p, perm.p);
@@ -720,8 +745,8 @@ cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint3
     const uint32_t ns = (uint32_t)small.size();
     Buf<STask> dst;
     Buf<SResult> dres;
-    BK(dst.alloc(ns));
-    BK(dres.alloc(ns));
+    BK(dst.alloc(ns, st));
+    BK(dres.alloc(ns, st));
     BK(cudaMemcpyAsync(dst.p, small.data(), ns * sizeof(STask), cudaMemcpyHostToDevice, st));
     const size_t smem = 3 * SMALL * sizeof(float4) + SMALL * (sizeof(uint32_t) + sizeof(uint16_t));
     BK(cudaFuncSetAttribute(k_small_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -781,9 +806,9 @@ cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint3
     }
     Buf<SrGpuNode> dl;
     Buf<uint32_t> dlat, dsb;
-    BK(dl.alloc(lnodes.size()));
-    BK(dlat.alloc(lat.size()));
-    BK(dsb.alloc(ns));
+    BK(dl.alloc(lnodes.size(), st));
+    BK(dlat.alloc(lat.size(), st));
+    BK(dsb.alloc(ns, st));
     BK(cudaMemcpyAsync(dl.p, lnodes.data(), lnodes.size() * sizeof(SrGpuNode), cudaMemcpyHostToDevice, st));
     BK(cudaMemcpyAsync(dlat.p, lat.data(), lat.size() * 4, cudaMemcpyHostToDevice, st));
     BK(cudaMemcpyAsync(dsb.p, sbase.data(), ns * 4, cudaMemcpyHostToDevice, st));

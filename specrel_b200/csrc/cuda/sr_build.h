@@ -19,8 +19,12 @@ struct GpuBuildInfo {
 cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint32_t* order, GpuBuildInfo* info,
                           cudaStream_t st);
 
+// Keeps the current device's stream-ordered pool from returning memory at synchronisation (once).
+cudaError_t keep_build_pool();
+
 // The simplices of worldtubes (build order) extruded on the device: records and boxes in device
-// buffers the caller frees (cudaFree), num_prims of them.
+// buffers from the stream-ordered pool that the caller frees (cudaFreeAsync on the same stream),
+// num_prims of them.
 struct ExtrudeOut {
     SrGpuGeom* geoms;
     SrGpuAttr* attrs;

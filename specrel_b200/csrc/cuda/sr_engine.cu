@@ -304,6 +304,19 @@ sr_status sr_update_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d, const
     return SR_OK;
 }
 
+// The slot a build fills: the index's previous scene, whose device buffers are reused when they
+// are large enough (a scene rebuilt every frame allocates nothing once warm), else a new one. The
+// index holds no scene until the build succeeds.
+static std::unique_ptr<SceneSlot> take_slot(sr_ctx* ctx, uint32_t idx) {
+    if (idx < ctx->scenes.size() && ctx->scenes[idx]) {
+        cudaStreamSynchronize(ctx->stream);  // frames queued on the old scene finish first
+        std::unique_ptr<SceneSlot> s = std::move(ctx->scenes[idx]);
+        s->present = false;
+        return s;
+    }
+    return std::make_unique<SceneSlot>();
+}
+
 // The tree, leaf order and node layout of a scene whose simplices (build order) are on the device.
 static sr_status finish_build(sr_ctx* ctx, SceneSlot& s, const float4* box, const SrGpuGeom* gin, const SrGpuAttr* ain,
                               uint32_t n, cudaStream_t st) {
@@ -379,7 +392,7 @@ sr_status sr_build_scene(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d) {
     sr_status r = check_build_desc(ctx, d, d->attrs, n);
     if (r != SR_OK) return r;
     CK(cudaSetDevice(ctx->device), "set device");
-    auto slot = std::make_unique<SceneSlot>();
+    auto slot = take_slot(ctx, idx);
     cudaStream_t st = ctx->stream;
     {
         DevBuf box, gin, ain;
@@ -414,14 +427,19 @@ sr_status sr_build_scene_tubes(sr_ctx* ctx, uint32_t idx, const SrTube* tubes, u
     sr_status r = check_build_desc(ctx, d, nullptr, 0);
     if (r != SR_OK) return r;
     CK(cudaSetDevice(ctx->device), "set device");
-    auto slot = std::make_unique<SceneSlot>();
+    auto slot = take_slot(ctx, idx);
     cudaStream_t st = ctx->stream;
     ExtrudeOut ex{};
     cudaError_t e = gpu_extrude(tubes, num_tubes, &ex, st);
     struct Free {
         ExtrudeOut* x;
-        ~Free() { if (x->geoms) cudaFree(x->geoms); if (x->attrs) cudaFree(x->attrs); if (x->boxes) cudaFree(x->boxes); }
-    } free_ex{&ex};
+        cudaStream_t st;
+        ~Free() {
+            if (x->geoms) cudaFreeAsync(x->geoms, st);
+            if (x->attrs) cudaFreeAsync(x->attrs, st);
+            if (x->boxes) cudaFreeAsync(x->boxes, st);
+        }
+    } free_ex{&ex, st};
     CK(e, "extrude");
     if (ex.num_prims == 0) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "the tubes hold no simplices");
     r = finish_build(ctx, *slot, ex.boxes, ex.geoms, ex.attrs, ex.num_prims, st);

@@ -65,18 +65,24 @@ __global__ void k_tube_compact(uint64_t ncand, const uint32_t* valid, const uint
     }
 }
 
+// Scratch from the stream-ordered pool (see sr_build.cu).
 template <class T>
 struct DBuf {
     T* p = nullptr;
-    ~DBuf() { if (p) cudaFree(p); }
-    cudaError_t alloc(size_t n) { return cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)); }
+    cudaStream_t st = nullptr;
+    ~DBuf() { if (p) cudaFreeAsync(p, st); }
+    cudaError_t alloc(size_t n, cudaStream_t s) {
+        st = s;
+        return cudaMallocAsync(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T), s);
+    }
 };
 
 }  // namespace
 
 cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out, cudaStream_t st) {
     *out = ExtrudeOut{};
-    cudaError_t e;
+    cudaError_t e = keep_build_pool();
+    if (e != cudaSuccess) return e;
 #define EK(x) do { if ((e = (x)) != cudaSuccess) return e; } while (0)
     std::vector<BodyDev> bodies(num_tubes);
     std::vector<V3f> verts;
@@ -131,16 +137,16 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
     DBuf<SrGpuAttr> ca;
     DBuf<float4> cb;
     DBuf<uint32_t> valid, pos;
-    EK(db.alloc(num_tubes));
-    EK(dv.alloc(verts.size()));
-    EK(dt.alloc(tris.size()));
-    EK(ds.alloc(samples.size()));
-    EK(dev.alloc(nev));
-    EK(cg.alloc(ncand));
-    EK(ca.alloc(ncand));
-    EK(cb.alloc(2 * ncand));
-    EK(valid.alloc(ncand + 1));
-    EK(pos.alloc(ncand + 1));
+    EK(db.alloc(num_tubes, st));
+    EK(dv.alloc(verts.size(), st));
+    EK(dt.alloc(tris.size(), st));
+    EK(ds.alloc(samples.size(), st));
+    EK(dev.alloc(nev, st));
+    EK(cg.alloc(ncand, st));
+    EK(ca.alloc(ncand, st));
+    EK(cb.alloc(2 * ncand, st));
+    EK(valid.alloc(ncand + 1, st));
+    EK(pos.alloc(ncand + 1, st));
     EK(cudaMemcpyAsync(db.p, bodies.data(), bodies.size() * sizeof(BodyDev), cudaMemcpyHostToDevice, st));
     EK(cudaMemcpyAsync(dv.p, verts.data(), verts.size() * sizeof(V3f), cudaMemcpyHostToDevice, st));
     EK(cudaMemcpyAsync(dt.p, tris.data(), tris.size() * sizeof(TubeTri), cudaMemcpyHostToDevice, st));
@@ -153,14 +159,14 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
     size_t tmp_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, valid.p, pos.p, (int)(ncand + 1), st);
     DBuf<unsigned char> tmp;
-    EK(tmp.alloc(tmp_bytes));
+    EK(tmp.alloc(tmp_bytes, st));
     EK(cub::DeviceScan::ExclusiveSum(tmp.p, tmp_bytes, valid.p, pos.p, (int)(ncand + 1), st));
     uint32_t n = 0;
     EK(cudaMemcpyAsync(&n, pos.p + ncand, 4, cudaMemcpyDeviceToHost, st));
     EK(cudaStreamSynchronize(st));
-    EK(cudaMalloc(&out->geoms, std::max<size_t>(n, 1) * sizeof(SrGpuGeom)));
-    EK(cudaMalloc(&out->attrs, std::max<size_t>(n, 1) * sizeof(SrGpuAttr)));
-    EK(cudaMalloc(&out->boxes, std::max<size_t>(n, 1) * 2 * sizeof(float4)));
+    EK(cudaMallocAsync(reinterpret_cast<void**>(&out->geoms), std::max<size_t>(n, 1) * sizeof(SrGpuGeom), st));
+    EK(cudaMallocAsync(reinterpret_cast<void**>(&out->attrs), std::max<size_t>(n, 1) * sizeof(SrGpuAttr), st));
+    EK(cudaMallocAsync(reinterpret_cast<void**>(&out->boxes), std::max<size_t>(n, 1) * 2 * sizeof(float4), st));
     out->num_prims = n;
     k_tube_compact<<<148 * 8, 256, 0, st>>>(ncand, valid.p, pos.p, cg.p, ca.p, cb.p, out->geoms, out->attrs, out->boxes);
     EK(cudaGetLastError());

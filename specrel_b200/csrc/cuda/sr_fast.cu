@@ -78,7 +78,12 @@ void fast_release(FastCtx& c) {
 
 cudaError_t fast_build(FastCtx& c, FastScene& s, const SrGpuNode* nodes, uint32_t n, uint32_t depth, uint32_t num_prims,
                        uint32_t max_leaf, cudaStream_t st) {
-    (void)c;
+    // Captured batch graphs hold the scene's parameters (root box, octant stride, counts) and are
+    // keyed by buffer addresses that a rebuilt or re-uploaded scene can reuse: drop them all, once
+    // the launches already queued on the stream have finished.
+    cudaError_t e0 = cudaStreamSynchronize(st);
+    if (e0 != cudaSuccess) return e0;
+    fast_release(c);
     s.num_wide = 0;
     s.depth = depth;
     s.empty = n == 0;

@@ -140,3 +140,21 @@ def test_update_scene_patches_ranges(engine):
     fresh = engine.render(4, u).rgb
     assert (patched == fresh).all()
     assert n_nodes > 0 and n_prims > 0
+
+
+def test_render_update_render_uses_the_new_scene(engine):
+    """A frame rendered before sr_update_scene must not leave a captured launch sequence holding the
+    old scene's parameters (root box, layout stride, counts): after the update the frames equal a
+    fresh upload's."""
+    a = sr.synth_scene(1, 5, n_bodies=64, steps=8)
+    b = sr.synth_scene(1, 6, n_bodies=48, steps=8)  # fits a's arrays: patched in place
+    assert b.num_nodes < a.num_nodes and b.num_prims < a.num_prims
+    u = sr.uniforms(sr.camera((0.0, 0.0, 0.0, -3.0), 90.0), 160, 100, num_nodes=b.num_nodes)
+    engine.upload(6, a)
+    before = engine.render(6, u).rgb
+    engine.update(6, b, node_ranges=[(0, b.num_nodes)], prim_ranges=[(0, b.num_prims)])
+    after = engine.render(6, u).rgb
+    engine.upload(7, b)
+    fresh = engine.render(7, u).rgb
+    assert (after == fresh).all()
+    assert not (before == after).all()
