@@ -47,10 +47,11 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch parameters")
     ap.add_argument("--bodies", type=int, default=64,
                     help="icospheres in the scene (64 is the workload; fewer only for small profiling captures)")
-    ap.add_argument("--workload", choices=["config2", "config4"], default="config2",
+    ap.add_argument("--workload", choices=["config2", "config4", "config5"], default="config2",
                     help="config2: the headline (8 observers of the 7.9M-tet scene per step); config4: 64 observers "
                          "of mixed resolution and slice mode over the 147k-tet cube scene, batched against a loop "
-                         "of the plain single-frame path")
+                         "of the plain single-frame path; config5: the image-loss gradient of one 1280x800 observer "
+                         "over 100k stars and the cube occluders")
     return ap.parse_args()
 
 
@@ -478,6 +479,65 @@ def run_config4(args, rank, world, local):
     eng.close()
 
 
+def run_config5(args, rank, world, local):
+    """100k inertial stars on a sphere of radius 1e3 over the cube scene, 1280x800, target
+    rendered at rapidity (0.8, -0.3, 0.5). Times, with CUDA events on the engine's stream: one forward
+    frame on the fast path (FP64 camera, binned stars) and one loss-and-gradient evaluation
+    (sr_adjoint: the forward frame recomputed, then the 7-vector of rapidity and event derivatives in
+    f32 with f64 sums) at loss level 0 (full resolution) and level 3, from rapidity 0. One GPU."""
+    import torch
+    import specrel_b200 as sr
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    scene = sr.synth_scene(5, args.seed)
+    eng = sr.Engine(local)
+    eng.upload(0, scene)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    star = (0.8, -0.3, 0.5)
+    u = sr.uniforms(sr.camera(), W, H, 0, 1, 0, num_nodes=scene.num_nodes, num_stars=scene.num_stars,
+                    light_pos=scene.light_pos)
+    ev = (0.0, 0.0, 0.0, 0.0)
+    out = torch.empty(W * H, dtype=torch.int32, device=f"cuda:{local}")
+    with torch.cuda.stream(stream):
+        tgt = eng.render(0, u, path=sr.SR_PATH_FAST, hdr=True, cam=sr.cam64(ev, star)).hdr
+        tdev = torch.tensor(tgt, device=f"cuda:{local}").contiguous()
+        cam0 = sr.cam64(ev, (0.0, 0.0, 0.0))
+
+        def timed(fn, k):
+            for _ in range(max(1, args.warmup)):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(k):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / k
+
+        with ClockSampler(local) as clocks:
+            fwd = timed(lambda: eng.render_into(0, u, out.data_ptr(), path=sr.SR_PATH_FAST, cam=cam0), args.steps)
+            g0 = timed(lambda: eng.adjoint(0, u, cam0, tdev.data_ptr(), 0), args.steps)
+            g3 = timed(lambda: eng.adjoint(0, u, cam0, tdev.data_ptr(), 3), args.steps)
+        r = eng.adjoint(0, u, cam0, tdev.data_ptr(), 0)
+    clk = clocks.summary()
+    line = {
+        "metric": "ms per image-loss gradient on 1 B200, configs[4]: 100k stars over the cube scene, 1280x800",
+        "value": g0, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": g0,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 sums)",
+        "data": "synthetic (seeded configs[4] stars and occluders)",
+        "config": {"workload": f"configs[4]: {scene.num_prims} tets, {scene.num_stars} stars, 1280x800, target at "
+                               "rapidity (0.8, -0.3, 0.5), gradient at rapidity 0", "seed": args.seed},
+        "forward_frame_ms": fwd, "gradient_level3_ms": g3,
+        "gradient": {"loss": r.loss, "grad": list(r.grad), "star_terms": r.star_terms},
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+    }
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -487,6 +547,8 @@ def main():
         run_reference(args, rank, world)
     elif args.workload == "config4":
         run_config4(args, rank, world, local)
+    elif args.workload == "config5":
+        run_config5(args, rank, world, local)
     else:
         run_engine(args, rank, world, local)
 
