@@ -204,6 +204,12 @@ sr_status sr_synchronize(sr_ctx* ctx);
 /* GpuRenderer::upload_scene (gpu.rs:622-699): copies the packed arrays to the device, validates
  * them (child links, leaf ranges, material ids) and builds the B200 node layout on the device. */
 sr_status sr_upload_scene(sr_ctx* ctx, uint32_t scene_idx, const SrSceneDesc* desc);
+/* Whether a node is BvhNode4D::NOTHING (bvh4d.rs:31): interior, both links to node 0, and an
+ * empty box. As the root it makes the scene's tree empty (an arena before anything is written). */
+#define SR_NODE_IS_NOTHING(n)                                                                   \
+    ((n)->count == 0 && (n)->left == 0 && (n)->right_or_first == 0 &&                              \
+     ((n)->min[0] > (n)->max[0] || (n)->min[1] > (n)->max[1] || (n)->min[2] > (n)->max[2] ||       \
+      (n)->min[3] > (n)->max[3]))
 /* The host-side checks sr_upload_scene runs before copying (no device needed): child links and
  * leaf ranges in bounds, every node reached once from the root, material ids, leaf_to_orig and
  * star segment ranges in bounds. `depth` (optional) receives the tree depth. The reference's
@@ -240,7 +246,8 @@ typedef struct SrBuildDesc {
  * every frame allocates nothing once warm); after a failed build the index holds no scene. */
 sr_status sr_build_scene(sr_ctx* ctx, uint32_t scene_idx, const SrBuildDesc* desc);
 /* Worldtubes for the build on the device: a body's mesh swept along its sampled worldline
- * (extend_worldtube_simplices, mesh4d.rs:721-854; static geometry). */
+ * (extend_worldtube_simplices, mesh4d.rs:721-854), static geometry unless per-sample causal
+ * decision stamps are given (build_worldtube_simplices_with_decided, mesh4d.rs:648-660). */
 typedef struct SrTubeTriangle {       /* Triangle3D (mesh4d.rs:438-443) */
     uint32_t idx[3];
     float uv[3][2];
@@ -262,6 +269,8 @@ typedef struct SrTube {
     const SrTubeSample* samples;
     uint32_t num_samples;
     uint32_t material;
+    const float* decided_at;          /* num_samples stamps (tetrahedron corners on sample k get
+                                         decided_at[k]), or NULL: static geometry (-1e9) */
 } SrTube;
 /* The whole scene build on the device: the worldtubes' simplices (Simplex4D::new, mesh4d.rs:312-371,
  * the Dompierre split of each triangle between consecutive samples, degenerate tetrahedra skipped)
@@ -277,6 +286,52 @@ sr_status sr_scene_tree(sr_ctx* ctx, uint32_t scene_idx, SrGpuNode* nodes, uint3
                         uint32_t order_cap, uint32_t* num_nodes);
 /* The device scene's hot and cold records (leaf order) read back; either buffer may be NULL. */
 sr_status sr_scene_records(sr_ctx* ctx, uint32_t scene_idx, SrGpuGeom* geoms, SrGpuAttr* attrs, uint32_t cap);
+
+/* ---- Incremental scenes: the scene cache over a device arena -------------------------------
+ * SceneCache (dynamic/scene_cache.rs:120-356) with the arena edits of Bvh4D (bvh4d.rs:168-215,
+ * 583-644), the arena living in the scene's device arrays. A snapshot is cut into chunks, each a
+ * BVH of its own; a chunk whose inputs equal the previous snapshot's keeps its nodes and records
+ * where they are, the others are extruded (tubes) and built (all of a snapshot's new chunks in one
+ * device build) into free room of the arrays, and a tree over the chunks' roots (top_tree) goes to
+ * node 0 and free room. Once the free room exceeds half the live slots plus 16384, the chunks are
+ * moved together first (compaction, no BVH build). The node array, hot and cold records equal the
+ * reference's arena byte for byte. Hit ids are arena slots (the arena's leaf order is the
+ * identity). The scene at `scene_idx` renders as it was until sr_arena_finish, which makes the
+ * new snapshot live. A slot that does not hold this cache's arena starts afresh. */
+typedef struct SrArenaPart {          /* Part (scene_cache.rs:39-44) */
+    uint32_t kind;                    /* 0 body, 1 hull, 2 pulse */
+    uint32_t player;
+    uint64_t id;                      /* body uid, or pulse sequence number */
+} SrArenaPart;
+typedef struct SrArenaStats {         /* CacheStats (scene_cache.rs:59-70) */
+    uint32_t chunks_built, chunks_reused;
+    uint64_t simplices_built, simplices_reused;
+    uint64_t arena_simplices;         /* simplex slots in use or free */
+    uint32_t compacted;
+    uint32_t num_nodes;               /* node slots in use or free */
+    uint32_t bvh_depth;
+    uint32_t pad;
+} SrArenaStats;
+/* SceneCache::begin: start a snapshot into the arena at `scene_idx`. */
+sr_status sr_arena_begin(sr_ctx* ctx, uint32_t scene_idx);
+/* SceneCache::tube: `tube` in chunks of 1.0 lab time (by each segment's first sample, the sample at
+ * a boundary shared by both chunks); a chunk made from the same bits as last snapshot's is reused,
+ * the others are made in sr_arena_finish. The mesh's full contents stand for the reference's hash
+ * of it in the chunk's key. */
+sr_status sr_arena_tube(sr_ctx* ctx, uint32_t scene_idx, SrArenaPart part, const SrTube* tube);
+/* SceneCache::piece in two steps: `reused` is 1 when chunk (part, index) was last made from the
+ * same `key`; when 0, give its simplices (build order, as SrBuildDesc) with sr_arena_install
+ * before sr_arena_finish (a chunk never installed is empty). A chunk used twice in one snapshot is
+ * an error. */
+sr_status sr_arena_reuse(sr_ctx* ctx, uint32_t scene_idx, SrArenaPart part, int64_t index, const uint32_t* key,
+                         uint32_t key_len, int32_t* reused);
+sr_status sr_arena_install(sr_ctx* ctx, uint32_t scene_idx, SrArenaPart part, int64_t index, const float* boxes,
+                           const SrGpuGeom* geoms, const SrGpuAttr* attrs, uint32_t num_prims);
+/* SceneCache::finish: chunks unused this snapshot are dropped, new chunks built on the device and
+ * written, `desc`'s simplices (the volatile part, may be empty) built afresh as one more chunk,
+ * the tree over all chunks written, and the B200 node layout rebuilt; materials, stars, light
+ * and anchor come from `desc`. `stats` (optional) receives the snapshot's CacheStats. */
+sr_status sr_arena_finish(sr_ctx* ctx, uint32_t scene_idx, const SrBuildDesc* desc, SrArenaStats* stats);
 
 typedef struct SrSceneStats {
     uint32_t num_nodes, num_prims, num_stars, bvh_depth;
@@ -383,6 +438,8 @@ static_assert(sizeof(SrGpuGeom) == 80, "GpuGeom is 80 bytes (gpu.rs:68-74)");
 static_assert(sizeof(SrGpuAttr) == 192, "GpuAttr is 192 bytes (gpu.rs:79-92)");
 static_assert(sizeof(SrTubeTriangle) == 48, "SrTubeTriangle is 48 bytes");
 static_assert(sizeof(SrTubeSample) == 112, "SrTubeSample is 112 bytes");
+static_assert(sizeof(SrTube) == 48, "SrTube is 48 bytes");
+static_assert(sizeof(SrArenaPart) == 16 && sizeof(SrArenaStats) == 48, "arena structs");
 static_assert(sizeof(SrGpuMaterial) == 48, "GpuMaterial is 48 bytes (gpu.rs:96-100)");
 static_assert(sizeof(SrGpuUniforms) == 768, "GpuUniforms is 768 bytes (gpu.rs:122-144)");
 static_assert(sizeof(SrTuning) == 48, "SrTuning is 12 words");

@@ -59,6 +59,16 @@ sr_status sr_scene_boxes(const sr_scene* s, const float** boxes);
  * of sr_build_scene_tubes (valid until sr_scene_free). */
 sr_status sr_scene_tubes(const sr_scene* s, const SrTube** tubes, uint32_t* num_tubes);
 
+/* top_tree (bvh4d.rs:593-644), on the host: the tree over n >= 2 subtrees already in an arena,
+ * item i with box boxes[8i .. 8i+7] (min t, x, y, z, then max), root node roots[i], weight
+ * weights[i] (its simplex count) and depth depths[i] (optional). Writes the n - 1 tree nodes to
+ * `nodes` in the reference's order: the first goes to node 0, the k-th to node base + k - 1, and
+ * they link to each other and to the roots accordingly. `depth` (optional) receives the depth of
+ * the whole tree (tree nodes above a subtree plus its own depth). The scene cache calls it for
+ * every snapshot (sr_arena_finish). */
+sr_status sr_top_tree(const float* boxes, const uint32_t* roots, const float* weights, const uint32_t* depths,
+                      uint32_t n, uint32_t base, SrGpuNode* nodes, uint32_t* depth);
+
 /* One observer of the batched workload (configuration 4). */
 typedef struct SrObserverDraw {
     uint32_t width, height, slice_mode, pad;

@@ -102,6 +102,21 @@ def lib():
         L.orc_frozen_loss.restype = C.c_double
         L.orc_frozen_loss.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Camera), C.POINTER(Config), C.c_void_p,
                                       C.c_uint32, C.c_int, C.c_void_p]
+        L.orc_arena_new.restype = C.c_void_p
+        L.orc_arena_new.argtypes = []
+        L.orc_arena_free.argtypes = [C.c_void_p]
+        L.orc_arena_begin.argtypes = [C.c_void_p]
+        L.orc_arena_tube.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p, C.c_uint32,
+                                     C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32]
+        L.orc_arena_piece.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int64, C.c_void_p,
+                                      C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+        L.orc_arena_finish.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        L.orc_arena_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        L.orc_arena_pack.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_top_tree.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
+        L.orc_tube_simplices.restype = C.c_int64
+        L.orc_tube_simplices.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                         C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -342,3 +357,93 @@ class Frozen:
         L = lib().orc_frozen_loss(self.scene.h, self.h, C.byref(camera), C.byref(self.cfg), t.ctypes.data, level,
                                   threads or (os.cpu_count() or 1), out.ctypes.data if hdr else None)
         return (L, out.reshape(-1, 3)) if hdr else L
+
+
+TRI_DTYPE = np.dtype([("idx", "<u4", 3), ("uv", "<f4", (3, 2)), ("normal", "<f4", 3)])
+SAMPLE_DTYPE = np.dtype([("center", "<f4", 4), ("tetrad", "<f4", (4, 4)), ("proper_time", "<f4"), ("phi", "<f4", 3),
+                         ("accel", "<f4", 3), ("pad", "<f4")])
+
+
+class Arena:
+    """The reference's scene cache over an arena (oracle_arena.hpp): the same calls as the engine's
+    sr_arena_* entry points; arrays() gives the arena's packed arrays, free room included."""
+
+    STAT_KEYS = ("chunks_built", "chunks_reused", "simplices_built", "simplices_reused", "arena_simplices", "compacted")
+
+    def __init__(self):
+        self.h = lib().orc_arena_new()
+        self._free = lib().orc_arena_free
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self._free(self.h)
+            self.h = None
+
+    def begin(self):
+        lib().orc_arena_begin(self.h)
+
+    def tube(self, part, vertices, triangles, samples, material, decided=None):
+        v = np.ascontiguousarray(vertices, np.float32)
+        t = np.ascontiguousarray(triangles, TRI_DTYPE)
+        s = np.ascontiguousarray(samples, SAMPLE_DTYPE)
+        d = None if decided is None else np.ascontiguousarray(decided, np.float32)
+        r = lib().orc_arena_tube(self.h, part[0], part[1], part[2], v.ctypes.data, len(v), t.ctypes.data, len(t),
+                                 s.ctypes.data, len(s), None if d is None else d.ctypes.data, material)
+        if r != 0:
+            raise ValueError("bad tube")
+
+    def piece(self, part, index, key, boxes, geoms, attrs):
+        k = np.ascontiguousarray(key, np.uint32)
+        b = np.ascontiguousarray(boxes, np.float32)
+        g = np.ascontiguousarray(geoms, GEOM_DTYPE)
+        a = np.ascontiguousarray(attrs, ATTR_DTYPE)
+        lib().orc_arena_piece(self.h, part[0], part[1], part[2], index, k.ctypes.data, len(k), b.ctypes.data,
+                              g.ctypes.data, a.ctypes.data, len(g))
+
+    def finish(self, boxes=None, geoms=None, attrs=None) -> dict:
+        st = np.zeros(6, np.uint64)
+        if geoms is None or not len(geoms):
+            lib().orc_arena_finish(self.h, None, None, None, 0, st.ctypes.data)
+        else:
+            b = np.ascontiguousarray(boxes, np.float32)
+            g = np.ascontiguousarray(geoms, GEOM_DTYPE)
+            a = np.ascontiguousarray(attrs, ATTR_DTYPE)
+            lib().orc_arena_finish(self.h, b.ctypes.data, g.ctypes.data, a.ctypes.data, len(g), st.ctypes.data)
+        return dict(zip(self.STAT_KEYS, (int(x) for x in st)))
+
+    def arrays(self):
+        nn, npr = C.c_uint32(), C.c_uint32()
+        lib().orc_arena_sizes(self.h, C.byref(nn), C.byref(npr))
+        nodes = np.zeros(nn.value, NODE_DTYPE)
+        geoms = np.zeros(npr.value, GEOM_DTYPE)
+        attrs = np.zeros(npr.value, ATTR_DTYPE)
+        lib().orc_arena_pack(self.h, nodes.ctypes.data, geoms.ctypes.data, attrs.ctypes.data)
+        return nodes, geoms, attrs
+
+
+def tube_simplices(vertices, triangles, samples, material, decided=None):
+    """A whole tube extruded at once: boxes (n x 8), hot and cold records, in build order."""
+    v = np.ascontiguousarray(vertices, np.float32)
+    t = np.ascontiguousarray(triangles, TRI_DTYPE)
+    s = np.ascontiguousarray(samples, SAMPLE_DTYPE)
+    d = None if decided is None else np.ascontiguousarray(decided, np.float32)
+    cap = 3 * len(t) * max(len(s) - 1, 0)
+    boxes = np.zeros((max(cap, 1), 8), np.float32)
+    geoms = np.zeros(max(cap, 1), GEOM_DTYPE)
+    attrs = np.zeros(max(cap, 1), ATTR_DTYPE)
+    n = lib().orc_tube_simplices(v.ctypes.data, len(v), t.ctypes.data, len(t), s.ctypes.data, len(s),
+                                 None if d is None else d.ctypes.data, material, boxes.ctypes.data, geoms.ctypes.data,
+                                 attrs.ctypes.data)
+    if n < 0:
+        raise ValueError("bad tube")
+    return boxes[:n], geoms[:n], attrs[:n]
+
+
+def top_tree(boxes, roots, weights, base):
+    """top_tree (bvh4d.rs:593-644): the n - 1 nodes over n subtrees, in the reference's order."""
+    b = np.ascontiguousarray(boxes, np.float32)
+    r = np.ascontiguousarray(roots, np.uint32)
+    w = np.ascontiguousarray(weights, np.float32)
+    out = np.zeros(len(r) - 1, NODE_DTYPE)
+    lib().orc_top_tree(b.ctypes.data, r.ctypes.data, w.ctypes.data, len(r), base, out.ctypes.data)
+    return out

@@ -3,6 +3,7 @@
 #include <cstring>
 #include <memory>
 
+#include "oracle_arena.hpp"
 #include "oracle_grad.hpp"
 #include "oracle_scenes.hpp"
 
@@ -438,6 +439,190 @@ double orc_frozen_loss(void* s, void* f, const OrcCamera* c, const OrcConfig* cf
     unsigned th = threads <= 0 ? 1u : (unsigned)threads;
     if (b->fp64) return frozen_loss_t(b->d->scene, fb->d, c, cf, target, level, th, hdr_out);
     return frozen_loss_t(b->f->scene, fb->f, c, cf, target, level, th, hdr_out);
+}
+
+}  // extern "C"
+
+// ---- The scene cache over an arena (oracle_arena.hpp) -------------------------------------------
+namespace {
+struct ArenaBox {
+    SceneCacheOracle<float> cache;
+    ArenaBvh<float> arena;
+};
+struct OTri { uint32_t idx[3]; float uv[3][2]; float normal[3]; };  // SrTubeTriangle
+struct OSample {                                                      // SrTubeSample
+    float center[4];
+    float tetrad[4][4];
+    float proper_time;
+    float phi[3];
+    float accel[3];
+    float pad;
+};
+static_assert(sizeof(OTri) == 48 && sizeof(OSample) == 112, "tube record layouts");
+
+std::vector<Simplex<float>> simplices_from_packed(const float* boxes, const void* geoms, const void* attrs, uint32_t n) {
+    std::vector<Simplex<float>> out(n);
+    for (uint32_t i = 0; i < n; ++i)
+        out[i] = simplex_from_packed(((const PGeom*)geoms)[i], ((const PAttr*)attrs)[i], boxes + 8ull * i);
+    return out;
+}
+}  // namespace
+
+extern "C" {
+
+void* orc_arena_new() { return new ArenaBox(); }
+void orc_arena_free(void* a) { delete (ArenaBox*)a; }
+
+int orc_arena_begin(void* a_) {
+    auto* a = (ArenaBox*)a_;
+    a->cache.begin(a->arena);
+    return 0;
+}
+
+int orc_arena_tube(void* a_, uint32_t kind, uint32_t player, uint64_t id, const float* verts, uint32_t nv,
+                   const void* tris_, uint32_t nt, const void* samples_, uint32_t ns, const float* decided,
+                   uint32_t material) {
+    auto* a = (ArenaBox*)a_;
+    const OTri* tris = (const OTri*)tris_;
+    const OSample* smp = (const OSample*)samples_;
+    Mesh3D<float> mesh;
+    std::vector<uint32_t> bits{nv, nt};
+    auto word = [&](const void* p) {
+        uint32_t u;
+        std::memcpy(&u, p, 4);
+        bits.push_back(u);
+    };
+    for (uint32_t i = 0; i < nv; ++i) {
+        mesh.vertices.push_back(V3<float>(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]));
+        for (int k = 0; k < 3; ++k) word(&verts[3 * i + k]);
+    }
+    for (uint32_t i = 0; i < nt; ++i) {
+        Triangle3D<float> t;
+        for (int k = 0; k < 3; ++k) {
+            if (tris[i].idx[k] >= nv) return -1;
+            t.indices[k] = tris[i].idx[k];
+            t.uv[k] = {tris[i].uv[k][0], tris[i].uv[k][1]};
+        }
+        t.normal = V3<float>(tris[i].normal[0], tris[i].normal[1], tris[i].normal[2]);
+        mesh.triangles.push_back(t);
+        for (size_t w = 0; w < sizeof(OTri) / 4; ++w) word((const char*)&tris[i] + 4 * w);
+    }
+    std::vector<WorldlineSample<float>> samples(ns);
+    for (uint32_t i = 0; i < ns; ++i) {
+        const OSample& q = smp[i];
+        WorldlineSample<float>& w = samples[i];
+        w.center = V4<float>(q.center[0], q.center[1], q.center[2], q.center[3]);
+        w.proper_time = q.proper_time;
+        w.phi = V3<float>(q.phi[0], q.phi[1], q.phi[2]);
+        w.proper_accel_local = V3<float>(q.accel[0], q.accel[1], q.accel[2]);
+        for (int k = 0; k < 4; ++k) w.tetrad.e[k] = V4<float>(q.tetrad[k][0], q.tetrad[k][1], q.tetrad[k][2], q.tetrad[k][3]);
+    }
+    a->cache.tube(CachePart{kind, player, id}, mesh, bits, samples, decided, material);
+    return 0;
+}
+
+int orc_arena_piece(void* a_, uint32_t kind, uint32_t player, uint64_t id, int64_t index, const uint32_t* key,
+                    uint32_t key_len, const float* boxes, const void* geoms, const void* attrs, uint32_t n) {
+    auto* a = (ArenaBox*)a_;
+    std::vector<uint32_t> k(key, key + key_len);
+    a->cache.piece(CachePart{kind, player, id}, index, k, simplices_from_packed(boxes, geoms, attrs, n));
+    return 0;
+}
+
+// A whole tube extruded at once (build_worldtube_simplices_with_decided, mesh4d.rs:648-660), as
+// boxes and packed records; returns the count (the arrays need room for 3 per triangle and step).
+int64_t orc_tube_simplices(const float* verts, uint32_t nv, const void* tris_, uint32_t nt, const void* samples_,
+                           uint32_t ns, const float* decided, uint32_t material, float* boxes, void* geoms,
+                           void* attrs) {
+    const OTri* tris = (const OTri*)tris_;
+    const OSample* smp = (const OSample*)samples_;
+    Mesh3D<float> mesh;
+    for (uint32_t i = 0; i < nv; ++i) mesh.vertices.push_back(V3<float>(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]));
+    for (uint32_t i = 0; i < nt; ++i) {
+        Triangle3D<float> t;
+        for (int k = 0; k < 3; ++k) {
+            if (tris[i].idx[k] >= nv) return -1;
+            t.indices[k] = tris[i].idx[k];
+            t.uv[k] = {tris[i].uv[k][0], tris[i].uv[k][1]};
+        }
+        t.normal = V3<float>(tris[i].normal[0], tris[i].normal[1], tris[i].normal[2]);
+        mesh.triangles.push_back(t);
+    }
+    std::vector<WorldlineSample<float>> samples(ns);
+    for (uint32_t i = 0; i < ns; ++i) {
+        const OSample& q = smp[i];
+        WorldlineSample<float>& w = samples[i];
+        w.center = V4<float>(q.center[0], q.center[1], q.center[2], q.center[3]);
+        w.proper_time = q.proper_time;
+        w.phi = V3<float>(q.phi[0], q.phi[1], q.phi[2]);
+        w.proper_accel_local = V3<float>(q.accel[0], q.accel[1], q.accel[2]);
+        for (int k = 0; k < 4; ++k) w.tetrad.e[k] = V4<float>(q.tetrad[k][0], q.tetrad[k][1], q.tetrad[k][2], q.tetrad[k][3]);
+    }
+    std::vector<Simplex<float>> out;
+    extend_worldtube_simplices(out, mesh, samples, decided, material);
+    Bvh<float> b;  // no tree: the records in build order
+    b.hot.resize(out.size());
+    b.order.resize(out.size());
+    for (size_t i = 0; i < out.size(); ++i) {
+        b.hot[i] = out[i].g;
+        b.order[i] = (uint32_t)i;
+        const Aabb<float>& bx = out[i].aabb;
+        float* o = boxes + 8 * i;
+        o[0] = bx.min.t; o[1] = bx.min.x; o[2] = bx.min.y; o[3] = bx.min.z;
+        o[4] = bx.max.t; o[5] = bx.max.x; o[6] = bx.max.y; o[7] = bx.max.z;
+    }
+    b.simplices = std::move(out);
+    Scene<float> sc;
+    sc.bvh = std::move(b);
+    pack_scene(sc, (PNode*)nullptr, (PGeom*)geoms, (PAttr*)attrs, nullptr, nullptr, nullptr);
+    return (int64_t)sc.bvh.hot.size();
+}
+
+// top_tree over n items (boxes n x 8: min then max, roots, weights): the n - 1 nodes in order.
+int orc_top_tree(const float* boxes, const uint32_t* roots, const float* weights, uint32_t n, uint32_t base,
+                 void* nodes_out) {
+    if (n < 2) return -1;
+    std::vector<TopItem<float>> items(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* b = boxes + 8 * i;
+        items[i].box.min = V4<float>(b[0], b[1], b[2], b[3]);
+        items[i].box.max = V4<float>(b[4], b[5], b[6], b[7]);
+        items[i].root = roots[i];
+        items[i].weight = weights[i];
+    }
+    std::vector<BvhNode<float>> tree;
+    top_tree_rec(items, 0, n, base, tree);
+    Scene<float> sc;
+    sc.bvh.nodes = tree;
+    pack_scene(sc, (PNode*)nodes_out, nullptr, nullptr, nullptr, nullptr, nullptr);
+    return 0;
+}
+
+// stats6: chunks built, reused, simplices built, reused, arena simplices, compacted.
+int orc_arena_finish(void* a_, const float* boxes, const void* geoms, const void* attrs, uint32_t n, uint64_t* stats6) {
+    auto* a = (ArenaBox*)a_;
+    a->cache.finish(Bvh<float>::build(simplices_from_packed(boxes, geoms, attrs, n)), a->arena);
+    const CacheStats& s = a->cache.stats;
+    if (stats6) {
+        stats6[0] = s.chunks_built; stats6[1] = s.chunks_reused; stats6[2] = s.simplices_built;
+        stats6[3] = s.simplices_reused; stats6[4] = s.arena_simplices; stats6[5] = s.compacted;
+    }
+    return 0;
+}
+
+int orc_arena_sizes(void* a_, uint32_t* n_nodes, uint32_t* n_prims) {
+    auto* a = (ArenaBox*)a_;
+    *n_nodes = (uint32_t)a->arena.b.nodes.size();
+    *n_prims = (uint32_t)a->arena.b.hot.size();
+    return 0;
+}
+
+int orc_arena_pack(void* a_, void* nodes, void* geoms, void* attrs) {
+    auto* a = (ArenaBox*)a_;
+    Scene<float> sc;
+    sc.bvh = a->arena.b;
+    pack_scene(sc, (PNode*)nodes, (PGeom*)geoms, (PAttr*)attrs, nullptr, nullptr, nullptr);
+    return 0;
 }
 
 }  // extern "C"

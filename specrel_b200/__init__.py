@@ -17,10 +17,10 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import (ATTR_DTYPE, GEOM_DTYPE, MAT_DTYPE, NODE_DTYPE, SR_FLAG_DEVICE_OUTPUT, SR_FLAG_TIMING,
-                   SR_PATH_FAST, SR_PATH_PLAIN, CameraF64, GpuUniforms, SrError)
+from ._lib import (ATTR_DTYPE, GEOM_DTYPE, MAT_DTYPE, NODE_DTYPE, SAMPLE_DTYPE, SR_FLAG_DEVICE_OUTPUT,
+                   SR_FLAG_TIMING, SR_PATH_FAST, SR_PATH_PLAIN, TRI_DTYPE, CameraF64, GpuUniforms, SrError)
 
-__all__ = ["Engine", "PackedScene", "SynthScene", "synth_scene", "camera", "uniforms", "observers", "tables",
+__all__ = ["Engine", "PackedScene", "SynthScene", "TubeData", "synth_scene", "camera", "uniforms", "observers", "tables",
            "SR_PATH_FAST", "SR_PATH_PLAIN", "SR_FLAG_TIMING", "SR_FLAG_DEVICE_OUTPUT", "SrError", "CameraF64",
            "GpuUniforms", "validate"]
 
@@ -152,6 +152,22 @@ class SynthScene:
         attrs[p.leaf_to_orig] = p.attrs
         return boxes, geoms, attrs, p
 
+    def tubes(self) -> list["TubeData"]:
+        """Copies of the scene's worldtubes (mesh, triangles, worldline samples, material)."""
+        tp = C.c_void_p()
+        nt = C.c_uint32()
+        _check(_lib.lib().sr_scene_tubes(self.h, C.byref(tp), C.byref(nt)), what="scene_tubes")
+        out = []
+        for t in (_lib.Tube * nt.value).from_address(tp.value) if nt.value else ():
+            def arr(ptr, n, dtype):
+                if not n:
+                    return np.zeros(0, dtype)
+                return np.frombuffer((C.c_char * (n * np.dtype(dtype).itemsize)).from_address(ptr), dtype).copy()
+            out.append(TubeData(arr(t.vertices, 3 * t.num_vertices, np.float32).reshape(-1, 3),
+                                arr(t.triangles, t.num_triangles, TRI_DTYPE), arr(t.samples, t.num_samples, SAMPLE_DTYPE),
+                                int(t.material)))
+        return out
+
     def packed(self) -> PackedScene:
         """Copies of the packed arrays as numpy (for comparisons in tests)."""
         d = self._desc
@@ -256,6 +272,50 @@ class Frame:
     timings: _lib.Timings | None = None
 
 
+def top_tree(boxes, roots, weights, base: int, depths=None):
+    """sr_top_tree (bvh4d.rs:593-644, host): the n - 1 nodes over n subtrees and the tree's depth."""
+    b = np.ascontiguousarray(boxes, np.float32)
+    r = np.ascontiguousarray(roots, np.uint32)
+    w = np.ascontiguousarray(weights, np.float32)
+    d = None if depths is None else np.ascontiguousarray(depths, np.uint32)
+    out = np.zeros(len(r) - 1, NODE_DTYPE)
+    depth = C.c_uint32()
+    _check(_lib.lib().sr_top_tree(b.ctypes.data, r.ctypes.data, w.ctypes.data, None if d is None else d.ctypes.data,
+                                  len(r), base, out.ctypes.data, C.byref(depth)), what="top_tree")
+    return out, depth.value
+
+
+@dataclass
+class TubeData:
+    """One worldtube (SrTube): a mesh in its body frame swept along worldline samples."""
+    vertices: np.ndarray              # (n, 3) float32
+    triangles: np.ndarray             # TRI_DTYPE
+    samples: np.ndarray               # SAMPLE_DTYPE
+    material: int
+    decided: np.ndarray | None = None  # per-sample causal decision stamps, or None (static)
+
+    def struct(self):
+        keep = [np.ascontiguousarray(self.vertices, np.float32), np.ascontiguousarray(self.triangles, TRI_DTYPE),
+                np.ascontiguousarray(self.samples, SAMPLE_DTYPE)]
+        t = _lib.Tube()
+        t.vertices, t.triangles, t.samples = (a.ctypes.data for a in keep)
+        t.num_vertices = len(keep[0])
+        t.num_triangles = len(keep[1])
+        t.num_samples = len(keep[2])
+        t.material = self.material
+        if self.decided is not None:
+            d = np.ascontiguousarray(self.decided, np.float32)
+            assert len(d) == len(keep[2])
+            keep.append(d)
+            t.decided_at = d.ctypes.data
+        return t, keep
+
+
+def _part(part) -> "_lib.ArenaPart":
+    kind, player, pid = part
+    return _lib.ArenaPart(kind, player, pid)
+
+
 class Engine:
     """GpuRenderer over the C ABI: one CUDA context, scenes uploaded once, frames rendered on demand."""
 
@@ -335,6 +395,53 @@ class Engine:
         d.anchor = sd.anchor
         _check(self.L.sr_build_scene_tubes(self.h, idx, tp, nt.value, C.byref(d)), self.h, "build_scene_tubes")
         self.scenes[idx] = scene
+
+    # ---- the scene cache over a device arena (SceneCache, dynamic/scene_cache.rs) ----
+    def arena_begin(self, idx: int) -> None:
+        _check(self.L.sr_arena_begin(self.h, idx), self.h, "arena_begin")
+
+    def arena_tube(self, idx: int, part, tube: TubeData) -> None:
+        """SceneCache::tube; part = (kind, player, id) with kind 0 body, 1 hull, 2 pulse."""
+        t, keep = tube.struct()
+        _check(self.L.sr_arena_tube(self.h, idx, _part(part), C.byref(t)), self.h, "arena_tube")
+
+    def arena_piece(self, idx: int, part, index: int, key, boxes, geoms, attrs) -> bool:
+        """SceneCache::piece: returns whether the chunk was reused (else its simplices are installed)."""
+        k = np.ascontiguousarray(key, np.uint32)
+        reused = C.c_int32()
+        _check(self.L.sr_arena_reuse(self.h, idx, _part(part), index, k.ctypes.data, len(k), C.byref(reused)),
+               self.h, "arena_reuse")
+        if not reused.value:
+            b = np.ascontiguousarray(boxes, np.float32)
+            g = np.ascontiguousarray(geoms, GEOM_DTYPE)
+            a = np.ascontiguousarray(attrs, ATTR_DTYPE)
+            _check(self.L.sr_arena_install(self.h, idx, _part(part), index, b.ctypes.data, g.ctypes.data,
+                                           a.ctypes.data, len(g)), self.h, "arena_install")
+        return bool(reused.value)
+
+    def arena_finish(self, idx: int, rest: "SynthScene", boxes=None, geoms=None, attrs=None) -> dict:
+        """SceneCache::finish with the volatile simplices (build order, may be None); materials, stars,
+        light and anchor from `rest`. Returns the snapshot's CacheStats."""
+        sd = rest._desc
+        d = _lib.BuildDesc()
+        keep = []
+        if geoms is not None and len(geoms):
+            keep = [np.ascontiguousarray(boxes, np.float32), np.ascontiguousarray(geoms, GEOM_DTYPE),
+                    np.ascontiguousarray(attrs, ATTR_DTYPE)]
+            d.boxes, d.geoms, d.attrs = (a.ctypes.data for a in keep)
+            d.num_prims = len(keep[1])
+        d.materials = sd.materials
+        d.num_materials = sd.num_materials
+        d.stars = sd.stars
+        d.num_star_vec4 = sd.num_star_vec4
+        d.num_stars = sd.num_stars
+        for k in range(4):
+            d.light_pos[k] = sd.light_pos[k]
+        d.anchor = sd.anchor
+        st = _lib.ArenaStats()
+        _check(self.L.sr_arena_finish(self.h, idx, C.byref(d), C.byref(st)), self.h, "arena_finish")
+        self.scenes[idx] = rest
+        return {k: getattr(st, k) for k, _ in _lib.ArenaStats._fields_ if k != "pad"}
 
     def records(self, idx: int):
         """The device scene's hot and cold records (leaf order)."""

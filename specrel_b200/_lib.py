@@ -42,6 +42,9 @@ GEOM_DTYPE = np.dtype([("v0", "<f4", 4), ("n", "<f4", 4), ("b1", "<f4", 4), ("b2
 ATTR_DTYPE = np.dtype([(k, "<f4", 4) for k in ("uv_u", "uv_v", "tb_x", "tb_y", "tb_z", "tau", "grad_u", "grad_v",
                                               "normal", "four_vel", "misc", "decided_at")])
 MAT_DTYPE = np.dtype([("base", "<f4", 4), ("checker", "<f4", 4), ("params", "<f4", 4)])
+TRI_DTYPE = np.dtype([("idx", "<u4", 3), ("uv", "<f4", (3, 2)), ("normal", "<f4", 3)])  # SrTubeTriangle
+SAMPLE_DTYPE = np.dtype([("center", "<f4", 4), ("tetrad", "<f4", (4, 4)), ("proper_time", "<f4"), ("phi", "<f4", 3),
+                         ("accel", "<f4", 3), ("pad", "<f4")])  # SrTubeSample
 
 
 class GpuUniforms(C.Structure):
@@ -67,6 +70,22 @@ class BuildDesc(C.Structure):
                 ("materials", C.c_void_p), ("num_materials", C.c_uint32), ("num_stars", C.c_uint32),
                 ("stars", C.c_void_p), ("num_star_vec4", C.c_uint64), ("light_pos", C.c_float * 4),
                 ("anchor", C.c_void_p)]
+
+
+class Tube(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("num_vertices", C.c_uint32), ("num_triangles", C.c_uint32),
+                ("triangles", C.c_void_p), ("samples", C.c_void_p), ("num_samples", C.c_uint32),
+                ("material", C.c_uint32), ("decided_at", C.c_void_p)]
+
+
+class ArenaPart(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("player", C.c_uint32), ("id", C.c_uint64)]
+
+
+class ArenaStats(C.Structure):
+    _fields_ = [("chunks_built", C.c_uint32), ("chunks_reused", C.c_uint32), ("simplices_built", C.c_uint64),
+                ("simplices_reused", C.c_uint64), ("arena_simplices", C.c_uint64), ("compacted", C.c_uint32),
+                ("num_nodes", C.c_uint32), ("bvh_depth", C.c_uint32), ("pad", C.c_uint32)]
 
 
 class Range(C.Structure):
@@ -171,7 +190,16 @@ SIGNATURES = {
                                   C.POINTER(C.c_uint32)]),
     "sr_scene_boxes": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "sr_scene_tubes": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint32)]),
+    "sr_top_tree": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                C.POINTER(C.c_uint32)]),
     "sr_build_scene_tubes": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.POINTER(BuildDesc)]),
+    "sr_arena_begin": (C.c_int32, [C.c_void_p, C.c_uint32]),
+    "sr_arena_tube": (C.c_int32, [C.c_void_p, C.c_uint32, ArenaPart, C.POINTER(Tube)]),
+    "sr_arena_reuse": (C.c_int32, [C.c_void_p, C.c_uint32, ArenaPart, C.c_int64, C.c_void_p, C.c_uint32,
+                                   C.POINTER(C.c_int32)]),
+    "sr_arena_install": (C.c_int32, [C.c_void_p, C.c_uint32, ArenaPart, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_uint32]),
+    "sr_arena_finish": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(BuildDesc), C.POINTER(ArenaStats)]),
     "sr_scene_records": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32]),
     "sr_update_scene": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(SceneDesc), C.POINTER(Range), C.c_uint32,
                                     C.POINTER(Range), C.c_uint32]),

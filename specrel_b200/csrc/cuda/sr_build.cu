@@ -597,9 +597,11 @@ cudaError_t gpu_gather_records(const uint32_t* order, uint32_t n, const SrGpuGeo
     return cudaGetLastError();
 }
 
-cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint32_t* order,
-                          GpuBuildInfo* info, cudaStream_t st) {
+cudaError_t gpu_bvh_build_forest(const float4* box, uint32_t n, const GpuSegment* seg, uint32_t num_seg,
+                                 SrGpuNode* nodes, uint32_t* order, GpuTreeInfo* tree, GpuBuildInfo* info,
+                                 cudaStream_t st) {
     *info = GpuBuildInfo{};
+    for (uint32_t s = 0; s < num_seg; ++s) tree[s] = GpuTreeInfo{0, 0, 0, 0};
     if (n == 0) return cudaSuccess;
     cudaError_t e = keep_build_pool();
     if (e != cudaSuccess) return e;
@@ -616,41 +618,48 @@ cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint3
     BK(cudaGetLastError());
 
     // Host view of the large nodes: bounds, children and the small subtree at each leaf of this
-    // part of the tree.
+    // part of the tree; `seg` is the tree the node belongs to.
     struct HNode {
         float lo[4], hi[4];
-        uint32_t start, count;
+        uint32_t start, count, seg;
         int left = -1, right = -1, small = -1, leaf = 0;
     };
     std::vector<HNode> hn;
     std::vector<STask> small;
     std::vector<int> small_owner;
     std::vector<uint32_t> level;  // hn ids of this level's large nodes
-    if (n > SMALL) {
+    std::vector<int> root(num_seg, -1);
+    bool any_large = false;
+    for (uint32_t sg = 0; sg < num_seg; ++sg) {
+        if (seg[sg].count == 0) continue;
         HNode r{};
-        r.start = 0;
-        r.count = n;
+        r.start = seg[sg].start;
+        r.count = seg[sg].count;
+        r.seg = sg;
+        root[sg] = (int)hn.size();
+        if (r.count > SMALL) {
+            level.push_back((uint32_t)hn.size());
+            any_large = true;
+        } else {
+            r.small = (int)small.size();
+            small.push_back({r.start, r.count});
+            small_owner.push_back((int)hn.size());
+        }
         hn.push_back(r);
-        level.push_back(0);
-    } else {
-        HNode r{};
-        r.start = 0;
-        r.count = n;
-        r.small = 0;
-        hn.push_back(r);
-        small.push_back({0, n});
-        small_owner.push_back(0);
     }
     size_t scan_bytes = 0;
-    cub::DeviceScan::ExclusiveSumByKey(nullptr, scan_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)n);
     Buf<unsigned char> scan_tmp;
-    BK(scan_tmp.alloc(scan_bytes, st));
-    BK(flag.alloc(n, st));
-    BK(key.alloc(n, st));
-    BK(lb.alloc(n, st));
-    BK(svc.alloc(n, st));
-    BK(sb.alloc(n, st));
-    for (int k = 0; k < 2; ++k) { BK(ei[k].alloc(2ull * n, st)); BK(er[k].alloc(2ull * n, st)); }
+    if (any_large) {
+        cub::DeviceScan::ExclusiveSumByKey(nullptr, scan_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                           (uint32_t*)nullptr, (int)n);
+        BK(scan_tmp.alloc(scan_bytes, st));
+        BK(flag.alloc(n, st));
+        BK(key.alloc(n, st));
+        BK(lb.alloc(n, st));
+        BK(svc.alloc(n, st));
+        BK(sb.alloc(n, st));
+        for (int k = 0; k < 2; ++k) { BK(ei[k].alloc(2ull * n, st)); BK(er[k].alloc(2ull * n, st)); }
+    }
     while (!level.empty()) {
         const uint32_t nt = (uint32_t)level.size();
         std::vector<LTask> tasks(nt);
@@ -712,7 +721,8 @@ cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint3
             for (int k = 0; k < 4; ++k) { hn[id].lo[k] = oval_host(h.blo[k]); hn[id].hi[k] = oval_host(h.bhi[k]); }
             if (h.leaf) {
                 hn[id].leaf = 1;
-                info->max_leaf = std::max(info->max_leaf, hn[id].count);
+                GpuTreeInfo& ti = tree[hn[id].seg];
+                ti.max_leaf = std::max(ti.max_leaf, hn[id].count);
                 continue;
             }
             if (h.m == 0 || h.m == hn[id].count) {
@@ -725,6 +735,7 @@ cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint3
                 HNode ch{};
                 ch.start = parts[side][0];
                 ch.count = parts[side][1];
+                ch.seg = hn[id].seg;
                 const int cid = (int)hn.size();
                 if (ch.count > SMALL) {
                     next.push_back((uint32_t)cid);
@@ -745,46 +756,59 @@ cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint3
     const uint32_t ns = (uint32_t)small.size();
     Buf<STask> dst;
     Buf<SResult> dres;
-    BK(dst.alloc(ns, st));
-    BK(dres.alloc(ns, st));
-    BK(cudaMemcpyAsync(dst.p, small.data(), ns * sizeof(STask), cudaMemcpyHostToDevice, st));
-    const size_t smem = 3 * SMALL * sizeof(float4) + SMALL * (sizeof(uint32_t) + sizeof(uint16_t));
-    BK(cudaFuncSetAttribute(k_small_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_small_build<<<ns, 256, smem, st>>>(dst.p, box, cen.p, perm.p, tmp.p, dres.p);
-    BK(cudaGetLastError());
     std::vector<SResult> res(ns);
-    BK(cudaMemcpyAsync(res.data(), dres.p, ns * sizeof(SResult), cudaMemcpyDeviceToHost, st));
-    BK(cudaStreamSynchronize(st));
-    for (const SResult& r : res) {
-        if (r.bad) { info->unsupported = 1; return cudaSuccess; }
-        info->max_leaf = std::max(info->max_leaf, r.max_leaf);
+    if (ns) {
+        BK(dst.alloc(ns, st));
+        BK(dres.alloc(ns, st));
+        BK(cudaMemcpyAsync(dst.p, small.data(), ns * sizeof(STask), cudaMemcpyHostToDevice, st));
+        const size_t smem = 3 * SMALL * sizeof(float4) + SMALL * (sizeof(uint32_t) + sizeof(uint16_t));
+        BK(cudaFuncSetAttribute(k_small_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_small_build<<<ns, 256, smem, st>>>(dst.p, box, cen.p, perm.p, tmp.p, dres.p);
+        BK(cudaGetLastError());
+        BK(cudaMemcpyAsync(res.data(), dres.p, ns * sizeof(SResult), cudaMemcpyDeviceToHost, st));
+        BK(cudaStreamSynchronize(st));
+    }
+    for (uint32_t k = 0; k < ns; ++k) {
+        if (res[k].bad) { info->unsupported = 1; return cudaSuccess; }
+        GpuTreeInfo& ti = tree[hn[small_owner[k]].seg];
+        ti.max_leaf = std::max(ti.max_leaf, res[k].max_leaf);
     }
 
-    // Depth-first numbering of the large nodes and the small subtrees' bases.
+    // Depth-first numbering of the large nodes and the small subtrees' bases, tree after tree.
     std::vector<uint32_t> pre(hn.size(), 0), sbase(ns, 0);
     std::vector<SrGpuNode> lnodes;
     std::vector<uint32_t> lat;
-    uint32_t nextidx = 0, depth = 0;
+    uint32_t nextidx = 0;
     struct Fr { int id; uint32_t d; };
-    std::vector<Fr> stack{{0, 1}};
-    std::vector<std::pair<int, uint32_t>> patch;  // (large node, hn id of its right child)
-    while (!stack.empty()) {
-        Fr f = stack.back();
-        stack.pop_back();
-        HNode& h = hn[f.id];
-        pre[f.id] = nextidx;
-        if (h.small >= 0) {
-            sbase[h.small] = nextidx;
-            nextidx += res[h.small].nodes;
-            depth = std::max(depth, f.d - 1 + res[h.small].depth);
-            continue;
+    std::vector<Fr> stack;
+    for (uint32_t sg = 0; sg < num_seg; ++sg) {
+        GpuTreeInfo& ti = tree[sg];
+        ti.node_base = nextidx;
+        if (root[sg] < 0) continue;
+        uint32_t depth = 0;
+        stack.push_back({root[sg], 1});
+        while (!stack.empty()) {
+            Fr f = stack.back();
+            stack.pop_back();
+            HNode& h = hn[f.id];
+            pre[f.id] = nextidx;
+            if (h.small >= 0) {
+                sbase[h.small] = nextidx;
+                nextidx += res[h.small].nodes;
+                depth = std::max(depth, f.d - 1 + res[h.small].depth);
+                continue;
+            }
+            depth = std::max(depth, f.d);
+            ++nextidx;
+            if (!h.leaf) {
+                stack.push_back({h.right, f.d + 1});
+                stack.push_back({h.left, f.d + 1});
+            }
         }
-        depth = std::max(depth, f.d);
-        ++nextidx;
-        if (!h.leaf) {
-            stack.push_back({h.right, f.d + 1});
-            stack.push_back({h.left, f.d + 1});
-        }
+        ti.num_nodes = nextidx - ti.node_base;
+        ti.depth = depth;
+        info->depth = std::max(info->depth, depth);
+        info->max_leaf = std::max(info->max_leaf, ti.max_leaf);
     }
     for (size_t id = 0; id < hn.size(); ++id) {
         const HNode& h = hn[id];
@@ -814,14 +838,20 @@ cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint3
     BK(cudaMemcpyAsync(dsb.p, sbase.data(), ns * 4, cudaMemcpyHostToDevice, st));
     if (!lnodes.empty())
         k_place_large<<<((uint32_t)lnodes.size() + 255) / 256, 256, 0, st>>>(dl.p, dlat.p, (uint32_t)lnodes.size(), nodes);
-    k_place_small<<<ns, 256, 0, st>>>(dst.p, dres.p, dsb.p, tmp.p, nodes);
+    if (ns) k_place_small<<<ns, 256, 0, st>>>(dst.p, dres.p, dsb.p, tmp.p, nodes);
     BK(cudaGetLastError());
     BK(cudaMemcpyAsync(order, perm.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
     BK(cudaStreamSynchronize(st));
     info->num_nodes = nextidx;
-    info->depth = depth;
 #undef BK
     return cudaSuccess;
+}
+
+cudaError_t gpu_bvh_build(const float4* box, uint32_t n, SrGpuNode* nodes, uint32_t* order, GpuBuildInfo* info,
+                          cudaStream_t st) {
+    const GpuSegment all{0, n};
+    GpuTreeInfo tree{};
+    return gpu_bvh_build_forest(box, n, &all, 1, nodes, order, &tree, info, st);
 }
 
 }  // namespace srk

@@ -17,76 +17,12 @@
 #include "../../../include/specrel_scene.h"
 #include "sr_build.h"
 #include "sr_fast.h"
-#include "sr_kernels.h"
+#include "sr_engine.h"
 
 using namespace srk;
+using namespace sre;
 
 namespace {
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    ~DevBuf() { if (p) cudaFree(p); }
-    cudaError_t ensure(size_t n) {
-        if (n <= bytes && p) return cudaSuccess;
-        if (p) { cudaFree(p); p = nullptr; bytes = 0; }
-        if (n == 0) return cudaSuccess;
-        cudaError_t e = cudaMalloc(&p, n);
-        if (e == cudaSuccess) bytes = n;
-        return e;
-    }
-    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
-};
-
-struct SceneSlot {
-    bool present = false;
-    DevBuf nodes, geoms, attrs, mats, stars, l2o;
-    uint32_t num_nodes = 0, num_prims = 0, num_mats = 0, num_stars = 0;
-    uint64_t num_star_vec4 = 0;
-    float light_pos[4] = {0, 0, 0, 0};
-    double anchor[4] = {0, 0, 0, 0};
-    uint32_t depth = 0;
-    bool has_l2o = false;
-    FastScene fast;  // the B200 node layout
-    SrTuning tuning{};
-};
-
-struct Frame {
-    uint32_t w = 0, h = 0;
-    Pyramid pyr{};
-    DevBuf hdr, rgb, hit, lam, tau;
-};
-
-}  // namespace
-
-struct sr_ctx {
-    int device = 0;
-    cudaStream_t own = nullptr, stream = nullptr;
-    std::string last_error;
-    std::string name;
-    DevBuf tables, counters, cam;
-    BBConst bb{};
-    std::vector<std::unique_ptr<SceneSlot>> scenes;
-    Frame frame;
-    cudaEvent_t ev[8] = {};
-    FastCtx fast;
-};
-
-namespace {
-
-sr_status fail(sr_ctx* c, sr_status s, const std::string& m) {
-    if (c) c->last_error = m;
-    return s;
-}
-sr_status cuda_fail(sr_ctx* c, cudaError_t e, const char* where) {
-    return fail(c, e == cudaErrorMemoryAllocation ? SR_ERR_OUT_OF_MEMORY : SR_ERR_CUDA,
-                std::string(where) + ": " + cudaGetErrorString(e));
-}
-#define CK(expr, where)                                \
-    do {                                               \
-        cudaError_t e_ = (expr);                       \
-        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
-    } while (0)
 
 // Blackbody constants (star.rs:162-180): powi(5) folded in double precision, white-point Planck
 // values in f32, as the compiled reference evaluates them.
@@ -116,7 +52,7 @@ SceneDev scene_dev(const sr_ctx* ctx, const SceneSlot& s) {
     d.leaf_to_orig = s.has_l2o ? s.l2o.as<uint32_t>() : nullptr;
     d.tables = ctx->tables.as<uint32_t>();
     d.wide = nullptr;
-    d.num_nodes = s.num_nodes;
+    d.num_nodes = s.empty_tree ? 0 : s.num_nodes;
     d.num_prims = s.num_prims;
     d.num_mats = s.num_mats;
     d.num_stars = s.num_stars;
@@ -242,6 +178,7 @@ sr_status sr_upload_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d) {
     }
     s.num_nodes = d->num_nodes;
     s.num_prims = d->num_prims;
+    s.empty_tree = d->num_nodes && SR_NODE_IS_NOTHING(&d->nodes[0]);
     s.num_mats = d->num_materials;
     s.num_stars = d->num_stars;
     s.num_star_vec4 = d->num_star_vec4;
@@ -273,6 +210,7 @@ sr_status sr_update_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d, const
     for (uint32_t i = 0; i < n_nr && fits; ++i) fits = nr[i].start <= nr[i].end && nr[i].end <= d->num_nodes;
     for (uint32_t i = 0; i < n_pr && fits; ++i) fits = pr[i].start <= pr[i].end && pr[i].end <= d->num_prims;
     if (!fits) return sr_upload_scene(ctx, idx, d);  // gpu.rs:730: upload afresh
+    s.arena.reset();  // patched from the host: no longer a device scene cache's arena
     uint32_t depth = 0;
     char why[256] = {0};
     if (sr_scene_validate(d, &depth, why, sizeof(why)) != SR_OK)
@@ -294,6 +232,7 @@ sr_status sr_update_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d, const
         CK(cudaMemcpyAsync(s.stars.p, d->stars, (size_t)d->num_star_vec4 * 16, cudaMemcpyHostToDevice, ctx->stream), "patch stars");
     s.num_nodes = d->num_nodes;
     s.num_prims = d->num_prims;
+    s.empty_tree = d->num_nodes && SR_NODE_IS_NOTHING(&d->nodes[0]);
     s.num_stars = d->num_stars;
     s.num_star_vec4 = d->num_star_vec4;
     s.depth = depth;
@@ -312,6 +251,7 @@ static std::unique_ptr<SceneSlot> take_slot(sr_ctx* ctx, uint32_t idx) {
         cudaStreamSynchronize(ctx->stream);  // frames queued on the old scene finish first
         std::unique_ptr<SceneSlot> s = std::move(ctx->scenes[idx]);
         s->present = false;
+        s->arena.reset();  // its arrays stop being a scene cache's arena
         return s;
     }
     return std::make_unique<SceneSlot>();
@@ -335,6 +275,7 @@ static sr_status finish_build(sr_ctx* ctx, SceneSlot& s, const float4* box, cons
     s.num_nodes = info.num_nodes;
     s.depth = info.depth;
     s.has_l2o = true;
+    s.empty_tree = false;
     s.num_prims = n;
     CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, s.depth, n, info.max_leaf, st),
        "build node layout");
@@ -342,8 +283,10 @@ static sr_status finish_build(sr_ctx* ctx, SceneSlot& s, const float4* box, cons
 }
 
 // Materials, stars, light and anchor of a built scene; the slot goes live at `idx`.
-static sr_status finish_scene(sr_ctx* ctx, uint32_t idx, std::unique_ptr<SceneSlot> slot, const SrBuildDesc* d) {
-    SceneSlot& s = *slot;
+}  // extern "C"
+
+namespace sre {
+sr_status upload_scene_rest(sr_ctx* ctx, SceneSlot& s, const SrBuildDesc* d) {
     auto up = [&](DevBuf& b, const void* src, size_t bytes) -> cudaError_t {
         cudaError_t e = b.ensure(std::max<size_t>(bytes, 16));
         if (e != cudaSuccess || !bytes) return e;
@@ -358,6 +301,16 @@ static sr_status finish_scene(sr_ctx* ctx, uint32_t idx, std::unique_ptr<SceneSl
         s.light_pos[k] = d->light_pos[k];
         s.anchor[k] = d->anchor ? d->anchor[k] : 0.0;
     }
+    return SR_OK;
+}
+}  // namespace sre
+
+extern "C" {
+
+static sr_status finish_scene(sr_ctx* ctx, uint32_t idx, std::unique_ptr<SceneSlot> slot, const SrBuildDesc* d) {
+    SceneSlot& s = *slot;
+    sr_status r = upload_scene_rest(ctx, s, d);
+    if (r != SR_OK) return r;
     s.tuning = fast_default_tuning(ctx->fast);
     CK(cudaStreamSynchronize(ctx->stream), "build sync");
     s.present = true;
@@ -367,7 +320,9 @@ static sr_status finish_scene(sr_ctx* ctx, uint32_t idx, std::unique_ptr<SceneSl
 }
 
 // Materials and star segments checked as sr_upload_scene checks them (no tree yet).
-static sr_status check_build_desc(sr_ctx* ctx, const SrBuildDesc* d, const SrGpuAttr* host_attrs, uint32_t n) {
+}  // extern "C"
+
+sr_status sre::check_build_desc(sr_ctx* ctx, const SrBuildDesc* d, const SrGpuAttr* host_attrs, uint32_t n) {
     SrSceneDesc v{};
     v.num_prims = host_attrs ? n : 0;
     v.attrs = host_attrs;
@@ -383,6 +338,8 @@ static sr_status check_build_desc(sr_ctx* ctx, const SrBuildDesc* d, const SrGpu
         return fail(ctx, SR_ERR_BAD_SCENE, std::string("invalid scene: ") + why);
     return SR_OK;
 }
+
+extern "C" {
 
 sr_status sr_build_scene(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d) {
     if (!ctx || !d) return SR_ERR_INVALID_ARGUMENT;

@@ -6,6 +6,7 @@
 // records and boxes are the host's bit for bit.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <vector>
 
 #include "../host/tube_build.hpp"
@@ -20,7 +21,10 @@ namespace {
 struct BodyDev {
     uint32_t vert_off, nv, tri_off, nt, samp_off, ns, mat, ev_off;
     uint64_t cand_off;
+    uint32_t dec_off;  // first decided stamp, or NO_DECIDED (static geometry)
+    uint32_t pad;
 };
+constexpr uint32_t NO_DECIDED = 0xFFFFFFFFu;
 
 __global__ void k_tube_events(const BodyDev* bodies, const V3f* verts, const TubeSample* samples, V4f* ev) {
     const BodyDev b = bodies[blockIdx.y];
@@ -31,16 +35,18 @@ __global__ void k_tube_events(const BodyDev* bodies, const V3f* verts, const Tub
     ev[b.ev_off + i] = smp.center + to_world(smp, verts[b.vert_off + v]);
 }
 
-__global__ void k_tube_tets(const BodyDev* bodies, const TubeTri* tris, const TubeSample* samples, const V4f* ev,
-                            SrGpuGeom* cg, SrGpuAttr* ca, float4* cb, uint32_t* valid) {
+__global__ void k_tube_tets(const BodyDev* bodies, const TubeTri* tris, const TubeSample* samples, const float* dec,
+                            const V4f* ev, SrGpuGeom* cg, SrGpuAttr* ca, float4* cb, uint32_t* valid) {
     const BodyDev b = bodies[blockIdx.y];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (b.ns < 2 || i >= (b.ns - 1) * b.nt) return;
     const uint32_t st = i / b.nt, t = i % b.nt;
     Tet tet[3];
     bool ok[3];
+    const float d0 = b.dec_off == NO_DECIDED ? DECIDED_STATIC : dec[b.dec_off + st];
+    const float d1 = b.dec_off == NO_DECIDED ? DECIDED_STATIC : dec[b.dec_off + st + 1];
     tube_segment(tris[b.tri_off + t], ev + b.ev_off + (size_t)st * b.nv, ev + b.ev_off + (size_t)(st + 1) * b.nv,
-                 samples[b.samp_off + st], samples[b.samp_off + st + 1], b.mat, tet, ok);
+                 samples[b.samp_off + st], samples[b.samp_off + st + 1], b.mat, d0, d1, tet, ok);
     const uint64_t c = b.cand_off + 3ull * i;
     for (int k = 0; k < 3; ++k) {
         valid[c + k] = ok[k] ? 1u : 0u;
@@ -65,6 +71,14 @@ __global__ void k_tube_compact(uint64_t ncand, const uint32_t* valid, const uint
     }
 }
 
+// The first simplex of each tube after compaction, and the total.
+__global__ void k_tube_first(const BodyDev* bodies, uint32_t num_tubes, uint64_t ncand, const uint32_t* pos,
+                             uint32_t* first) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < num_tubes) first[b] = pos[bodies[b].cand_off];
+    if (b == num_tubes) first[b] = pos[ncand];
+}
+
 // Scratch from the stream-ordered pool (see sr_build.cu).
 template <class T>
 struct DBuf {
@@ -79,8 +93,10 @@ struct DBuf {
 
 }  // namespace
 
-cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out, cudaStream_t st) {
+cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out, cudaStream_t st,
+                        uint32_t* tube_first) {
     *out = ExtrudeOut{};
+    if (tube_first) std::fill(tube_first, tube_first + num_tubes + 1, 0u);
     cudaError_t e = keep_build_pool();
     if (e != cudaSuccess) return e;
 #define EK(x) do { if ((e = (x)) != cudaSuccess) return e; } while (0)
@@ -88,6 +104,7 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
     std::vector<V3f> verts;
     std::vector<TubeTri> tris;
     std::vector<TubeSample> samples;
+    std::vector<float> decs;
     uint64_t ncand = 0;
     uint32_t nev = 0, max_ev = 0, max_seg = 0;
     for (uint32_t b = 0; b < num_tubes; ++b) {
@@ -102,6 +119,9 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
         d.mat = tb.material;
         d.ev_off = nev;
         d.cand_off = ncand;
+        d.dec_off = tb.decided_at ? (uint32_t)decs.size() : NO_DECIDED;
+        d.pad = 0;
+        if (tb.decided_at) decs.insert(decs.end(), tb.decided_at, tb.decided_at + tb.num_samples);
         const size_t v0 = verts.size();
         for (uint32_t v = 0; v < tb.num_vertices; ++v)
             verts.push_back(V3f(tb.vertices[3 * v], tb.vertices[3 * v + 1], tb.vertices[3 * v + 2]));
@@ -132,6 +152,7 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
     DBuf<V3f> dv;
     DBuf<TubeTri> dt;
     DBuf<TubeSample> ds;
+    DBuf<float> ddec;
     DBuf<V4f> dev;
     DBuf<SrGpuGeom> cg;
     DBuf<SrGpuAttr> ca;
@@ -141,6 +162,7 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
     EK(dv.alloc(verts.size(), st));
     EK(dt.alloc(tris.size(), st));
     EK(ds.alloc(samples.size(), st));
+    EK(ddec.alloc(decs.size(), st));
     EK(dev.alloc(nev, st));
     EK(cg.alloc(ncand, st));
     EK(ca.alloc(ncand, st));
@@ -151,10 +173,12 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
     EK(cudaMemcpyAsync(dv.p, verts.data(), verts.size() * sizeof(V3f), cudaMemcpyHostToDevice, st));
     EK(cudaMemcpyAsync(dt.p, tris.data(), tris.size() * sizeof(TubeTri), cudaMemcpyHostToDevice, st));
     EK(cudaMemcpyAsync(ds.p, samples.data(), samples.size() * sizeof(TubeSample), cudaMemcpyHostToDevice, st));
+    if (!decs.empty())
+        EK(cudaMemcpyAsync(ddec.p, decs.data(), decs.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     EK(cudaMemsetAsync(valid.p, 0, (ncand + 1) * 4, st));
     k_tube_events<<<dim3((max_ev + 255) / 256, num_tubes), 256, 0, st>>>(db.p, dv.p, ds.p, dev.p);
-    k_tube_tets<<<dim3((max_seg + 127) / 128, num_tubes), 128, 0, st>>>(db.p, dt.p, ds.p, dev.p, cg.p, ca.p, cb.p,
-                                                                        valid.p);
+    k_tube_tets<<<dim3((max_seg + 127) / 128, num_tubes), 128, 0, st>>>(db.p, dt.p, ds.p, ddec.p, dev.p, cg.p, ca.p,
+                                                                        cb.p, valid.p);
     EK(cudaGetLastError());
     size_t tmp_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, valid.p, pos.p, (int)(ncand + 1), st);
@@ -163,6 +187,13 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
     EK(cub::DeviceScan::ExclusiveSum(tmp.p, tmp_bytes, valid.p, pos.p, (int)(ncand + 1), st));
     uint32_t n = 0;
     EK(cudaMemcpyAsync(&n, pos.p + ncand, 4, cudaMemcpyDeviceToHost, st));
+    DBuf<uint32_t> dfirst;
+    if (tube_first) {
+        EK(dfirst.alloc(num_tubes + 1, st));
+        k_tube_first<<<(num_tubes + 256) / 256, 256, 0, st>>>(db.p, num_tubes, ncand, pos.p, dfirst.p);
+        EK(cudaGetLastError());
+        EK(cudaMemcpyAsync(tube_first, dfirst.p, (num_tubes + 1) * 4, cudaMemcpyDeviceToHost, st));
+    }
     EK(cudaStreamSynchronize(st));
     EK(cudaMallocAsync(reinterpret_cast<void**>(&out->geoms), std::max<size_t>(n, 1) * sizeof(SrGpuGeom), st));
     EK(cudaMallocAsync(reinterpret_cast<void**>(&out->attrs), std::max<size_t>(n, 1) * sizeof(SrGpuAttr), st));

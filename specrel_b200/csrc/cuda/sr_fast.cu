@@ -94,6 +94,10 @@ cudaError_t fast_build(FastCtx& c, FastScene& s, const SrGpuNode* nodes, uint32_
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return e;
     for (int k = 0; k < 4; ++k) { s.root_min[k] = root.min[k]; s.root_max[k] = root.max[k]; }
+    if (SR_NODE_IS_NOTHING(&root)) {  // an empty tree (an arena with nothing written)
+        s.empty = true;
+        return cudaSuccess;
+    }
     if (root.count > 0) {
         s.root_ref = pack_leaf(root.right_or_first, root.count);
         return cudaSuccess;

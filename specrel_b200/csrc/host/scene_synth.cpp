@@ -223,7 +223,8 @@ bool extrude(std::vector<Tet>& out, const Mesh& mesh, const std::vector<Sample>&
         for (auto& t : tt) {
             Tet tet[3];
             bool ok[3];
-            tube_segment(t, &ev[st * nv], &ev[(st + 1) * nv], ts[st], ts[st + 1], mat, tet, ok);
+            tube_segment(t, &ev[st * nv], &ev[(st + 1) * nv], ts[st], ts[st + 1], mat, DECIDED_STATIC, DECIDED_STATIC, tet,
+                         ok);
             for (int k = 0; k < 3; ++k)
                 if (ok[k]) out.push_back(tet[k]);
         }
@@ -608,7 +609,7 @@ extern "C" sr_status sr_scene_synth(const SrSynthParams* p, sr_scene** out, char
     }
     for (auto& rec : sc->tube_recs)
         sc->tubes.push_back(SrTube{rec.verts.data(), (uint32_t)(rec.verts.size() / 3), (uint32_t)rec.tris.size(),
-                                   rec.tris.data(), rec.samples.data(), (uint32_t)rec.samples.size(), rec.mat});
+                                   rec.tris.data(), rec.samples.data(), (uint32_t)rec.samples.size(), rec.mat, nullptr});
     sc->info.rindler_ok = 1;
     for (char c : rok) if (!c) sc->info.rindler_ok = 0;
     size_t n = 0;

@@ -18,7 +18,11 @@ static std::string check(const SrSceneDesc* d, uint32_t* depth_out) {
     std::vector<uint8_t> seen(d->num_nodes, 0);
     std::vector<std::pair<uint32_t, uint32_t>> st;
     uint32_t depth = 0;
-    if (d->num_nodes) st.push_back({0u, 1u});
+    // A root over nothing (BvhNode4D::NOTHING, bvh4d.rs:31: an empty box linking to itself, what an
+    // arena holds before anything is written to it) is an empty tree; the rest is free room.
+    const bool nothing = d->num_nodes && SR_NODE_IS_NOTHING(&d->nodes[0]);
+    if (d->num_nodes && !nothing) st.push_back({0u, 1u});
+    if (nothing) depth = 1;
     while (!st.empty()) {
         auto [i, dd] = st.back();
         st.pop_back();

@@ -126,13 +126,16 @@ inline TubeTri make_tube_tri(const V3f* verts, const uint32_t* tri_idx, const fl
     return t;
 }
 
+// decided_at of static geometry (DECIDED_AT_STATIC, mesh4d.rs:3-5).
+constexpr float DECIDED_STATIC = -1.0e9f;
+
 // The three tetrahedra of triangle t between samples sc and sn (extend_worldtube_simplices,
-// mesh4d.rs:776-854; the Dompierre split (A0,B0,C0,C1), (A0,B0,B1,C1), (A0,A1,B1,C1)), static
-// geometry (decided_at = -1e9). vc and vn are the worldtube's events at the two samples. ok[k]
-// says whether tetrahedron k is kept (Simplex4D::new skips degenerate ones).
+// mesh4d.rs:776-854; the Dompierre split (A0,B0,C0,C1), (A0,B0,B1,C1), (A0,A1,B1,C1)). vc and vn
+// are the worldtube's events at the two samples, dec0 and dec1 their causal decision stamps
+// (DECIDED_STATIC for static geometry). ok[k] says whether tetrahedron k is kept (Simplex4D::new
+// skips degenerate ones).
 SRH_HD inline void tube_segment(const TubeTri& t, const V4f* vc, const V4f* vn, const TubeSample& sc,
-                                const TubeSample& sn, uint32_t mat, Tet* out, bool* ok) {
-    const float DEC = -1.0e9f;
+                                const TubeSample& sn, uint32_t mat, float dec0, float dec1, Tet* out, bool* ok) {
     V4f ur = sc.e[0] + sn.e[0];
     V4f u = ur * (1.0f / std::sqrt(mx(-ur.mdot(ur), 1e-12f)));
     V4f a0 = vc[t.idx[0]], b0 = vc[t.idx[1]], c0 = vc[t.idx[2]];
@@ -162,7 +165,7 @@ SRH_HD inline void tube_segment(const TubeTri& t, const V4f* vc, const V4f* vn, 
             gr[j][0] = g[0];
             gr[j][1] = g[1];
         }
-        ok[k] = make_tet(V[k], uv, TB[k], TAU[k], gr, uvs_u, uvs_v, nrm, u, mat, DEC, DEC, SEL[k], &out[k]);
+        ok[k] = make_tet(V[k], uv, TB[k], TAU[k], gr, uvs_u, uvs_v, nrm, u, mat, dec0, dec1, SEL[k], &out[k]);
     }
 }
 

@@ -45,6 +45,8 @@ def test_struct_layouts_match_the_reference():
     assert L.ATTR_DTYPE.fields["misc"][1] == 160 and L.ATTR_DTYPE.fields["decided_at"][1] == 176
     assert C.sizeof(L.Tuning) == 48 and L.Tuning.leaf_coop.offset == 24 and L.Tuning.home_pct.offset == 32
     assert C.sizeof(L.Timings) == 96
+    assert L.TRI_DTYPE.itemsize == 48 and L.SAMPLE_DTYPE.itemsize == 112 and C.sizeof(L.Tube) == 48
+    assert C.sizeof(L.ArenaPart) == 16 and C.sizeof(L.ArenaStats) == 48 and L.Tube.decided_at.offset == 40
 
 
 def test_create_without_device_fails_cleanly():

@@ -1,0 +1,142 @@
+"""The engine's scene cache over its device arena (sr_arena_*) against the oracle's (test_arena.py
+holds the oracle to the properties the reference's own tests check): after every snapshot the node
+array and the hot and cold records, free room included, equal the oracle arena's byte for byte, the
+CacheStats agree, and frames rendered from the arena equal frames rendered from the same arrays
+uploaded with sr_upload_scene (the reference's path: the host arena patched into the GPU copy)."""
+import time
+
+import numpy as np
+import pytest
+
+import specrel_b200 as sr
+from oracle import oracle as O
+
+import arena_world as W
+
+pytestmark = pytest.mark.gpu
+
+IDX, UPLOADED = 31, 32
+
+
+@pytest.fixture(scope="module")
+def inputs():
+    sc = sr.synth_scene(1, 1, n_bodies=4, steps=8)
+    boxes, geoms, attrs, p = sc.build_inputs()
+    return sc, sc.tubes()[0], (boxes, geoms, attrs), p
+
+
+def engine_drive(eng, w, k, rest, idx=IDX):
+    return w.drive(k, lambda: eng.arena_begin(idx),
+                   lambda part, s, d, m: eng.arena_tube(idx, part, sr.TubeData(w.vertices, w.triangles, s, m, d)),
+                   lambda part, i, key, b, g, a: eng.arena_piece(idx, part, i, key, b, g, a),
+                   lambda b, g, a: eng.arena_finish(idx, rest, b, g, a))
+
+
+def oracle_drive(A, w, k):
+    return w.drive(k, A.begin, lambda part, s, d, m: A.tube(part, w.vertices, w.triangles, s, m, d), A.piece,
+                   A.finish)
+
+
+def assert_same_arena(eng, A, idx=IDX):
+    nodes, order = eng.tree(idx)
+    g, a = eng.records(idx)
+    on, og, oa = A.arrays()
+    assert len(nodes) == len(on) and len(g) == len(og)
+    assert nodes.tobytes() == on.tobytes()
+    assert g.tobytes() == og.tobytes() and a.tobytes() == oa.tobytes()
+    assert (order == np.arange(len(g))).all()  # hit ids are arena slots
+    return on, og, oa
+
+
+def assert_same_frames(eng, arrays, p, yaw):
+    nodes, geoms, attrs = arrays
+    up = sr.PackedScene(nodes, geoms, attrs, p.materials, np.zeros(4, np.float32), 0, tuple(p.light_pos),
+                        anchor=p.anchor)
+    eng.upload(UPLOADED, up)
+    u = sr.uniforms(sr.camera(fov_deg=100.0, yaw=yaw), 320, 200, 0, 1, 0, num_nodes=len(nodes),
+                    light_pos=tuple(p.light_pos))
+    hits = 0
+    for path in (sr.SR_PATH_FAST, sr.SR_PATH_PLAIN):
+        fa = eng.render(IDX, u, path=path, aux=True)
+        fb = eng.render(UPLOADED, u, path=path, aux=True)
+        assert (fa.rgb == fb.rgb).all() and (fa.hit_id == fb.hit_id).all() and (fa.lam == fb.lam).all()
+        hits = int((fa.hit_id != 0xFFFFFFFF).sum())
+    return hits
+
+
+def test_device_arena_equals_the_oracle_arena(engine, inputs):
+    sc, tube, simplices, p = inputs
+    w = W.World(tube, simplices)
+    A = O.Arena()
+    hits = 0
+    for k in range(10):
+        es = engine_drive(engine, w, k, sc)
+        os_ = oracle_drive(A, w, k)
+        for key, v in os_.items():
+            assert es[key] == v, (k, key, es, os_)
+        arrays = assert_same_arena(engine, A)
+        assert es["num_nodes"] == len(arrays[0])
+        if k in (0, 4, 9):
+            hits += assert_same_frames(engine, arrays, p, yaw=90.0 * (k % 4))
+    assert hits > 1000
+
+
+def test_device_arena_rebase_compacts_as_the_oracle(engine, inputs):
+    sc, tube, simplices, p = inputs
+    w = W.World(tube, simplices, n_bodies=12, base=60)
+    A = O.Arena()
+    for k in range(3):
+        engine_drive(engine, w, k, sc)
+        oracle_drive(A, w, k)
+    w.shift = -7.25
+    compacted = 0
+    for _ in range(3):
+        es = engine_drive(engine, w, 3, sc)
+        os_ = oracle_drive(A, w, 3)
+        assert {k: es[k] for k in os_} == os_
+        compacted += es["compacted"]
+        arrays = assert_same_arena(engine, A)
+    assert compacted == 1
+    assert_same_frames(engine, arrays, p, yaw=0.0)
+
+
+def test_empty_snapshot_and_restart(engine, inputs):
+    """A snapshot with nothing in it leaves the root over nothing (no hits, sky only); a scene
+    uploaded or built at the index makes the next snapshot start afresh."""
+    sc, tube, simplices, p = inputs
+    engine.arena_begin(IDX + 5)
+    st = engine.arena_finish(IDX + 5, sc)
+    assert st["num_nodes"] == 1 and st["arena_simplices"] == 0
+    u = sr.uniforms(sr.camera(), 64, 40, 0, 1, 0, num_nodes=1)
+    for path in (sr.SR_PATH_FAST, sr.SR_PATH_PLAIN):
+        f = engine.render(IDX + 5, u, path=path, aux=True)
+        assert (f.hit_id == 0xFFFFFFFF).all()
+    engine.upload(IDX + 5, sc)
+    w = W.World(tube, simplices)
+    A = O.Arena()
+    engine_drive(engine, w, 0, sc, idx=IDX + 5)
+    oracle_drive(A, w, 0)
+    assert_same_arena(engine, A, idx=IDX + 5)
+    with pytest.raises(sr.SrError):
+        engine.arena_tube(IDX + 5, (0, 0, 1), sr.TubeData(w.vertices, w.triangles, w.tube_of(0, 0)[0], 0))
+
+
+def test_snapshot_timing(engine, inputs):
+    """The per-snapshot cost the reference measures (bench.rs:213-218, rebuild + GPU patch): a world
+    of 12 bodies with long histories, three new samples per body per snapshot; the whole
+    sr_arena_* sequence timed on the host, against the oracle's host scene cache."""
+    sc, tube, simplices, p = inputs
+    w = W.World(tube, simplices, n_bodies=12, base=200)
+    A = O.Arena()
+    te, to, stats = [], [], None
+    for k in range(8):
+        t0 = time.perf_counter()
+        stats = engine_drive(engine, w, k, sc)
+        te.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        oracle_drive(A, w, k)
+        to.append(time.perf_counter() - t0)
+    assert_same_arena(engine, A)
+    print(f"snapshot of {stats['arena_simplices']} simplices ({stats['simplices_built']} new): device arena "
+          f"{np.median(te[2:]) * 1e3:.2f} ms, oracle scene cache on the host {np.median(to[2:]) * 1e3:.2f} ms "
+          f"(medians of 6)")
