@@ -201,6 +201,7 @@ struct ArenaCache {
     std::vector<NewTube> tubes;
     std::vector<NewPrims> prims_in;
     std::vector<uint32_t> key;  // scratch
+    std::map<std::vector<uint32_t>, uint32_t> mesh_ids;  // each distinct mesh's bits, interned
 
     ArenaCache() { nodes.end = 1; }  // node 0 is the root
 
@@ -328,7 +329,8 @@ sr_status sr_arena_tube(sr_ctx* ctx, uint32_t idx, SrArenaPart part, const SrTub
         return fail(ctx, SR_ERR_INVALID_ARGUMENT, "tube: too many samples");
     ArenaCache& a = *ap;
     if (t.num_samples < 2) return SR_OK;
-    // The mesh's bits, standing for mesh_fingerprint (scene_cache.rs:368-380) in every chunk's key.
+    // The mesh's bits stand for mesh_fingerprint (scene_cache.rs:368-380): interned once, the
+    // chunks' keys hold the mesh's id (equal ids, equal meshes).
     std::vector<uint32_t> mesh;
     mesh.push_back(t.num_vertices);
     mesh.push_back(t.num_triangles);
@@ -341,6 +343,7 @@ sr_status sr_arena_tube(sr_ctx* ctx, uint32_t idx, SrArenaPart part, const SrTub
         const uint32_t* w = reinterpret_cast<const uint32_t*>(&t.triangles[i]);
         mesh.insert(mesh.end(), w, w + sizeof(SrTubeTriangle) / 4);
     }
+    const uint32_t mesh_id = a.mesh_ids.emplace(std::move(mesh), (uint32_t)a.mesh_ids.size()).first->second;
     auto bucket = [&](uint32_t i) -> int64_t {  // (center.t / CHUNK_T).floor() as i64
         const double f = std::floor((double)(t.samples[i].center[0] / CHUNK_T));
         if (std::isnan(f)) return 0;
@@ -358,7 +361,7 @@ sr_status sr_arena_tube(sr_ctx* ctx, uint32_t idx, SrArenaPart part, const SrTub
         key.clear();
         key.push_back(t.material);
         key.push_back(t.decided_at ? 1u : 0u);
-        key.insert(key.end(), mesh.begin(), mesh.end());
+        key.push_back(mesh_id);
         for (uint32_t i = first; i <= end; ++i) push_sample_key(key, t.samples[i]);
         if (t.decided_at)
             for (uint32_t i = first; i <= end; ++i) {

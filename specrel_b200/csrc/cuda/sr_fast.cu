@@ -117,8 +117,8 @@ cudaError_t fast_build(FastCtx& c, FastScene& s, const SrGpuNode* nodes, uint32_
     cudaMemcpyAsync(&last[1], flags + n - 1, 4, cudaMemcpyDeviceToHost, st);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
     s.num_wide = last[0] + last[1];
-    if ((e = s.boxes.ensure((size_t)s.num_wide * 64 * 16)) != cudaSuccess) return e;
-    if ((e = s.refs.ensure((size_t)s.num_wide * 8)) != cudaSuccess) return e;
+    if ((e = s.boxes.ensure_grow((size_t)s.num_wide * 64 * 16)) != cudaSuccess) return e;
+    if ((e = s.refs.ensure_grow((size_t)s.num_wide * 8)) != cudaSuccess) return e;
     k_wide_fill<<<(n + 255) / 256, 256, 0, st>>>(nodes, n, wid, s.boxes.as<float4>(), 4ull * s.num_wide,
                                                  s.refs.as<uint2>());
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <map>
 #include <vector>
@@ -25,6 +26,12 @@ struct DevMem {
         cudaError_t e = cudaMalloc(&p, n);
         if (e == cudaSuccess) bytes = n;
         return e;
+    }
+    // As ensure, but a buffer that has to grow grows by a quarter more than asked, so that a scene
+    // rebuilt with slowly growing arrays (an arena) does not reallocate at every rebuild.
+    cudaError_t ensure_grow(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        return ensure(p ? std::max(n, bytes + bytes / 4) : n);
     }
     template <class T> T* as() const { return reinterpret_cast<T*>(p); }
 };

@@ -6,10 +6,15 @@
 // precomputed integer keys, and each node's order on every axis is handed down to its children by
 // a stable partition. A child whose inherited order has no ties on an axis takes it as is (a strict
 // order is what any stable sort gives); only orders with ties are sorted again, by an
-// allocation-free stable merge sort, from the order the reference sorts.
+// allocation-free stable merge sort, from the order the reference sorts. A subtree over m items
+// has m - 1 nodes, so each subtree's node slots are known before it is built, and subtrees of 256
+// items or more are built on threads of their own.
+#include <immintrin.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <future>
 #include <vector>
 
 #include "../../../include/specrel.h"
@@ -23,27 +28,22 @@ inline int32_t total_key(float f) {  // f32::total_cmp as an integer order
     return b ^ (int32_t)((uint32_t)(b >> 31) >> 1);
 }
 
-inline float box_measure(const float* lo, const float* hi) {  // bvh4d.rs:8-13, (t, x, y, z)
-    const float et = hi[0] - lo[0], ex = hi[1] - lo[1], ey = hi[2] - lo[2], ez = hi[3] - lo[3];
-    const float spatial = ex * ey + ey * ez + ez * ex;
-    const float temporal = 0.22f * et * (ex + ey + ez);
+// Aabb4D::union. Boxes hold no NaN and no -0 (simplex boxes are padded by 1e-4), where SSE's
+// min / max (and a compare-select) give f32::min / max's values.
+struct Box4 {
+    __m128 lo, hi;
+};
+inline Box4 empty4() { return {_mm_set1_ps(INFINITY), _mm_set1_ps(-INFINITY)}; }
+inline void unite4(Box4& b, const float* item) {
+    b.lo = _mm_min_ps(b.lo, _mm_loadu_ps(item));
+    b.hi = _mm_max_ps(b.hi, _mm_loadu_ps(item + 4));
+}
+inline float measure4(const Box4& b) {  // box_measure (bvh4d.rs:8-13) on (t, x, y, z) lanes
+    alignas(16) float e[4];
+    _mm_store_ps(e, _mm_sub_ps(b.hi, b.lo));
+    const float spatial = e[1] * e[2] + e[2] * e[3] + e[3] * e[1];
+    const float temporal = 0.22f * e[0] * (e[1] + e[2] + e[3]);
     return spatial + temporal;
-}
-
-// Aabb4D::union. Boxes hold no NaN and no -0 (simplex boxes are padded by 1e-4), where a
-// compare-select gives f32::min / max's values without a libm call.
-inline void unite(float* lo, float* hi, const float* blo, const float* bhi) {
-    for (int k = 0; k < 4; ++k) {
-        lo[k] = blo[k] < lo[k] ? blo[k] : lo[k];
-        hi[k] = bhi[k] > hi[k] ? bhi[k] : hi[k];
-    }
-}
-
-inline void empty_box(float* lo, float* hi) {
-    for (int k = 0; k < 4; ++k) {
-        lo[k] = INFINITY;
-        hi[k] = -INFINITY;
-    }
 }
 
 struct Builder {
@@ -57,12 +57,12 @@ struct Builder {
     std::vector<uint32_t> buf;      // merge scratch
     std::vector<uint32_t> saved[4]; // saved[a][lo, hi): the node's items in its order on axis a
     std::vector<uint8_t> side;      // per item: 0 left, 1 right of the current split
-    std::vector<float> rlo, rhi, rw;
+    std::vector<float> rm, rw;  // per position: the right side's measure and weight
     std::vector<SrGpuNode> out;
-    uint32_t max_depth = 0;
 
-    // Stable sort of v[0, n) by k: insertion-sorted runs of 16, then bottom-up merges.
-    void stable_sort(uint32_t* v, size_t n, const int32_t* k) {
+    // Stable sort of v[0, n) by k: insertion-sorted runs of 16, then bottom-up merges through
+    // `scratch` (n entries).
+    static void stable_sort(uint32_t* v, size_t n, const int32_t* k, uint32_t* scratch) {
         const size_t RUN = 16;
         for (size_t s = 0; s < n; s += RUN) {
             const size_t e = std::min(n, s + RUN);
@@ -79,7 +79,7 @@ struct Builder {
         }
         if (n <= RUN) return;
         uint32_t* src = v;
-        uint32_t* dst = buf.data();
+        uint32_t* dst = scratch;
         for (size_t w = RUN; w < n; w *= 2) {
             for (size_t s = 0; s < n; s += 2 * w) {
                 const size_t m = std::min(n, s + w), e = std::min(n, s + 2 * w);
@@ -101,31 +101,33 @@ struct Builder {
     }
 
     // Stable partition of v[0, n) by side: the left items first.
-    void partition(uint32_t* v, size_t n) {
+    void partition(uint32_t* v, size_t n, uint32_t* scratch) {
         size_t l = 0, r = 0;
         for (size_t i = 0; i < n; ++i) {
             if (side[v[i]] == 0) v[l++] = v[i];
-            else buf[r++] = v[i];
+            else scratch[r++] = v[i];
         }
-        std::memcpy(v + l, buf.data(), r * sizeof(uint32_t));
+        std::memcpy(v + l, scratch, r * sizeof(uint32_t));
     }
 
-    // The subtree over order[a, b); returns its node index. `levels`: tree nodes above it.
-    // `inherited`: saved[*][a, b) holds the parent's orders restricted to these items.
-    uint32_t build(size_t a, size_t b, uint32_t levels, bool inherited) {
+    // The subtree over order[a, b); returns its node index and raises `max_d` to its depth.
+    // `levels`: tree nodes above it. `inherited`: saved[*][a, b) holds the parent's orders
+    // restricted to these items. Its nodes take out[slot, slot + b - a - 1) in depth-first order
+    // (a subtree over m items has m - 1 nodes), so subtrees can be built concurrently; every
+    // scratch array is used in the subtree's own range [a, b).
+    uint32_t build(size_t a, size_t b, uint32_t levels, bool inherited, size_t slot, uint32_t& max_d, int spawn) {
         const size_t n = b - a;
         if (n == 1) {
             const uint32_t it = order[a];
-            max_depth = std::max(max_depth, levels + depth[it]);
+            max_d = std::max(max_d, levels + depth[it]);
             return root[it];
         }
-        const size_t slot = out.size();
-        SrGpuNode blank{};
-        out.push_back(blank);
         const uint32_t at = slot == 0 ? 0u : base + (uint32_t)slot - 1;
-        float blo[4], bhi[4];
-        empty_box(blo, bhi);
-        for (size_t i = a; i < b; ++i) unite(blo, bhi, box + 8 * order[i], box + 8 * order[i] + 4);
+        uint32_t* scratch = buf.data() + a;
+        float* rm_ = rm.data() + a;
+        float* rw_ = rw.data() + a;
+        Box4 bounds = empty4();
+        for (size_t i = a; i < b; ++i) unite4(bounds, box + 8 * order[i]);
 
         float best_cost = INFINITY;
         int best_axis = 0;
@@ -137,28 +139,27 @@ struct Builder {
             if (inherited && strict(sv, n, key[axis].data())) {
                 std::memcpy(v, sv, n * sizeof(uint32_t));
             } else {
-                stable_sort(v, n, key[axis].data());
+                stable_sort(v, n, key[axis].data(), scratch);
                 std::memcpy(sv, v, n * sizeof(uint32_t));
             }
-            float alo[4], ahi[4];
-            empty_box(alo, ahi);
+            // The right sides' boxes accumulated from the end (their measures kept), then the
+            // left sides' from the front: cost = left weight * measure + right weight * measure.
+            Box4 acc = empty4();
             float aw = 0.0f;
             for (size_t j = n - 1; j >= 1; --j) {
                 const uint32_t it = v[j];
-                unite(alo, ahi, box + 8 * it, box + 8 * it + 4);
+                unite4(acc, box + 8 * it);
                 aw = aw + weight[it];
-                std::memcpy(&rlo[4 * j], alo, 16);
-                std::memcpy(&rhi[4 * j], ahi, 16);
-                rw[j] = aw;
+                rm_[j] = measure4(acc);
+                rw_[j] = aw;
             }
-            float llo[4], lhi[4];
-            empty_box(llo, lhi);
+            Box4 left_box = empty4();
             float lw = 0.0f;
             for (size_t j = 1; j < n; ++j) {
                 const uint32_t it = v[j - 1];
-                unite(llo, lhi, box + 8 * it, box + 8 * it + 4);
+                unite4(left_box, box + 8 * it);
                 lw = lw + weight[it];
-                const float cost = lw * box_measure(llo, lhi) + rw[j] * box_measure(&rlo[4 * j], &rhi[4 * j]);
+                const float cost = lw * measure4(left_box) + rw_[j] * rm_[j];
                 if (cost < best_cost) {
                     best_cost = cost;
                     best_axis = axis;
@@ -172,21 +173,34 @@ struct Builder {
             const int32_t* k = key[best_axis].data();
             const uint32_t* sv = saved[best_axis].data() + a;
             if (strict(sv, n, k)) std::memcpy(v, sv, n * sizeof(uint32_t));
-            else stable_sort(v, n, k);
+            else stable_sort(v, n, k, scratch);
         }
         for (size_t i = 0; i < n; ++i) side[v[i]] = i < best_mid ? 0 : 1;
-        for (int axis = 0; axis < 4; ++axis) partition(saved[axis].data() + a, n);
-        const uint32_t left = build(a, a + best_mid, levels + 1, true);
-        const uint32_t right = build(a + best_mid, b, levels + 1, true);
+        for (int axis = 0; axis < 4; ++axis) partition(saved[axis].data() + a, n, scratch);
+        // Left subtree's nodes from slot + 1 (best_mid - 1 of them), the right's after them.
+        uint32_t left, right;
+        if (spawn > 0 && best_mid >= PAR_MIN && n - best_mid >= PAR_MIN) {
+            uint32_t dl = 0;
+            auto fut = std::async(std::launch::async, [&] {
+                return build(a, a + best_mid, levels + 1, true, slot + 1, dl, spawn - 1);
+            });
+            right = build(a + best_mid, b, levels + 1, true, slot + best_mid, max_d, spawn - 1);
+            left = fut.get();
+            max_d = std::max(max_d, dl);
+        } else {
+            left = build(a, a + best_mid, levels + 1, true, slot + 1, max_d, 0);
+            right = build(a + best_mid, b, levels + 1, true, slot + best_mid, max_d, 0);
+        }
         SrGpuNode nd{};
-        std::memcpy(nd.min, blo, 16);
-        std::memcpy(nd.max, bhi, 16);
+        _mm_storeu_ps(nd.min, bounds.lo);
+        _mm_storeu_ps(nd.max, bounds.hi);
         nd.right_or_first = right;
         nd.count = 0;
         nd.left = left;
         out[slot] = nd;
         return at;
     }
+    static constexpr size_t PAR_MIN = 256;  // items of a subtree worth a thread of its own
 };
 
 }  // namespace
@@ -212,12 +226,12 @@ extern "C" sr_status sr_top_tree(const float* boxes, const uint32_t* roots, cons
     bld.order.resize(n);
     for (uint32_t i = 0; i < n; ++i) bld.order[i] = i;
     bld.buf.resize(n);
-    bld.rlo.resize(4 * (size_t)n);
-    bld.rhi.resize(4 * (size_t)n);
+    bld.rm.resize(n);
     bld.rw.resize(n);
-    bld.out.reserve(n - 1);
-    bld.build(0, n, 0, false);
+    bld.out.resize(n - 1);
+    uint32_t max_d = 0;
+    bld.build(0, n, 0, false, 0, max_d, 2);
     std::memcpy(nodes, bld.out.data(), bld.out.size() * sizeof(SrGpuNode));
-    if (depth) *depth = bld.max_depth;
+    if (depth) *depth = max_d;
     return SR_OK;
 }
