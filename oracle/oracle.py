@@ -112,6 +112,8 @@ def lib():
                                       C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
         L.orc_arena_finish.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
         L.orc_arena_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        L.orc_arena_dirty.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_void_p,
+                                      C.POINTER(C.c_uint32), C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32]
         L.orc_arena_pack.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_top_tree.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
         L.orc_tube_simplices.restype = C.c_int64
@@ -410,6 +412,20 @@ class Arena:
             a = np.ascontiguousarray(attrs, ATTR_DTYPE)
             lib().orc_arena_finish(self.h, b.ctypes.data, g.ctypes.data, a.ctypes.data, len(g), st.ctypes.data)
         return dict(zip(self.STAT_KEYS, (int(x) for x in st)))
+
+    def dirty(self):
+        """(layout, edit, node ranges, prim ranges): the arena's version and what its latest edit
+        wrote (Bvh4D::version / dirty)."""
+        lay, ed = C.c_uint64(), C.c_uint64()
+        nn, npr = C.c_uint32(), C.c_uint32()
+        lib().orc_arena_dirty(self.h, C.byref(lay), C.byref(ed), None, C.byref(nn), None, C.byref(npr), 0)
+        cap = max(nn.value, npr.value, 1)
+        nr = np.zeros(2 * cap, np.uint64)
+        pr = np.zeros(2 * cap, np.uint64)
+        lib().orc_arena_dirty(self.h, C.byref(lay), C.byref(ed), nr.ctypes.data, C.byref(nn), pr.ctypes.data,
+                              C.byref(npr), cap)
+        pairs = lambda a, n: [(int(a[2 * i]), int(a[2 * i + 1])) for i in range(n)]
+        return lay.value, ed.value, pairs(nr, nn.value), pairs(pr, npr.value)
 
     def arrays(self):
         nn, npr = C.c_uint32(), C.c_uint32()

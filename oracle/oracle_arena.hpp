@@ -4,7 +4,8 @@
 //   src/dynamic/scene_cache.rs:120-356  SceneCache: begin, reuse, install, tube, piece, finish, compact
 //   src/dynamic/scene_cache.rs:358-366  push_sample (a chunk's key)
 //   src/bvh4d.rs:31-44                  BvhNode4D::NOTHING, moved
-//   src/bvh4d.rs:168-215, 583-591       reset_arena, begin_edit, write_part, write_nodes, put
+//   src/bvh4d.rs:48-61, 157-215, 583-591 BvhVersion, dirty, reset_arena, begin_edit, write_part,
+//                                       write_nodes, put
 //   src/bvh4d.rs:593-644                top_tree
 // The mesh's bits stand for mesh_fingerprint's 64-bit hash of them in a chunk's key (equal keys
 // either way, barring a hash collision).
@@ -78,7 +79,14 @@ template <class T> BvhNode<T> nothing() { return BvhNode<T>{}; }  // empty box, 
 // are kept in leaf order.
 template <class T> struct ArenaBvh {
     Bvh<T> b;
-    uint64_t layout = 0;
+    uint64_t layout = 0, edit = 0;             // BvhVersion (bvh4d.rs:48-61)
+    std::vector<Span> dirty_nodes, dirty_prims;  // what the latest edit wrote
+
+    void begin_edit() {
+        ++edit;
+        dirty_nodes.clear();
+        dirty_prims.clear();
+    }
 
     template <class V, class F> static void put(std::vector<V>& v, size_t at, size_t n, F item) {
         for (size_t i = 0; i < n; ++i) {
@@ -92,6 +100,9 @@ template <class T> struct ArenaBvh {
         b.order.clear();
         b.simplices.clear();
         layout = next_layout();
+        edit = 0;
+        dirty_nodes.clear();
+        dirty_prims.clear();
     }
     void write_part(const Bvh<T>& src, Span nodes, Span prims, size_t node_at, size_t prim_at) {
         const uint32_t dn = (uint32_t)node_at - (uint32_t)nodes.lo, dp = (uint32_t)prim_at - (uint32_t)prims.lo;
@@ -108,9 +119,12 @@ template <class T> struct ArenaBvh {
         put(b.hot, prim_at, prims.size(), [&](size_t i) { return src.hot[prims.lo + i]; });
         put(b.order, prim_at, prims.size(), [&](size_t i) { return (uint32_t)(prim_at + i); });
         put(b.simplices, prim_at, prims.size(), [&](size_t i) { return src.leaf_simplex(prims.lo + i); });
+        dirty_nodes.push_back(Span{node_at, node_at + nodes.size()});
+        dirty_prims.push_back(Span{prim_at, prim_at + prims.size()});
     }
     void write_nodes(size_t at, const BvhNode<T>* nodes, size_t n) {
         put(b.nodes, at, n, [&](size_t i) { return nodes[i]; });
+        dirty_nodes.push_back(Span{at, at + n});
     }
 };
 
@@ -225,6 +239,7 @@ template <class T> struct SceneCacheOracle {
             top = Span{};
             vol_nodes = vol_prims = Span{};
         }
+        arena.begin_edit();
     }
     bool reuse(const CacheChunkId& id, const std::vector<uint32_t>& key) {
         Chunk& c = chunks[id];
@@ -305,6 +320,7 @@ template <class T> struct SceneCacheOracle {
         ArenaBvh<T> old;
         std::swap(old, arena);
         arena.reset();
+        arena.begin_edit();
         layout = arena.layout;
         nodes = FreeList{};
         nodes.end = 1;

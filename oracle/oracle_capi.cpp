@@ -610,6 +610,26 @@ int orc_arena_finish(void* a_, const float* boxes, const void* geoms, const void
     return 0;
 }
 
+// The arena's version and the ranges its latest edit wrote (Bvh4D::version / dirty): ranges as
+// (start, end) pairs, up to `cap` of each; returns via the counts how many there are.
+int orc_arena_dirty(void* a_, uint64_t* layout, uint64_t* edit, uint64_t* nodes, uint32_t* n_nodes, uint64_t* prims,
+                    uint32_t* n_prims, uint32_t cap) {
+    auto* a = (ArenaBox*)a_;
+    *layout = a->arena.layout;
+    *edit = a->arena.edit;
+    *n_nodes = (uint32_t)a->arena.dirty_nodes.size();
+    *n_prims = (uint32_t)a->arena.dirty_prims.size();
+    for (uint32_t i = 0; i < *n_nodes && i < cap; ++i) {
+        nodes[2 * i] = a->arena.dirty_nodes[i].lo;
+        nodes[2 * i + 1] = a->arena.dirty_nodes[i].hi;
+    }
+    for (uint32_t i = 0; i < *n_prims && i < cap; ++i) {
+        prims[2 * i] = a->arena.dirty_prims[i].lo;
+        prims[2 * i + 1] = a->arena.dirty_prims[i].hi;
+    }
+    return 0;
+}
+
 int orc_arena_sizes(void* a_, uint32_t* n_nodes, uint32_t* n_prims) {
     auto* a = (ArenaBox*)a_;
     *n_nodes = (uint32_t)a->arena.b.nodes.size();

@@ -117,3 +117,35 @@ def test_top_tree_equals_the_restatement(n, quant):
     got, depth = sr.top_tree(boxes, roots, weights, base, depths=np.full(n, 3, np.uint32))
     assert got.tobytes() == ref.tobytes()
     assert depth >= 4
+
+
+def test_dirty_ranges_patch_a_copy_into_the_arena():
+    """PackedSceneGpuData::update (gpu.rs:296-315): a copy of the arrays patched with each edit's
+    dirty ranges, when it holds the edit before of the same layout (else copied afresh), equals the
+    arrays; most snapshots are patched (bench.rs:488-510)."""
+    sc = sr.synth_scene(1, 1, n_bodies=4, steps=8)
+    boxes, geoms, attrs, p = sc.build_inputs()
+    w = W.World(sc.tubes()[0], (boxes, geoms, attrs))
+    A = O.Arena()
+    copy, version, patched = None, None, 0
+    for k in range(10):
+        drive(w, A, k)
+        lay, ed, nr, pr = A.dirty()
+        nodes, g, a = A.arrays()
+        if version is not None and version == (lay, ed - 1):
+            cn, cg, ca = copy
+            cn = np.concatenate([cn, np.zeros(max(0, len(nodes) - len(cn)), cn.dtype)])
+            cg = np.concatenate([cg, np.zeros(max(0, len(g) - len(cg)), cg.dtype)])
+            ca = np.concatenate([ca, np.zeros(max(0, len(a) - len(ca)), ca.dtype)])
+            for s, e in nr:
+                cn[s:e] = nodes[s:e]
+            for s, e in pr:
+                cg[s:e] = g[s:e]
+                ca[s:e] = a[s:e]
+            copy = (cn, cg, ca)
+            patched += 1
+        else:
+            copy = (nodes.copy(), g.copy(), a.copy())
+        version = (lay, ed)
+        assert all(x.tobytes() == y.tobytes() for x, y in zip(copy, (nodes, g, a))), k
+    assert patched == 9

@@ -48,7 +48,7 @@ def assert_same_arena(eng, A, idx=IDX):
     return on, og, oa
 
 
-def assert_same_frames(eng, arrays, p, yaw):
+def assert_same_frames(eng, arrays, p, yaw, idx=IDX):
     nodes, geoms, attrs = arrays
     up = sr.PackedScene(nodes, geoms, attrs, p.materials, np.zeros(4, np.float32), 0, tuple(p.light_pos),
                         anchor=p.anchor)
@@ -57,7 +57,7 @@ def assert_same_frames(eng, arrays, p, yaw):
                     light_pos=tuple(p.light_pos))
     hits = 0
     for path in (sr.SR_PATH_FAST, sr.SR_PATH_PLAIN):
-        fa = eng.render(IDX, u, path=path, aux=True)
+        fa = eng.render(idx, u, path=path, aux=True)
         fb = eng.render(UPLOADED, u, path=path, aux=True)
         assert (fa.rgb == fb.rgb).all() and (fa.hit_id == fb.hit_id).all() and (fa.lam == fb.lam).all()
         hits = int((fa.hit_id != 0xFFFFFFFF).sum())
@@ -85,19 +85,55 @@ def test_device_arena_rebase_compacts_as_the_oracle(engine, inputs):
     sc, tube, simplices, p = inputs
     w = W.World(tube, simplices, n_bodies=12, base=60)
     A = O.Arena()
+    idx = IDX + 10
     for k in range(3):
-        engine_drive(engine, w, k, sc)
+        engine_drive(engine, w, k, sc, idx)
         oracle_drive(A, w, k)
     w.shift = -7.25
     compacted = 0
     for _ in range(3):
-        es = engine_drive(engine, w, 3, sc)
+        es = engine_drive(engine, w, 3, sc, idx)
         os_ = oracle_drive(A, w, 3)
         assert {k: es[k] for k in os_} == os_
         compacted += es["compacted"]
-        arrays = assert_same_arena(engine, A)
+        arrays = assert_same_arena(engine, A, idx)
     assert compacted == 1
-    assert_same_frames(engine, arrays, p, yaw=0.0)
+    assert_same_frames(engine, arrays, p, yaw=0.0, idx=idx)
+
+
+def test_the_reference_flow_patches_the_gpu_copy(engine, inputs):
+    """The reference's own dynamic flow on the drop-in boundary: the host arena (the oracle's) is
+    patched into the device copy with each edit's dirty ranges through sr_update_scene when the copy
+    holds the previous edit of the same layout, else uploaded afresh (update_scene, gpu.rs:704-731);
+    the copy then equals the host arena and renders as the device arena does."""
+    sc, tube, simplices, p = inputs
+    w = W.World(tube, simplices)
+    A = O.Arena()
+    idx = IDX + 20
+    version, patched = None, 0
+    for k in range(10):
+        engine_drive(engine, w, k, sc, idx)
+        oracle_drive(A, w, k)
+        lay, ed, nr, pr = A.dirty()
+        nodes, g, a = A.arrays()
+        up = sr.PackedScene(nodes, g, a, p.materials, np.zeros(4, np.float32), 0, tuple(p.light_pos), anchor=p.anchor)
+        if version == (lay, ed - 1):
+            engine.update(UPLOADED, up, node_ranges=nr, prim_ranges=pr)
+            patched += 1
+        else:
+            engine.upload(UPLOADED, up)
+        version = (lay, ed)
+        dn, _ = engine.tree(UPLOADED)
+        dg, da = engine.records(UPLOADED)
+        assert dn.tobytes() == nodes.tobytes() and dg.tobytes() == g.tobytes() and da.tobytes() == a.tobytes()
+        if k in (3, 9):
+            u = sr.uniforms(sr.camera(fov_deg=100.0, yaw=90.0 * k), 320, 200, 0, 1, 0, num_nodes=len(nodes),
+                            light_pos=tuple(p.light_pos))
+            for path in (sr.SR_PATH_FAST, sr.SR_PATH_PLAIN):
+                fa = engine.render(idx, u, path=path, aux=True)
+                fb = engine.render(UPLOADED, u, path=path, aux=True)
+                assert (fa.rgb == fb.rgb).all() and (fa.hit_id == fb.hit_id).all()
+    assert patched == 9
 
 
 def test_empty_snapshot_and_restart(engine, inputs):
@@ -128,15 +164,16 @@ def test_snapshot_timing(engine, inputs):
     sc, tube, simplices, p = inputs
     w = W.World(tube, simplices, n_bodies=12, base=200)
     A = O.Arena()
+    idx = IDX + 30
     te, to, stats = [], [], None
     for k in range(8):
         t0 = time.perf_counter()
-        stats = engine_drive(engine, w, k, sc)
+        stats = engine_drive(engine, w, k, sc, idx)
         te.append(time.perf_counter() - t0)
         t0 = time.perf_counter()
         oracle_drive(A, w, k)
         to.append(time.perf_counter() - t0)
-    assert_same_arena(engine, A)
+    assert_same_arena(engine, A, idx)
     print(f"snapshot of {stats['arena_simplices']} simplices ({stats['simplices_built']} new): device arena "
           f"{np.median(te[2:]) * 1e3:.2f} ms, oracle scene cache on the host {np.median(to[2:]) * 1e3:.2f} ms "
           f"(medians of 6)")
