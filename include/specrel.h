@@ -276,7 +276,9 @@ typedef struct SrTube {
  * the Dompierre split of each triangle between consecutive samples, degenerate tetrahedra skipped)
  * in tube order, then the tree and packing of sr_build_scene. `rest` supplies materials, stars,
  * light_pos and anchor (its boxes, geoms and attrs are not used). The records equal the host
- * builder's bit for bit. */
+ * builder's bit for bit. A tube that crosses its Rindler horizon (1 + a_local . p <= 0 for a
+ * vertex at a sample, where the reference asserts, mesh4d.rs:738-751) is extruded all the same,
+ * as the host builder does, and flagged in SrSceneStats.rindler_crossed. */
 sr_status sr_build_scene_tubes(sr_ctx* ctx, uint32_t scene_idx, const SrTube* tubes, uint32_t num_tubes,
                                const SrBuildDesc* rest);
 /* The device scene's node array and leaf order (leaf slot -> build index) read back. Either buffer
@@ -310,7 +312,7 @@ typedef struct SrArenaStats {         /* CacheStats (scene_cache.rs:59-70) */
     uint32_t compacted;
     uint32_t num_nodes;               /* node slots in use or free */
     uint32_t bvh_depth;
-    uint32_t pad;
+    uint32_t rindler_crossed;         /* a new chunk's tube crosses its Rindler horizon (see below) */
 } SrArenaStats;
 /* SceneCache::begin: start a snapshot into the arena at `scene_idx`. */
 sr_status sr_arena_begin(sr_ctx* ctx, uint32_t scene_idx);
@@ -330,14 +332,20 @@ sr_status sr_arena_install(sr_ctx* ctx, uint32_t scene_idx, SrArenaPart part, in
 /* SceneCache::finish: chunks unused this snapshot are dropped, new chunks built on the device and
  * written, `desc`'s simplices (the volatile part, may be empty) built afresh as one more chunk,
  * the tree over all chunks written, and the B200 node layout rebuilt; materials, stars, light
- * and anchor come from `desc`. `stats` (optional) receives the snapshot's CacheStats. */
+ * and anchor come from `desc`. `stats` (optional) receives the snapshot's CacheStats. A failure
+ * before the arena is written (invalid input) undoes the snapshot: the scene and the cache are as
+ * they were, and so they are after a snapshot begun and never finished; a later failure (device
+ * memory) leaves no scene at the index, and the next snapshot starts afresh. A tube crossing its
+ * Rindler horizon (1 + a_local . p <= 0 for a vertex at a sample, mesh4d.rs:738-751, where the
+ * reference asserts) is extruded all the same, as the host builders do, and flagged in
+ * `rindler_crossed`. */
 sr_status sr_arena_finish(sr_ctx* ctx, uint32_t scene_idx, const SrBuildDesc* desc, SrArenaStats* stats);
 
 typedef struct SrSceneStats {
     uint32_t num_nodes, num_prims, num_stars, bvh_depth;
     uint64_t device_bytes;
     uint32_t fast_nodes;   /* nodes of the B200 layout */
-    uint32_t pad;
+    uint32_t rindler_crossed; /* built from tubes, some vertex at some sample has 1 + a_local . p <= 0 */
 } SrSceneStats;
 sr_status sr_scene_stats(const sr_ctx* ctx, uint32_t scene_idx, SrSceneStats* out);
 

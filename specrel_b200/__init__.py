@@ -441,7 +441,7 @@ class Engine:
         st = _lib.ArenaStats()
         _check(self.L.sr_arena_finish(self.h, idx, C.byref(d), C.byref(st)), self.h, "arena_finish")
         self.scenes[idx] = rest
-        return {k: getattr(st, k) for k, _ in _lib.ArenaStats._fields_ if k != "pad"}
+        return {k: getattr(st, k) for k, _ in _lib.ArenaStats._fields_}
 
     def records(self, idx: int):
         """The device scene's hot and cold records (leaf order)."""

@@ -85,7 +85,7 @@ class ArenaPart(C.Structure):
 class ArenaStats(C.Structure):
     _fields_ = [("chunks_built", C.c_uint32), ("chunks_reused", C.c_uint32), ("simplices_built", C.c_uint64),
                 ("simplices_reused", C.c_uint64), ("arena_simplices", C.c_uint64), ("compacted", C.c_uint32),
-                ("num_nodes", C.c_uint32), ("bvh_depth", C.c_uint32), ("pad", C.c_uint32)]
+                ("num_nodes", C.c_uint32), ("bvh_depth", C.c_uint32), ("rindler_crossed", C.c_uint32)]
 
 
 class Range(C.Structure):
@@ -119,7 +119,7 @@ class RenderOpts(C.Structure):
 class SceneStats(C.Structure):
     _fields_ = [("num_nodes", C.c_uint32), ("num_prims", C.c_uint32), ("num_stars", C.c_uint32),
                 ("bvh_depth", C.c_uint32), ("device_bytes", C.c_uint64), ("fast_nodes", C.c_uint32),
-                ("pad", C.c_uint32)]
+                ("rindler_crossed", C.c_uint32)]
 
 
 class AdjointResult(C.Structure):

@@ -202,14 +202,36 @@ struct ArenaCache {
     std::vector<NewPrims> prims_in;
     std::vector<uint32_t> key;  // scratch
     std::map<std::vector<uint32_t>, uint32_t> mesh_ids;  // each distinct mesh's bits, interned
+    // What this snapshot changed before anything is written, to undo a snapshot that fails or is
+    // never finished: the free lists at sr_arena_begin and the chunks replaced since (whether they
+    // existed, and their state then).
+    Space nodes0, prims0;
+    std::map<ChunkId, std::pair<bool, Chunk>> journal;
 
     ArenaCache() { nodes.end = 1; }  // node 0 is the root
 
+    void rollback() {
+        for (auto& kv : journal) {
+            if (kv.second.first) chunks[kv.first] = std::move(kv.second.second);
+            else chunks.erase(kv.first);
+        }
+        journal.clear();
+        nodes = nodes0;
+        prims = prims0;
+        for (auto& kv : chunks) {
+            kv.second.fresh = -1;
+            kv.second.made = false;
+        }
+    }
+
     // SceneCache::reuse (scene_cache.rs:168-192). Returns 1 reused, 0 not, -1 used twice.
     int reuse(const ChunkId& id, const std::vector<uint32_t>& k) {
-        Chunk& c = chunks[id];
+        auto found = chunks.find(id);
+        const bool existed = found != chunks.end();
+        Chunk& c = existed ? found->second : chunks[id];
         if (c.used == generation) return -1;
         const bool reused = c.used != 0 && c.key == k;
+        if (!reused && !journal.count(id)) journal.emplace(id, std::make_pair(existed, existed ? c : Chunk{}));
         if (reused) {
             stats.chunks_reused += 1;
             stats.simplices_reused += c.prims.len();
@@ -300,16 +322,16 @@ sr_status sr_arena_begin(sr_ctx* ctx, uint32_t idx) {
     SceneSlot& s = *ctx->scenes[idx];
     if (!s.arena) s.arena = std::make_shared<ArenaCache>();  // a fresh layout (SceneCache::begin)
     ArenaCache& a = *s.arena;
+    if (a.open) a.rollback();  // a snapshot begun and never finished is undone
     a.generation += 1;
     a.order.clear();
     a.stats = SrArenaStats{};
     a.fresh.clear();
     a.tubes.clear();
     a.prims_in.clear();
-    for (auto it = a.chunks.begin(); it != a.chunks.end();) {  // made by a snapshot never finished
-        if (it->second.made) it = a.chunks.erase(it);
-        else ++it;
-    }
+    a.journal.clear();
+    a.nodes0 = a.nodes;
+    a.prims0 = a.prims;
     a.open = true;
     return SR_OK;
 }
@@ -441,17 +463,22 @@ sr_status sr_arena_finish(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d, SrAre
     cudaStream_t st = ctx->stream;
     SceneSlot& s = *ctx->scenes[idx];
     a.open = false;
-    // Whatever fails from here leaves no scene at the index and the next snapshot starts afresh.
+    // Until the arrays are written, a failure undoes the snapshot (the scene and its cache are as
+    // they were); after, it leaves no scene at the index.
     struct Abandon {
         SceneSlot* s;
-        bool armed = true;
+        ArenaCache* a;
+        bool armed = false, done = false;
         ~Abandon() {
+            if (done) return;
             if (armed) {
                 s->present = false;
                 s->arena.reset();
+            } else {
+                a->rollback();
             }
         }
-    } abandon{&s};
+    } abandon{&s, &a};
     std::shared_ptr<ArenaCache> hold = s.arena;  // `a` outlives the slot's reference on failure
     CK(keep_build_pool(), "memory pool");
 
@@ -474,6 +501,7 @@ sr_status sr_arena_finish(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d, SrAre
         }
     } free_ex{&ex, st};
     if (!tv.empty()) CK(gpu_extrude(tv.data(), (uint32_t)tv.size(), &ex, st, tube_first.data()), "extrude");
+    a.stats.rindler_crossed = ex.rindler_bad;
     std::vector<GpuSegment> segs;
     std::vector<size_t> seg_of_fresh(a.fresh.size());
     uint64_t total = ex.num_prims;
@@ -551,6 +579,7 @@ sr_status sr_arena_finish(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d, SrAre
 
     // 2. SceneCache::finish (scene_cache.rs:281-336): drop unused chunks, free the old top tree and
     // volatile part, compact if the free room is too large, place the new chunks, the tree.
+    abandon.armed = true;
     const uint64_t gen = a.generation;
     for (auto it = a.chunks.begin(); it != a.chunks.end();) {
         if (it->second.used != gen) {
@@ -729,6 +758,7 @@ sr_status sr_arena_finish(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d, SrAre
     s.depth = depth;
     s.has_l2o = false;
     s.empty_tree = items.empty();
+    s.rindler_crossed = a.stats.rindler_crossed != 0;
     CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, depth, s.num_prims, max_leaf, st),
        "build node layout");
     s.tuning = fast_default_tuning(ctx->fast);
@@ -736,7 +766,8 @@ sr_status sr_arena_finish(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d, SrAre
     a.tubes.clear();
     a.prims_in.clear();
     s.present = true;
-    abandon.armed = false;
+    a.journal.clear();
+    abandon.done = true;
     if (stats_out) *stats_out = a.stats;
     return SR_OK;
 }

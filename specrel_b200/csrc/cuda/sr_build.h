@@ -40,12 +40,14 @@ cudaError_t keep_build_pool();
 // The simplices of worldtubes (build order) extruded on the device: records and boxes in device
 // buffers from the stream-ordered pool that the caller frees (cudaFreeAsync on the same stream),
 // num_prims of them. With `tube_first` (host, num_tubes + 1 entries), tube b's simplices are
-// [tube_first[b], tube_first[b + 1]).
+// [tube_first[b], tube_first[b + 1]). rindler_bad: some tube of two samples or more has a vertex
+// with 1 + a_local . p <= 0 at some sample (the reference asserts against it).
 struct ExtrudeOut {
     SrGpuGeom* geoms;
     SrGpuAttr* attrs;
     float4* boxes;
     uint32_t num_prims;
+    uint32_t rindler_bad;
 };
 cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out, cudaStream_t st,
                         uint32_t* tube_first = nullptr);

@@ -276,6 +276,7 @@ static sr_status finish_build(sr_ctx* ctx, SceneSlot& s, const float4* box, cons
     s.depth = info.depth;
     s.has_l2o = true;
     s.empty_tree = false;
+    s.rindler_crossed = false;
     s.num_prims = n;
     CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, s.depth, n, info.max_leaf, st),
        "build node layout");
@@ -401,6 +402,7 @@ sr_status sr_build_scene_tubes(sr_ctx* ctx, uint32_t idx, const SrTube* tubes, u
     if (ex.num_prims == 0) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "the tubes hold no simplices");
     r = finish_build(ctx, *slot, ex.boxes, ex.geoms, ex.attrs, ex.num_prims, st);
     if (r != SR_OK) return r;
+    slot->rindler_crossed = ex.rindler_bad != 0;
     return finish_scene(ctx, idx, std::move(slot), d);
 }
 
@@ -444,6 +446,7 @@ sr_status sr_scene_stats(const sr_ctx* ctx, uint32_t idx, SrSceneStats* o) {
     o->bvh_depth = s.depth;
     o->device_bytes = s.nodes.bytes + s.geoms.bytes + s.attrs.bytes + s.mats.bytes + s.stars.bytes + s.l2o.bytes + s.fast.bytes();
     o->fast_nodes = s.fast.num_wide;
+    o->rindler_crossed = s.rindler_crossed ? 1u : 0u;
     return SR_OK;
 }
 

@@ -42,6 +42,7 @@ struct SceneSlot {
     uint32_t depth = 0;
     bool has_l2o = false;
     bool empty_tree = false;  // node 0 is BvhNode4D::NOTHING: nothing to trace
+    bool rindler_crossed = false;  // built from a tube that crosses its Rindler horizon
     FastScene fast;  // the B200 node layout
     SrTuning tuning{};
     std::shared_ptr<ArenaCache> arena;  // the scene cache whose arena these arrays are, if any

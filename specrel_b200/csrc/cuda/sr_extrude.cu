@@ -26,13 +26,35 @@ struct BodyDev {
 };
 constexpr uint32_t NO_DECIDED = 0xFFFFFFFFu;
 
-__global__ void k_tube_events(const BodyDev* bodies, const V3f* verts, const TubeSample* samples, V4f* ev) {
+// The events of every vertex at every sample, and the Rindler horizon bound the reference asserts
+// for a tube of two samples or more (1 + a_local . p > 0, mesh4d.rs:738-751): `bad` is set where it
+// fails.
+__global__ void k_tube_events(const BodyDev* bodies, const V3f* verts, const TubeSample* samples, V4f* ev,
+                              uint32_t* bad) {
     const BodyDev b = bodies[blockIdx.y];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= b.ns * b.nv) return;
     const uint32_t s = i / b.nv, v = i % b.nv;
     const TubeSample& smp = samples[b.samp_off + s];
-    ev[b.ev_off + i] = smp.center + to_world(smp, verts[b.vert_off + v]);
+    const V3f p = verts[b.vert_off + v];
+    if (b.ns >= 2 && !(1.0f + smp.accel.dot(p) > 0.0f)) atomicOr(bad, 1u);
+    ev[b.ev_off + i] = smp.center + to_world(smp, p);
+}
+
+// The same bound on the host, for tubes that make no tetrahedra (no triangles).
+bool rindler_ok(const SrTube* tubes, uint32_t num_tubes) {
+    for (uint32_t b = 0; b < num_tubes; ++b) {
+        const SrTube& t = tubes[b];
+        if (t.num_samples < 2) continue;
+        for (uint32_t s = 0; s < t.num_samples; ++s) {
+            const float* a = t.samples[s].accel;
+            for (uint32_t v = 0; v < t.num_vertices; ++v) {
+                const float* p = t.vertices + 3 * v;
+                if (!(1.0f + (a[0] * p[0] + a[1] * p[1] + a[2] * p[2]) > 0.0f)) return false;
+            }
+        }
+    }
+    return true;
 }
 
 __global__ void k_tube_tets(const BodyDev* bodies, const TubeTri* tris, const TubeSample* samples, const float* dec,
@@ -147,7 +169,10 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
             ncand += 3ull * seg;
         }
     }
-    if (ncand == 0) return cudaSuccess;
+    if (ncand == 0) {
+        out->rindler_bad = rindler_ok(tubes, num_tubes) ? 0u : 1u;
+        return cudaSuccess;
+    }
     DBuf<BodyDev> db;
     DBuf<V3f> dv;
     DBuf<TubeTri> dt;
@@ -157,8 +182,10 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
     DBuf<SrGpuGeom> cg;
     DBuf<SrGpuAttr> ca;
     DBuf<float4> cb;
-    DBuf<uint32_t> valid, pos;
+    DBuf<uint32_t> valid, pos, bad;
     EK(db.alloc(num_tubes, st));
+    EK(bad.alloc(1, st));
+    EK(cudaMemsetAsync(bad.p, 0, 4, st));
     EK(dv.alloc(verts.size(), st));
     EK(dt.alloc(tris.size(), st));
     EK(ds.alloc(samples.size(), st));
@@ -176,7 +203,7 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
     if (!decs.empty())
         EK(cudaMemcpyAsync(ddec.p, decs.data(), decs.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     EK(cudaMemsetAsync(valid.p, 0, (ncand + 1) * 4, st));
-    k_tube_events<<<dim3((max_ev + 255) / 256, num_tubes), 256, 0, st>>>(db.p, dv.p, ds.p, dev.p);
+    k_tube_events<<<dim3((max_ev + 255) / 256, num_tubes), 256, 0, st>>>(db.p, dv.p, ds.p, dev.p, bad.p);
     k_tube_tets<<<dim3((max_seg + 127) / 128, num_tubes), 128, 0, st>>>(db.p, dt.p, ds.p, ddec.p, dev.p, cg.p, ca.p,
                                                                         cb.p, valid.p);
     EK(cudaGetLastError());
@@ -187,6 +214,7 @@ cudaError_t gpu_extrude(const SrTube* tubes, uint32_t num_tubes, ExtrudeOut* out
     EK(cub::DeviceScan::ExclusiveSum(tmp.p, tmp_bytes, valid.p, pos.p, (int)(ncand + 1), st));
     uint32_t n = 0;
     EK(cudaMemcpyAsync(&n, pos.p + ncand, 4, cudaMemcpyDeviceToHost, st));
+    EK(cudaMemcpyAsync(&out->rindler_bad, bad.p, 4, cudaMemcpyDeviceToHost, st));
     DBuf<uint32_t> dfirst;
     if (tube_first) {
         EK(dfirst.alloc(num_tubes + 1, st));

@@ -157,6 +157,52 @@ def test_empty_snapshot_and_restart(engine, inputs):
         engine.arena_tube(IDX + 5, (0, 0, 1), sr.TubeData(w.vertices, w.triangles, w.tube_of(0, 0)[0], 0))
 
 
+def test_a_failed_snapshot_is_undone(engine, inputs):
+    """A snapshot that fails before anything is written (here a tube's material id out of range)
+    leaves the scene rendering as before, and so does one begun and never finished; the next
+    snapshot goes on from the last one written, as the reference's cache would without them."""
+    sc, tube, simplices, p = inputs
+    w = W.World(tube, simplices)
+    idx = IDX + 40
+    engine_drive(engine, w, 0, sc, idx)
+    u = sr.uniforms(sr.camera(fov_deg=100.0), 160, 100, 0, 1, 0, light_pos=tuple(p.light_pos))
+    before = engine.render(idx, u, aux=True)
+    engine.arena_begin(idx)
+    engine.arena_tube(idx, (0, 0, 100), sr.TubeData(w.vertices, w.triangles, w.tube_of(0, 1)[0], 99))
+    with pytest.raises(sr.SrError) as e:
+        engine.arena_finish(idx, sc)
+    assert e.value.status == sr._lib.SR_ERR_BAD_SCENE
+    after = engine.render(idx, u, aux=True)
+    assert (after.rgb == before.rgb).all() and (after.hit_id == before.hit_id).all()
+    engine.arena_begin(idx)
+    engine.arena_tube(idx, (0, 0, 101), sr.TubeData(w.vertices, w.triangles, w.tube_of(1, 3)[0], 1))
+    A = O.Arena()
+    oracle_drive(A, w, 0)
+    engine_drive(engine, w, 1, sc, idx)
+    oracle_drive(A, w, 1)
+    assert_same_arena(engine, A, idx)
+
+
+def test_a_tube_past_its_rindler_horizon_is_flagged(engine, inputs):
+    """Where the reference asserts 1 + a_local . p > 0 (mesh4d.rs:738-751) the tube is extruded all
+    the same, as the host builders do, and the snapshot's stats say so."""
+    sc, tube, simplices, p = inputs
+    w = W.World(tube, simplices)
+    s, _ = w.tube_of(0, 1)
+    s["accel"][3] = (-2.0, 0.0, 0.0)  # 1 + a . p < 0 at the vertices with x = +1.5
+    idx = IDX + 45
+    A = O.Arena()
+    engine.arena_begin(idx)
+    engine.arena_tube(idx, (0, 0, 100), sr.TubeData(w.vertices, w.triangles, s, 0))
+    st = engine.arena_finish(idx, sc)
+    assert st["rindler_crossed"] == 1
+    A.begin()
+    A.tube((0, 0, 100), w.vertices, w.triangles, s, 0)
+    A.finish()
+    assert_same_arena(engine, A, idx)
+    assert engine.stats(idx).rindler_crossed == 1
+
+
 def test_snapshot_timing(engine, inputs):
     """The per-snapshot cost the reference measures (bench.rs:213-218, rebuild + GPU patch): a world
     of 12 bodies with long histories, three new samples per body per snapshot; the whole

@@ -85,6 +85,16 @@ def test_device_build_full_size(engine):
           f"{t_tubes:.3f} s from worldtubes (extrusion included)")
 
 
+def test_device_extrusion_flags_tubes_past_their_rindler_horizon(engine):
+    """The sampled accelerations of configs[1]'s bodies carry the reference's f32 finite-difference
+    noise, which crosses 1 + a_local . p > 0 for vertices of some larger bodies (the host builder
+    records it as rindler_ok = 0): the device build extrudes them all the same and flags it."""
+    for case in (dict(config=2, seed=4, n_bodies=24, steps=24), dict(config=1, seed=1)):
+        scene = sr.synth_scene(**case)
+        engine.build_tubes(27, scene)
+        assert engine.stats(27).rindler_crossed == (0 if scene.info.rindler_ok else 1), case
+
+
 def test_device_build_rejects_empty(engine):
     with pytest.raises(sr.SrError):
         engine.build(21, np.zeros((0, 8), np.float32), np.zeros(0, sr.GEOM_DTYPE), np.zeros(0, sr.ATTR_DTYPE),
