@@ -202,6 +202,7 @@ struct ArenaCache {
     std::vector<NewPrims> prims_in;
     std::vector<uint32_t> key;  // scratch
     std::map<std::vector<uint32_t>, uint32_t> mesh_ids;  // each distinct mesh's bits, interned
+    uint32_t next_mesh_id = 0;  // never reused, so a key made before the map was cleared stays distinct
     // What this snapshot changed before anything is written, to undo a snapshot that fails or is
     // never finished: the free lists at sr_arena_begin and the chunks replaced since (whether they
     // existed, and their state then).
@@ -365,7 +366,12 @@ sr_status sr_arena_tube(sr_ctx* ctx, uint32_t idx, SrArenaPart part, const SrTub
         const uint32_t* w = reinterpret_cast<const uint32_t*>(&t.triangles[i]);
         mesh.insert(mesh.end(), w, w + sizeof(SrTubeTriangle) / 4);
     }
-    const uint32_t mesh_id = a.mesh_ids.emplace(std::move(mesh), (uint32_t)a.mesh_ids.size()).first->second;
+    auto found = a.mesh_ids.find(mesh);
+    if (found == a.mesh_ids.end()) {
+        if (a.mesh_ids.size() >= 1024) a.mesh_ids.clear();  // bounded: chunks of forgotten meshes are rebuilt
+        found = a.mesh_ids.emplace(std::move(mesh), a.next_mesh_id++).first;
+    }
+    const uint32_t mesh_id = found->second;
     auto bucket = [&](uint32_t i) -> int64_t {  // (center.t / CHUNK_T).floor() as i64
         const double f = std::floor((double)(t.samples[i].center[0] / CHUNK_T));
         if (std::isnan(f)) return 0;
