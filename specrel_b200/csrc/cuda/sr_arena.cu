@@ -468,6 +468,7 @@ sr_status sr_arena_finish(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d, SrAre
     CK(cudaSetDevice(ctx->device), "set device");
     cudaStream_t st = ctx->stream;
     SceneSlot& s = *ctx->scenes[idx];
+    const bool was_live = s.present;  // its launch tuning (sr_set_tuning, sr_autotune) is kept
     a.open = false;
     // Until the arrays are written, a failure undoes the snapshot (the scene and its cache are as
     // they were); after, it leaves no scene at the index.
@@ -767,7 +768,7 @@ sr_status sr_arena_finish(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d, SrAre
     s.rindler_crossed = a.stats.rindler_crossed != 0;
     CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, depth, s.num_prims, max_leaf, st),
        "build node layout");
-    s.tuning = fast_default_tuning(ctx->fast);
+    if (!was_live) s.tuning = fast_default_tuning(ctx->fast);
     a.fresh.clear();
     a.tubes.clear();
     a.prims_in.clear();

@@ -203,6 +203,19 @@ def test_a_tube_past_its_rindler_horizon_is_flagged(engine, inputs):
     assert engine.stats(idx).rindler_crossed == 1
 
 
+def test_tuning_survives_snapshots(engine, inputs):
+    """A scene's launch tuning (sr_set_tuning / sr_autotune) stays across snapshots."""
+    sc, tube, simplices, p = inputs
+    w = W.World(tube, simplices)
+    idx = IDX + 50
+    engine_drive(engine, w, 0, sc, idx)
+    t = engine.tuning(idx)
+    t.blocks_per_sm = 7
+    engine.set_tuning(idx, t)
+    engine_drive(engine, w, 1, sc, idx)
+    assert engine.tuning(idx).blocks_per_sm == 7
+
+
 def test_snapshot_timing(engine, inputs):
     """The per-snapshot cost the reference measures (bench.rs:213-218, rebuild + GPU patch): a world
     of 12 bodies with long histories, three new samples per body per snapshot; the whole
