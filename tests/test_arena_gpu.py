@@ -216,6 +216,31 @@ def test_tuning_survives_snapshots(engine, inputs):
     assert engine.tuning(idx).blocks_per_sm == 7
 
 
+def test_batches_follow_the_snapshots(engine, inputs):
+    """Batched renders replay CUDA graphs keyed by the scene's buffers, which snapshots rewrite and
+    regrow: after every snapshot a batch of observers equals their single plain frames."""
+    sc, tube, simplices, p = inputs
+    w = W.World(tube, simplices)
+    idx = IDX + 55
+    us = []
+    for yaw in (0.0, 120.0, 240.0):
+        us.append(sr.uniforms(sr.camera(fov_deg=100.0, yaw=yaw), 160, 100, 0, 1, 0, light_pos=tuple(p.light_pos)))
+    total = sum(u.size[0] * u.size[1] for u in us)
+    hits = 0
+    for k in range(6):
+        engine_drive(engine, w, k, sc, idx)
+        out = np.zeros(total, np.uint32)
+        engine.render_batch(idx, us, out.ctypes.data, total, device_output=False)
+        off = 0
+        for u in us:
+            n = u.size[0] * u.size[1]
+            ref = engine.render(idx, u, path=sr.SR_PATH_PLAIN, aux=True)
+            assert (out[off:off + n] == ref.rgb).all(), k
+            hits += int((ref.hit_id != 0xFFFFFFFF).sum())
+            off += n
+    assert hits > 1000
+
+
 def test_snapshot_timing(engine, inputs):
     """The per-snapshot cost the reference measures (bench.rs:213-218, rebuild + GPU patch): a world
     of 12 bodies with long histories, three new samples per body per snapshot; the whole
