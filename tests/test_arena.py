@@ -149,3 +149,22 @@ def test_dirty_ranges_patch_a_copy_into_the_arena():
         version = (lay, ed)
         assert all(x.tobytes() == y.tobytes() for x, y in zip(copy, (nodes, g, a))), k
     assert patched == 9
+
+
+def test_single_chunk_root_and_nothing():
+    """One chunk: node 0 is a copy of its root (scene_cache.rs:328); nothing: node 0 over nothing."""
+    sc = sr.synth_scene(1, 1, n_bodies=4, steps=8)
+    boxes, geoms, attrs, _ = sc.build_inputs()
+    A = O.Arena()
+    A.begin()
+    A.piece((2, 0, 1), 0, [0], boxes[:25], geoms[:25], attrs[:25])
+    A.finish()
+    nodes, g, a = A.arrays()
+    assert nodes[0].tobytes() == nodes[1].tobytes()  # the chunk's root went to node 1
+    assert W.in_tree(nodes, g, a) == W.record_rows(geoms[:25], attrs[:25])
+    A.begin()
+    A.finish()
+    nodes, g, a = A.arrays()
+    assert nodes[0]["count"] == 0 and nodes[0]["left"] == 0 and nodes[0]["right_or_first"] == 0
+    assert (nodes[0]["min"] > nodes[0]["max"]).all()
+    assert W.in_tree(nodes, g, a) == []

@@ -216,6 +216,34 @@ def test_tuning_survives_snapshots(engine, inputs):
     assert engine.tuning(idx).blocks_per_sm == 7
 
 
+def test_one_chunk_empty_chunks_and_back(engine, inputs):
+    """The tree's edge cases as the reference writes them (scene_cache.rs:325-333): nothing (node 0
+    over nothing), one chunk (node 0 a copy of its root), an empty piece, many chunks, one again."""
+    sc, tube, simplices, p = inputs
+    boxes, geoms, attrs = simplices
+    idx = IDX + 60
+    A = O.Arena()
+    steps = [
+        [],                                   # nothing
+        [(0, [0], slice(0, 25))],             # one chunk
+        [(0, [0], slice(0, 25)), (1, [1], slice(30, 30))],   # plus an empty piece
+        [(0, [0], slice(0, 25)), (1, [1], slice(30, 30)), (2, [2], slice(40, 75)), (3, [3], slice(80, 81))],
+        [(2, [2], slice(40, 75))],            # one again (reused, elsewhere in the arena)
+    ]
+    for k, pieces in enumerate(steps):
+        engine.arena_begin(idx)
+        A.begin()
+        for i, key, sl in pieces:
+            engine.arena_piece(idx, (2, 0, 9), i, key, boxes[sl], geoms[sl], attrs[sl])
+            A.piece((2, 0, 9), i, key, boxes[sl], geoms[sl], attrs[sl])
+        es = engine.arena_finish(idx, sc)
+        os_ = A.finish()
+        assert {key: es[key] for key in os_} == os_, k
+        arrays = assert_same_arena(engine, A, idx)
+        if k in (1, 3, 4):
+            assert_same_frames(engine, arrays, p, yaw=0.0, idx=idx)
+
+
 def test_batches_follow_the_snapshots(engine, inputs):
     """Batched renders replay CUDA graphs keyed by the scene's buffers, which snapshots rewrite and
     regrow: after every snapshot a batch of observers equals their single plain frames."""
