@@ -162,6 +162,11 @@ typedef struct SrTimings {
 #define SR_FLAG_DEVICE_OUTPUT 2u   /* output pointers are device pointers; return without syncing */
 #define SR_FLAG_STAR_BRUTE 4u      /* stars: O(N_stars) per pixel as the reference, no binning */
 #define SR_FLAG_COUNT_WORK 8u      /* count traversal work into SrTimings (slower; blocks) */
+#define SR_FLAG_ASYNC_OUTPUT 16u   /* sr_render_batch with a host framebuffer: return once the batch
+                                      and its readback are queued; the readback runs beside the next
+                                      batch. The framebuffer holds the frames after sr_synchronize
+                                      (or after the call two batches later returns), which also
+                                      reports a device error of the batch. Not with timings. */
 
 /* Optional per-pixel outputs (host or device pointers, as the call's flags say). */
 typedef struct SrOutputs {

@@ -517,10 +517,11 @@ class Engine:
 
     def render_batch(self, idx: int, us: list, rgb_ptr: int, rgb_len: int, cams: list | None = None,
                      device_output: bool = True, timing: bool = False, phases: bool = False,
-                     count: bool = False, star_brute: bool = False) -> _lib.Timings:
+                     count: bool = False, star_brute: bool = False, async_output: bool = False) -> _lib.Timings:
         """Renders observers `us` into `rgb_ptr` (concatenated frames). `timing` returns the batch's
         device time; `phases` adds per-phase times, `count` the traversal work (both run the launch
-        sequence outside its CUDA graph)."""
+        sequence outside its CUDA graph). `async_output` (host framebuffer, pinned for overlap):
+        return once queued; the frames are there after `synchronize()`."""
         n = len(us)
         ua = (GpuUniforms * n)(*us)
         ca = (CameraF64 * n)(*cams) if cams else None
@@ -528,6 +529,7 @@ class Engine:
         flags = SR_FLAG_DEVICE_OUTPUT if device_output else 0
         flags |= (_lib.SR_FLAG_TIMING if phases else 0) | (_lib.SR_FLAG_COUNT_WORK if count else 0)
         flags |= _lib.SR_FLAG_STAR_BRUTE if star_brute else 0
+        flags |= _lib.SR_FLAG_ASYNC_OUTPUT if async_output else 0
         timing = timing or phases or count
         _check(self.L.sr_render_batch(self.h, idx, ua, ca, n, rgb_ptr, rgb_len, flags,
                                       C.byref(t) if timing else None), self.h, "render_batch")

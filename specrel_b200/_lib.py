@@ -31,6 +31,7 @@ SR_FLAG_TIMING = 1
 SR_FLAG_DEVICE_OUTPUT = 2
 SR_FLAG_STAR_BRUTE = 4
 SR_FLAG_COUNT_WORK = 8
+SR_FLAG_ASYNC_OUTPUT = 16
 SR_NOALLOC_SCRATCH_BYTES = 8 << 20
 SR_ADJ_FROZEN = 1
 SR_NOALLOC_MAX_PIXELS = 1 << 18

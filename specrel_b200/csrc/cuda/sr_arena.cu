@@ -464,7 +464,11 @@ sr_status sr_arena_finish(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d, SrAre
     for (const NewTube& t : a.tubes)
         if (t.material >= d->num_materials) return fail(ctx, SR_ERR_BAD_SCENE, "tube material id out of range");
     for (const NewPrims& p : a.prims_in)
-        if (check_build_desc(ctx, d, p.attrs.data(), (uint32_t)p.attrs.size()) != SR_OK) return SR_ERR_BAD_SCENE;
+        for (const SrGpuAttr& at : p.attrs) {  // the installed simplices' material ids
+            uint32_t m;
+            std::memcpy(&m, &at.misc[2], 4);
+            if (m >= d->num_materials) return fail(ctx, SR_ERR_BAD_SCENE, "an installed simplex's material id is out of range");
+        }
     CK(cudaSetDevice(ctx->device), "set device");
     cudaStream_t st = ctx->stream;
     SceneSlot& s = *ctx->scenes[idx];

@@ -123,6 +123,15 @@ void sr_destroy(sr_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     for (auto& ev : ctx->ev) if (ev) cudaEventDestroy(ev);
+    AsyncOutput& ao = ctx->async;
+    if (ao.copy) {
+        cudaStreamSynchronize(ao.copy);
+        cudaStreamDestroy(ao.copy);
+    }
+    for (int b = 0; b < 2; ++b) {
+        if (ao.rendered[b]) cudaEventDestroy(ao.rendered[b]);
+        if (ao.copied[b]) cudaEventDestroy(ao.copied[b]);
+    }
     fast_release(ctx->fast);
     ctx->scenes.clear();
     if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -144,10 +153,38 @@ sr_status sr_set_stream(sr_ctx* ctx, void* s) {
     return SR_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// The device error flags a batch left in its counters (counters[1]), as a status.
+sr_status batch_errors(sr_ctx* ctx, uint32_t flags) {
+    if (flags & ERR_TRAVERSAL_LIMIT) return fail(ctx, SR_ERR_TRAVERSAL_LIMIT, "a ray exceeded the traversal visit limit");
+    if (flags & ERR_SHADOW_MISMATCH) return fail(ctx, SR_ERR_CUDA, "internal error: shadow state mismatch");
+    if (flags) return fail(ctx, SR_ERR_BAD_SCENE, "device reported a bad index");
+    return SR_OK;
+}
+
+// Waits for the asynchronous batch that used framebuffer b (if any) and reports its errors.
+sr_status settle_async(sr_ctx* ctx, int b) {
+    AsyncOutput& ao = ctx->async;
+    if (!ao.pending[b]) return SR_OK;
+    CK(cudaEventSynchronize(ao.copied[b]), "async readback");
+    ao.pending[b] = false;
+    return batch_errors(ctx, ao.flags.as<uint32_t>()[16 * b + 1]);
+}
+}  // namespace
+
+extern "C" {
+
 sr_status sr_synchronize(sr_ctx* ctx) {
     if (!ctx) return SR_ERR_INVALID_ARGUMENT;
     CK(cudaStreamSynchronize(ctx->stream), "synchronize");
-    return SR_OK;
+    sr_status first = SR_OK;
+    for (int k = 0; k < 2; ++k) {  // oldest first
+        const sr_status r = settle_async(ctx, (ctx->async.next + k) & 1);
+        if (first == SR_OK) first = r;
+    }
+    return first;
 }
 
 sr_status sr_upload_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d) {
@@ -607,9 +644,47 @@ sr_status sr_render_batch(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, con
     if (total > (1ull << 30)) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "batch larger than 2^30 pixels");
     SceneSlot& s = *ctx->scenes[idx];
     const bool dev_out = (flags & SR_FLAG_DEVICE_OUTPUT) != 0;
+    const bool async_out = (flags & SR_FLAG_ASYNC_OUTPUT) != 0;
+    if (async_out && (dev_out || timings))
+        return fail(ctx, SR_ERR_INVALID_ARGUMENT, "SR_FLAG_ASYNC_OUTPUT takes a host framebuffer and no timings");
     CK(cudaSetDevice(ctx->device), "set device");
     cudaStream_t sm = ctx->stream;
     cudaEvent_t* ev = ctx->ev;
+    if (async_out && s.fast.usable) {
+        // The batch renders into framebuffer b once the readback of the batch before that used it
+        // has finished; its readback then runs on the copy stream while the next batch renders.
+        AsyncOutput& ao = ctx->async;
+        if (!ao.copy) {
+            CK(cudaStreamCreateWithFlags(&ao.copy, cudaStreamNonBlocking), "copy stream");
+            for (int b = 0; b < 2; ++b) {
+                CK(cudaEventCreateWithFlags(&ao.rendered[b], cudaEventDisableTiming), "event");
+                CK(cudaEventCreateWithFlags(&ao.copied[b], cudaEventDisableTiming), "event");
+            }
+            CK(ao.flags.ensure(2 * 16 * sizeof(uint32_t)), "pinned flags");
+        }
+        const int b = ao.next;
+        sr_status r = settle_async(ctx, b);
+        if (r != SR_OK) return r;
+        CK(ao.rgb[b].ensure(total * 4), "framebuffer");
+        BatchRequest br{};
+        br.n = n;
+        br.u = u;
+        br.cam64 = cam64;
+        br.rgb = ao.rgb[b].as<uint32_t>();
+        br.use_graph = true;
+        br.star_brute = (flags & SR_FLAG_STAR_BRUTE) != 0;
+        SceneDev sd = scene_dev(ctx, s);
+        CK(fast_render_batch(ctx->fast, s.fast, s.tuning, sd, s.anchor, ctx->bb, ctx->counters.as<uint32_t>(), br, sm),
+           "batch render");
+        CK(cudaMemcpyAsync(ao.flags.as<uint32_t>() + 16 * b, ctx->counters.p, 64, cudaMemcpyDeviceToHost, sm), "flags");
+        CK(cudaEventRecord(ao.rendered[b], sm), "event");
+        CK(cudaStreamWaitEvent(ao.copy, ao.rendered[b], 0), "event");
+        CK(cudaMemcpyAsync(rgb_out, ao.rgb[b].p, total * 4, cudaMemcpyDeviceToHost, ao.copy), "batch readback");
+        CK(cudaEventRecord(ao.copied[b], ao.copy), "event");
+        ao.pending[b] = true;
+        ao.next = 1 - b;
+        return SR_OK;
+    }
     if (!s.fast.usable) {  // trees the fast path cannot take render one by one on the plain path
         DevBuf staging;
         uint32_t* dst = rgb_out;
@@ -673,9 +748,7 @@ sr_status sr_render_batch(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, con
                 timings->shadow_tets_tested = w[5];
             }
         }
-        if (counters[1] & ERR_TRAVERSAL_LIMIT) return fail(ctx, SR_ERR_TRAVERSAL_LIMIT, "a ray exceeded the traversal visit limit");
-        if (counters[1] & ERR_SHADOW_MISMATCH) return fail(ctx, SR_ERR_CUDA, "internal error: shadow state mismatch");
-        if (counters[1]) return fail(ctx, SR_ERR_BAD_SCENE, "device reported a bad index");
+        return batch_errors(ctx, counters[1]);
     }
     return SR_OK;
 }
@@ -691,8 +764,6 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
     SrRenderOpts opts{SR_PATH_FAST, SR_FLAG_DEVICE_OUTPUT, nullptr};
     SrTuning keep = s.tuning, win = s.tuning;
     float win_ms = INFINITY;
-    // The schedules worth timing: whole-warp refills of single tiles were fastest on every scene
-    // measured (wider chunks or partial refills spread the rays in flight over more of the tree).
     // The schedules worth timing: whole-warp refills of single tiles were fastest on every scene
     // measured (wider chunks or partial refills spread the rays in flight over more of the tree).
     const uint32_t shapes[][2] = {{128, 8}, {128, 11}, {256, 4}, {256, 6}, {512, 3}};

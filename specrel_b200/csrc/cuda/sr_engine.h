@@ -54,6 +54,17 @@ struct Frame {
     DevBuf hdr, rgb, hit, lam, tau;
 };
 
+// Batches with SR_FLAG_ASYNC_OUTPUT: two device framebuffers used in turn, the readbacks on a copy
+// stream ordered by events, each batch's error flags in pinned memory until they are checked.
+struct AsyncOutput {
+    cudaStream_t copy = nullptr;
+    cudaEvent_t rendered[2] = {}, copied[2] = {};
+    DevBuf rgb[2];
+    HostMem flags;  // 2 x 16 words: the batch's counters
+    bool pending[2] = {false, false};
+    int next = 0;
+};
+
 }  // namespace sre
 
 struct sr_ctx {
@@ -67,6 +78,7 @@ struct sr_ctx {
     sre::Frame frame;
     cudaEvent_t ev[8] = {};
     srk::FastCtx fast;
+    sre::AsyncOutput async;
 };
 
 namespace sre {

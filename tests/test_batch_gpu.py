@@ -158,3 +158,21 @@ def test_render_update_render_uses_the_new_scene(engine):
     fresh = engine.render(7, u).rgb
     assert (after == fresh).all()
     assert not (before == after).all()
+
+
+def test_async_output_overlaps_and_equals_the_blocking_batch(engine, scene):
+    """SR_FLAG_ASYNC_OUTPUT: batches queued back to back into different pinned framebuffers, each
+    readback beside the next batch, equal the blocking batch once synchronized."""
+    import torch
+    obs, us, cams = _observers(31, 4, int(scene.info.n_nodes), scale=4)
+    total = sum(u.size[0] * u.size[1] for u in us)
+    ref = _batch(engine, 3, us, cams)
+    outs = [torch.zeros(total, dtype=torch.int32, pin_memory=True) for _ in range(3)]
+    for o in outs:
+        engine.render_batch(3, us, o.data_ptr(), total, cams=cams, device_output=False, async_output=True)
+    engine.synchronize()
+    for o in outs:
+        assert (o.numpy().view(np.uint32) == ref).all()
+    with pytest.raises(sr.SrError):
+        engine.render_batch(3, us, outs[0].data_ptr(), total, cams=cams, device_output=False, async_output=True,
+                            timing=True)
