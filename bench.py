@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Headline benchmark: primary rays per second on the 7.9M-tetrahedron 1280x800 scene.
 
-Workload (BASELINE configs[1]): 64 accelerated icospheres (subdivision 2) on Fermi-Walker
+Workload: 64 accelerated icospheres (subdivision 2) on Fermi-Walker
 worldlines, 128 time steps, ~7.9M tetrahedra; observers at t = 0 at the origin with rapidities
 |phi| <= 2; 1280x800; past light cone; Lorentz-invariant null shadows from a point light at
 (0, 50, 0); FP32 traversal. Synthetic, seeded (the reference ships no scenes for these configs).
@@ -180,8 +180,8 @@ def run_reference(args, rank, world):
     v = W * rows / t / 1e6
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded configs[1] scene)", "impl": "reference",
-            "config": {"workload": "configs[1]: 64 accelerated icospheres, 7.9M tets, 1280x800, null shadows",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded accelerated-icosphere scene)", "impl": "reference",
+            "config": {"workload": "64 accelerated icospheres, 7.9M tets, 1280x800, null shadows",
                        "sample": f"every {stride}th row ({W}x{rows} rays) per step"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"every {stride}th row of the 1280x800 frame, all host threads; the Rust "
@@ -341,8 +341,8 @@ def run_engine(args, rank, world, local):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded configs[1] scene: no dataset; the reference ships no such scene)",
-        "config": {"workload": "configs[1]: 64 accelerated icospheres (subdiv 2), 128 steps, "
+        "data": "synthetic (seeded accelerated-icosphere scene: no dataset; the reference ships no such scene)",
+        "config": {"workload": "64 accelerated icospheres (subdiv 2), 128 steps, "
                                f"{scene.num_prims} tets, 1280x800, past light cone, Lorentz-invariant null shadows, "
                                "light (0,50,0), FP32 traversal + FP64 camera",
                    "observers_per_step_per_gpu": B, "rays_per_step": total_rays, "seed": args.seed,
@@ -379,7 +379,7 @@ def run_engine(args, rank, world, local):
 
 
 def run_config4(args, rank, world, local):
-    """the config-1 scene (64 inertial unit cubes, 147k tets) seen by 64 observers in one
+    """The cube scene (64 inertial unit cubes, 147k tets) seen by 64 observers in one
     batch: resolutions drawn from {320x200, 640x400, 1280x800, 1920x1200}, events t in [-50, 0]
     with |x| <= 30, rapidities |phi| <= 3, half past light cone and half God's-eye slice (the
     shared observer draw of the scene builder). One step = the whole batch through the batched fast
@@ -463,11 +463,11 @@ def run_config4(args, rank, world, local):
         key = f"{o['width']}x{o['height']}"
         sizes[key] = sizes.get(key, 0) + 1
     line = {
-        "metric": "Mrays/s on 1 B200, configs[3]: 64 observers of the 147k-tet cube scene in one batch; primary rays",
+        "metric": "Mrays/s on 1 B200, 64 observers of the 147k-tet cube scene in one batch; primary rays",
         "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded configs[3] observers over the configs[0] scene)",
-        "config": {"workload": f"configs[3]: {scene.num_prims} tets, 64 observers (sizes {sizes}), past light cone "
+        "data": "synthetic (seeded observers over the cube scene)",
+        "config": {"workload": f"{scene.num_prims} tets, 64 observers (sizes {sizes}), past light cone "
                                "and God's-eye slice 50/50, FP64 cameras",
                    "rays_per_step": total, "seed": args.seed,
                    "l2": "scene L2-resident (%.1f MB on the device); every step renders 64 frames" %
@@ -484,7 +484,7 @@ def run_config4(args, rank, world, local):
 
 
 def run_config5(args, rank, world, local):
-    """configs[4]: 100k inertial stars on a sphere of radius 1e3 over the cube scene, 1280x800, target
+    """100k inertial stars on a sphere of radius 1e3 over the cube scene, 1280x800, target
     rendered at rapidity (0.8, -0.3, 0.5). Times, with CUDA events on the engine's stream: one forward
     frame on the fast path (FP64 camera, binned stars) and one loss-and-gradient evaluation
     (sr_adjoint: the forward frame recomputed, then the 7-vector of rapidity and event derivatives in
@@ -528,11 +528,11 @@ def run_config5(args, rank, world, local):
         r = eng.adjoint(0, u, cam0, tdev.data_ptr(), 0)
     clk = clocks.summary()
     line = {
-        "metric": "ms per image-loss gradient on 1 B200, configs[4]: 100k stars over the cube scene, 1280x800",
+        "metric": "ms per image-loss gradient on 1 B200, 100k stars over the cube scene, 1280x800",
         "value": g0, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": g0,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 sums)",
-        "data": "synthetic (seeded configs[4] stars and occluders)",
-        "config": {"workload": f"configs[4]: {scene.num_prims} tets, {scene.num_stars} stars, 1280x800, target at "
+        "data": "synthetic (seeded stars and occluders)",
+        "config": {"workload": f"{scene.num_prims} tets, {scene.num_stars} stars, 1280x800, target at "
                                "rapidity (0.8, -0.3, 0.5), gradient at rapidity 0", "seed": args.seed},
         "forward_frame_ms": fwd, "gradient_level3_ms": g3,
         "gradient": {"loss": r.loss, "grad": list(r.grad), "star_terms": r.star_terms},

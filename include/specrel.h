@@ -399,6 +399,15 @@ typedef struct SrAdjointResult {
                              a smooth function of theta for checking the gradient by differences */
 sr_status sr_adjoint(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, const SrCameraF64* cam,
                      const float* target_hdr, uint32_t level, uint32_t flags, SrAdjointResult* out);
+/* sr_adjoint over rows [row_begin, row_end) of the loss level (`level` halvings of the frame's
+ * height) and the frame's pixel rows under them: the loss terms of those rows and the gradient
+ * they contribute, plus their primal mismatches and star terms. The results over a partition of the
+ * rows sum to sr_adjoint's (up to the order of FP64 sums): each GPU of a group takes a band and one
+ * all-reduce of the ten doubles gives the whole (the forward frame is rendered whole on each). A
+ * frozen evaluation takes the rows of the gradient call before it. */
+sr_status sr_adjoint_rows(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, const SrCameraF64* cam,
+                          const float* target_hdr, uint32_t level, uint32_t flags, uint32_t row_begin,
+                          uint32_t row_end, SrAdjointResult* out);
 
 /* ---- Rendering without device allocation -------------------------------------------------
  * No counterpart in the reference: an entry point for callers that cannot call cudaMalloc while

@@ -136,7 +136,7 @@ assert MAT_DTYPE.itemsize == 48
 
 def synth_params(config: int, seed: int, n_bodies: int | None = None, steps: int | None = None,
                  subdiv: int = 2, n_stars: int | None = None, translate=(0.0, 0.0, 0.0, 0.0)) -> SynthParams:
-    """Default parameters of the five synthetic workloads (see DESIGN.md for the protocol)."""
+    """Default parameters of the five synthetic workloads."""
     p = SynthParams()
     p.config = config
     p.seed = seed

@@ -536,14 +536,19 @@ class Engine:
         return t
 
     def adjoint(self, idx: int, u: GpuUniforms, cam: CameraF64, target_hdr_ptr: int, level: int = 0,
-                frozen: bool = False) -> _lib.AdjointResult:
+                frozen: bool = False, rows: tuple[int, int] | None = None) -> _lib.AdjointResult:
         """Loss sum((P(HDR) - P(target))^2) of the observer `cam` (P: `level` 2x2 box halvings) and
         its gradient with respect to (rapidity x, y, z, event t, x, y, z); `target_hdr_ptr`: device,
-        width*height*4 floats. `frozen`: the loss only, under the previous call's discrete outcomes."""
+        width*height*4 floats. `frozen`: the loss only, under the previous call's discrete outcomes.
+        `rows`: only rows [begin, end) of the loss level (sr_adjoint_rows)."""
         r = _lib.AdjointResult()
         flags = _lib.SR_ADJ_FROZEN if frozen else 0
-        _check(self.L.sr_adjoint(self.h, idx, C.byref(u), C.byref(cam), target_hdr_ptr, level, flags, C.byref(r)),
-               self.h, "adjoint")
+        if rows is None:
+            st = self.L.sr_adjoint(self.h, idx, C.byref(u), C.byref(cam), target_hdr_ptr, level, flags, C.byref(r))
+        else:
+            st = self.L.sr_adjoint_rows(self.h, idx, C.byref(u), C.byref(cam), target_hdr_ptr, level, flags, rows[0],
+                                        rows[1], C.byref(r))
+        _check(st, self.h, "adjoint")
         return r
 
     def tuning(self, idx: int) -> _lib.Tuning:

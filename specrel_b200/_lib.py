@@ -213,6 +213,8 @@ SIGNATURES = {
                                     C.c_uint32, C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(Timings)]),
     "sr_adjoint": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64), C.c_void_p,
                                C.c_uint32, C.c_uint32, C.POINTER(AdjointResult)]),
+    "sr_adjoint_rows": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64), C.c_void_p,
+                                    C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(AdjointResult)]),
     "sr_render_noalloc": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64), C.c_void_p]),
     "sr_get_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),
     "sr_set_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),

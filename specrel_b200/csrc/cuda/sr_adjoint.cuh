@@ -100,6 +100,8 @@ struct AdjointArgs {
     uint32_t* pass;           // 8 words (256 bits) per list entry
     uint32_t frozen;          // 0: gradient, recording the outcomes; 1: values under the recorded outcomes
     float4* hdr_out;          // frozen: the HDR values (W*H)
+    uint32_t y0, y1;          // the pixel rows of this call (a band of the frame, or all of it)
+    uint32_t tile0;           // the first 16x16 tile of the launch (blocks take tile0, tile0 + 1, ...)
 };
 constexpr int ADJ_SLOTS = 10;
 
@@ -162,13 +164,13 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels(AdjointArgs a) {
     extern __shared__ uint32_t keys[];
     __shared__ double red[ADJ_SLOTS][8];
     __shared__ int bad;
-    const uint32_t tile = blockIdx.x;
+    const uint32_t tile = a.tile0 + blockIdx.x;
     const ObsDev& od = a.obs[0];
     const SrGpuUniforms& U = a.U[0];
     const uint32_t tx16 = (od.width + STAR_TILE - 1) / STAR_TILE;
     const uint32_t px = (tile % tx16) * STAR_TILE + threadIdx.x % STAR_TILE;
     const uint32_t py = (tile / tx16) * STAR_TILE + threadIdx.x / STAR_TILE;
-    const bool inside = px < od.width && py < od.height;
+    const bool inside = px < od.width && py < od.height && py >= a.y0 && py < a.y1;
     uint32_t cnt = 0;
     bool brute = false;
     if (a.stars_on) {
@@ -371,17 +373,21 @@ __global__ void k_adj_up(const double* gd, uint32_t dw, uint32_t dh, double* gs,
 }
 
 // Residual of the chosen level: the loss's per-block partial sums and its weights 2 (P - T).
-__global__ void __launch_bounds__(256) k_adj_residual(const float4* p, const float4* t, uint32_t n, double* weight,
-                                                      double* partials) {
+// The residual of the loss level's pixels in rows [r0, r1) (width w): the loss terms and their
+// weights; pixels outside the band weigh nothing.
+__global__ void __launch_bounds__(256) k_adj_residual(const float4* p, const float4* t, uint32_t n, uint32_t w,
+                                                      uint32_t r0, uint32_t r1, double* weight, double* partials) {
     __shared__ double red[8];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double acc = 0.0;
     if (i < n) {
+        const uint32_t row = i / w;
+        const bool in_band = row >= r0 && row < r1;
         const float4 a = p[i], b = t[i];
         const double r[3] = {(double)a.x - (double)b.x, (double)a.y - (double)b.y, (double)a.z - (double)b.z};
         for (int c = 0; c < 3; ++c) {
-            acc += r[c] * r[c];
-            weight[3ull * i + c] = 2.0 * r[c];
+            if (in_band) acc += r[c] * r[c];
+            weight[3ull * i + c] = in_band ? 2.0 * r[c] : 0.0;
         }
     }
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, off);

@@ -808,8 +808,21 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
 
 sr_status sr_adjoint(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const SrCameraF64* cam, const float* target_hdr,
                      uint32_t level, uint32_t flags, SrAdjointResult* out) {
+    if (!ctx || !u) return SR_ERR_INVALID_ARGUMENT;
+    uint32_t rows = u->size[1];
+    for (uint32_t k = 0; k < level && k < SR_BLOOM_LEVELS; ++k) rows = (rows + 1) / 2;
+    return sr_adjoint_rows(ctx, idx, u, cam, target_hdr, level, flags, 0, rows, out);
+}
+
+sr_status sr_adjoint_rows(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const SrCameraF64* cam,
+                          const float* target_hdr, uint32_t level, uint32_t flags, uint32_t row_begin, uint32_t row_end,
+                          SrAdjointResult* out) {
     if (!ctx || !u || !cam || !target_hdr || !out) return SR_ERR_INVALID_ARGUMENT;
     if (level > SR_BLOOM_LEVELS) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "loss level must be 0..6");
+    uint32_t level_rows = u->size[1];
+    for (uint32_t k = 0; k < level; ++k) level_rows = (level_rows + 1) / 2;
+    if (row_begin >= row_end || row_end > level_rows)
+        return fail(ctx, SR_ERR_INVALID_ARGUMENT, "rows must be a non-empty range of the loss level's rows");
     if (idx >= ctx->scenes.size() || !ctx->scenes[idx] || !ctx->scenes[idx]->present)
         return fail(ctx, SR_ERR_NO_SCENE, "scene " + std::to_string(idx) + " is not uploaded");
     if (u->size[0] == 0 || u->size[1] == 0 || (uint64_t)u->size[0] * u->size[1] > (1ull << 28))
@@ -823,11 +836,13 @@ sr_status sr_adjoint(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const Sr
     CK(cudaSetDevice(ctx->device), "set device");
     const bool frozen = (flags & SR_ADJ_FROZEN) != 0;
     if (frozen && (!ctx->fast.adj_valid || ctx->fast.adj_w != u->size[0] || ctx->fast.adj_h != u->size[1] ||
-                   ctx->fast.adj_geoms != scene_dev(ctx, s).geoms))
-        return fail(ctx, SR_ERR_INVALID_ARGUMENT, "a frozen evaluation needs a gradient call on this scene and frame size just before");
+                   ctx->fast.adj_geoms != scene_dev(ctx, s).geoms || ctx->fast.adj_level != level ||
+                   ctx->fast.adj_r0 != row_begin || ctx->fast.adj_r1 != row_end))
+        return fail(ctx, SR_ERR_INVALID_ARGUMENT,
+                    "a frozen evaluation needs a gradient call on this scene, frame size, level and rows just before");
     double r[10];
     CK(fast_adjoint(ctx->fast, s.fast, s.tuning, scene_dev(ctx, s), s.anchor, ctx->bb, ctx->counters.as<uint32_t>(), *u, *cam,
-                    target_hdr, level, frozen, r, ctx->stream),
+                    target_hdr, level, frozen, row_begin, row_end, r, ctx->stream),
        "gradient");
     uint32_t counters[4] = {0, 0, 0, 0};
     CK(cudaMemcpy(counters, ctx->counters.p, 16, cudaMemcpyDeviceToHost), "counters");

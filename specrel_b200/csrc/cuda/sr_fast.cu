@@ -1075,11 +1075,14 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
 // ---------------------------------------------------------------------------------------------
 cudaError_t fast_adjoint(FastCtx& c, const FastScene& s, const SrTuning& t, const SceneDev& sd, const double anchor[4],
                          const BBConst& bb, uint32_t* counters, const SrGpuUniforms& u, const SrCameraF64& cam,
-                         const float* target, uint32_t level, bool frozen, double out[10], cudaStream_t st) {
+                         const float* target, uint32_t level, bool frozen, uint32_t row0, uint32_t row1,
+                         double out[10], cudaStream_t st) {
     const uint32_t W = u.size[0], H = u.size[1];
     cudaError_t e;
     if (frozen) {
-        if (!c.adj_valid || c.adj_w != W || c.adj_h != H || c.adj_geoms != sd.geoms) return cudaErrorInvalidValue;
+        if (!c.adj_valid || c.adj_w != W || c.adj_h != H || c.adj_geoms != sd.geoms || c.adj_level != level ||
+            c.adj_r0 != row0 || c.adj_r1 != row1)
+            return cudaErrorInvalidValue;
     } else {
         // The forward frame: hits, shadow results, star lists and the HDR image the loss compares.
         BatchRequest br{};
@@ -1135,8 +1138,8 @@ cudaError_t fast_adjoint(FastCtx& c, const FastScene& s, const SrTuning& t, cons
         const size_t nl = (size_t)lw[level] * lh[level];
         double* gl = (level % 2 == 0) ? g0 : g1;  // ends in g0 after `level` transposes
         const uint32_t lblocks = (uint32_t)((nl + 255) / 256);
-        k_adj_residual<<<lblocks, 256, 0, st>>>(pyr + loff[level], tpyr + loff[level], (uint32_t)nl, gl,
-                                                 c.adj_partials.as<double>());
+        k_adj_residual<<<lblocks, 256, 0, st>>>(pyr + loff[level], tpyr + loff[level], (uint32_t)nl, lw[level], row0,
+                                                 row1, gl, c.adj_partials.as<double>());
         k_adjoint_reduce<<<1, 256, 0, st>>>(c.adj_partials.as<double>(), lblocks, c.adj_out.as<double>() + ADJ_SLOTS);
         for (uint32_t k = level; k >= 1; --k) {
             double* src = (k % 2 == 0) ? g0 : g1;
@@ -1179,8 +1182,15 @@ cudaError_t fast_adjoint(FastCtx& c, const FastScene& s, const SrTuning& t, cons
     a.pass = stars_on ? c.adj_pass.as<uint32_t>() : nullptr;
     a.frozen = frozen ? 1u : 0u;
     a.hdr_out = c.adj_hdr.as<float4>();
-    k_adjoint_pixels<<<tiles, 256, STAR_SORT_CAP * 4, st>>>(a);
-    k_adjoint_reduce<<<1, 256, 0, st>>>(a.partials, tiles, c.adj_out.as<double>());
+    // The band's pixel rows (level-`level` rows [row0, row1) cover rows row0 * 2^level on) and the
+    // 16x16 tiles over them.
+    a.y0 = std::min(H, row0 << level);
+    a.y1 = std::min(H, row1 << level);
+    const uint32_t ty0 = a.y0 / STAR_TILE, ty1 = (a.y1 + STAR_TILE - 1) / STAR_TILE;
+    a.tile0 = ty0 * tx16;
+    const uint32_t band_tiles = (ty1 - ty0) * tx16;
+    if (band_tiles) k_adjoint_pixels<<<band_tiles, 256, STAR_SORT_CAP * 4, st>>>(a);
+    k_adjoint_reduce<<<1, 256, 0, st>>>(a.partials, band_tiles, c.adj_out.as<double>());
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (frozen && (e = loss_pass(c.adj_hdr.p)) != cudaSuccess) return e;
     double both[2 * ADJ_SLOTS];
@@ -1193,6 +1203,9 @@ cudaError_t fast_adjoint(FastCtx& c, const FastScene& s, const SrTuning& t, cons
         c.adj_w = W;
         c.adj_h = H;
         c.adj_geoms = sd.geoms;
+        c.adj_level = level;
+        c.adj_r0 = row0;
+        c.adj_r1 = row1;
     }
     return cudaSuccess;
 }

@@ -95,7 +95,7 @@ struct FastCtx {
     // The outcomes of the last gradient call (hits, shadows, star lists, grid lines, cut passes)
     // stay valid for frozen evaluations while no other frame is rendered.
     bool adj_valid = false;
-    uint32_t adj_w = 0, adj_h = 0;
+    uint32_t adj_w = 0, adj_h = 0, adj_level = 0, adj_r0 = 0, adj_r1 = 0;  // the last gradient call's frame and band
     const float4* adj_geoms = nullptr;
     HostMem hU, hcam64, hobs, hlvl;
     uint32_t cap_obs = 0;
@@ -133,10 +133,13 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
 // observer (see sr_adjoint.cuh). `target`: device, W*H*4 floats. out: loss, grad[7], primal
 // mismatches (pixels whose dual value differs from the forward frame, or whose star list was not
 // sortable), star terms. `frozen`: only the loss at `cam` under the last gradient call's discrete
-// outcomes (no forward frame; the finite-difference check of the gradient).
+// outcomes (no forward frame; the finite-difference check of the gradient). Only rows
+// [row0, row1) of the loss level count (and the frame's pixel rows under them): the results of a
+// partition of the rows sum to the whole frame's.
 cudaError_t fast_adjoint(FastCtx& c, const FastScene& s, const SrTuning& t, const SceneDev& sd, const double anchor[4],
                          const BBConst& bb, uint32_t* counters, const SrGpuUniforms& u, const SrCameraF64& cam,
-                         const float* target, uint32_t level, bool frozen, double out[10], cudaStream_t st);
+                         const float* target, uint32_t level, bool frozen, uint32_t row0, uint32_t row1,
+                         double out[10], cudaStream_t st);
 // The device HDR image (level 0) of observer `i` of the last batch, for side outputs.
 float4* fast_batch_hdr(FastCtx& c, uint32_t pix_base_of_obs);
 

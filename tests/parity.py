@@ -1,6 +1,6 @@
 """Parity metrics between an engine frame and the CPU oracle (test helper).
 
-The bar (BASELINE north star): bit-exact hit-tetrahedron ids on non-grazing rays, lambda and tau
+The bar: bit-exact hit-tetrahedron ids on non-grazing rays, lambda and tau
 within 1e-5 relative, RGB8 within 1/255. Colours may differ only through the last bits of the
 transcendentals (CUDA's sinf/cosf/expf/atan2f/acosf against glibc's); a pixel whose oracle
 colour changes by more than 1/255 when every transcendental result moves by +-PERTURB ulps is

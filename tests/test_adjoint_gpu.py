@@ -1,4 +1,4 @@
-"""The gradient of the image loss with respect to the observer (sr_adjoint), configs[4]'s setting:
+"""The gradient of the image loss with respect to the observer (sr_adjoint), in the star scene's setting:
 stars over cube occluders, past light cone, null shadows, loss on the linear pre-bloom HDR image.
 
 Checked against the FP64 CPU reference: the oracle's frozen-outcome loss (oracle/oracle_grad.hpp),
@@ -84,8 +84,35 @@ def test_frozen_needs_a_gradient_call_first(engine, setup):
         engine.adjoint(11, setup["u"], sr.cam64((0.0,) * 4, STAR), setup["tdev"].data_ptr(), frozen=True)
 
 
+@pytest.mark.parametrize("level", [0, 2])
+def test_row_bands_sum_to_the_whole(engine, setup, level):
+    """sr_adjoint_rows: the loss, gradient, primal mismatches and star terms of a partition of the
+    loss level's rows (as ranks shard them) sum to the whole frame's; the frozen loss of each band
+    follows its own gradient call."""
+    from specrel_b200 import shard
+    th = np.array((0.75, -0.25, 0.45, 0.0, 0.1, -0.05, 0.08))
+    u, tp = setup["u"], setup["tdev"].data_ptr()
+    whole = engine.adjoint(11, u, _cam64(th), tp, level)
+    rows = shard.loss_rows(H, level)
+    total = np.zeros(10)
+    frozen = 0.0
+    for rank in range(3):
+        r0, r1 = shard.row_band(rows, rank, 3)
+        r = engine.adjoint(11, u, _cam64(th), tp, level, rows=(r0, r1))
+        total += [r.loss, *[r.grad[k] for k in range(7)], r.primal_mismatch, r.star_terms]
+        frozen += engine.adjoint(11, u, _cam64(th), tp, level, frozen=True, rows=(r0, r1)).loss
+    ref = np.array([whole.loss, *[whole.grad[k] for k in range(7)], whole.primal_mismatch, whole.star_terms])
+    assert total[8] == ref[8] == 0 and total[9] == ref[9] > 0
+    scale = np.abs(ref[1:8]).max()
+    assert abs(total[0] - ref[0]) <= 1e-12 * ref[0]
+    assert np.abs(total[1:8] - ref[1:8]).max() <= 1e-12 * scale
+    assert abs(frozen - ref[0]) <= 1e-12 * ref[0]
+    with pytest.raises(sr.SrError):  # a frozen call takes the rows of the gradient call before it
+        engine.adjoint(11, u, _cam64(th), tp, level, frozen=True, rows=(0, 1))
+
+
 def test_gradient_descent_recovers_the_rapidity(engine):
-    """configs[4] at 320x200: 100k stars over the cubes; from rapidity 0, normalized gradient descent
+    """The 100k-star scene at 320x200: 100k stars over the cubes; from rapidity 0, normalized gradient descent
     with backtracking on loss levels 6, 5, ..., 0 reaches the target rapidity."""
     import torch
     s = O.Scene(O.synth_params(5, 1, n_bodies=64, steps=64))

@@ -1,11 +1,11 @@
-"""configs[1] at full size: the 7.9M-tet accelerated-icosphere scene at 1280x800, the workload's own
+"""At full size: the 7.9M-tet accelerated-icosphere scene at 1280x800, the workload's own
 observer (the bench's first frame), on the fast (batched) path.
 
 - With the reference's f32 camera, against the f32 oracle on the same packed scene: hit ids,
   lambda and tau bit-identical, RGB8 within 1/255 outside the near-threshold mask (the parity bar,
   at full size).
 - With the FP64 camera (the batched FP32 + FP64-rebase configuration the bench measures), against
-  the all-FP64 oracle (scene built and rendered in double): the north star's hit-id agreement
+  the all-FP64 oracle (scene built and rendered in double): the hit-id agreement bar
   (>= 99.99%) and colour within 1/255 on agreeing pixels outside the near-threshold mask, with the
   lambda and tau errors reported. The f32-camera frame is measured against the FP64 oracle too.
 The printed lines are the measurement quoted for this configuration.

@@ -76,7 +76,7 @@ def test_device_extrusion_and_build_equal_host_build(engine, case):
 
 
 def test_device_build_full_size(engine):
-    """configs[1] at full size: 7.9M simplices, from build-order simplices and from worldtubes."""
+    """The icosphere scene at full size: 7.9M simplices, from build-order simplices and from worldtubes."""
     scene = sr.synth_scene(2, 1, threads=os.cpu_count())
     t_gpu = _build_and_compare(engine, 21, scene)
     t_tubes = _tubes_and_compare(engine, 23, scene)
@@ -86,7 +86,7 @@ def test_device_build_full_size(engine):
 
 
 def test_device_extrusion_flags_tubes_past_their_rindler_horizon(engine):
-    """The sampled accelerations of configs[1]'s bodies carry the reference's f32 finite-difference
+    """The sampled accelerations of the icosphere scene's bodies carry the reference's f32 finite-difference
     noise, which crosses 1 + a_local . p > 0 for vertices of some larger bodies (the host builder
     records it as rindler_ok = 0): the device build extrudes them all the same and flags it."""
     for case in (dict(config=2, seed=4, n_bodies=24, steps=24), dict(config=1, seed=1)):

@@ -46,7 +46,7 @@ def _render_both(engine, idx, scene, cam_o, cam_e, w, h, mode=0, shadow=0, slice
 
 @pytest.mark.parametrize("path", PATHS)
 def test_config1_320x200_matches_oracle(engine, cubes, path):
-    """64 inertial cubes, camera at rest at the origin, 90 degrees, past cone, no shadows."""
+    """The cube scene: 64 inertial cubes, camera at rest at the origin, 90 degrees, past cone, no shadows."""
     rep, fr, base = _render_both(engine, 0, cubes, O.make_camera(), sr.camera(), 320, 200, path=path)
     _assert_parity(rep, f"config1 path={path}")
     assert (fr.hit_id != 0xFFFFFFFF).sum() > 100
@@ -90,7 +90,7 @@ def test_flashes_haze_and_frontier(engine, cubes):
 
 @pytest.mark.parametrize("path", PATHS)
 def test_config2_reduced_accelerated_bodies_with_null_shadows(engine, path):
-    """configs[1]'s scene type at reduced size: accelerated icospheres, boosted observer, null shadows."""
+    """The icosphere scene type at reduced size: accelerated icospheres, boosted observer, null shadows."""
     s = O.Scene(O.synth_params(2, 4, n_bodies=24, steps=24))
     engine.upload(1, packed_from_oracle(s))
     rap = tuple(s.info.cam_rapidity)
@@ -102,7 +102,7 @@ def test_config2_reduced_accelerated_bodies_with_null_shadows(engine, path):
 
 
 def test_stars_reduced(engine):
-    """Point stars with Doppler colour over the cube occluders (configs[4]'s scene at reduced size)."""
+    """Point stars with Doppler colour over the cube occluders (the star scene at reduced size)."""
     s = O.Scene(O.synth_params(5, 2, n_bodies=8, steps=16, n_stars=3000))
     engine.upload(2, packed_from_oracle(s))
     rap = tuple(s.info.cam_rapidity)

@@ -1,4 +1,4 @@
-"""the cube scene translated to t = 1e6, |x| = 1e5, observer at the same offset, at 1280x800.
+"""The cube scene translated to t = 1e6, |x| = 1e5, observer at the same offset, at 1280x800.
 
 The engine stores the scene's f32 coordinates relative to an FP64 anchor and builds the observer's
 event and tetrad in double on the GPU (SrCameraF64), so the f32 traversal runs on small numbers.

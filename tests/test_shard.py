@@ -59,6 +59,58 @@ def test_two_ranks_shard_observers_and_reduce_the_max():
     assert n0 == n1 == 2000
 
 
+class _BandEngine:
+    """Stands in for the engine's sr_adjoint_rows: each loss-level row r adds (r + 1) * (1, 2, ..., 10)
+    to the ten results, so the reduced sum checks that the bands cover every row exactly once."""
+
+    def adjoint(self, idx, u, cam, target, level, rows=None):
+        import types
+        r0, r1 = rows
+        w = sum(r + 1 for r in range(r0, r1))
+        return types.SimpleNamespace(loss=1.0 * w, grad=[(k + 2.0) * w for k in range(7)], primal_mismatch=9.0 * w,
+                                     star_terms=10.0 * w)
+
+
+def _adjoint_worker(rank, port, q):
+    import types
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=WORLD, timeout=datetime.timedelta(seconds=60))
+    try:
+        from specrel_b200 import shard
+        u = types.SimpleNamespace(size=(160, 101))
+        out = shard.adjoint_over_ranks(_BandEngine(), 0, u, None, 0, level=2, dist=dist)
+        q.put((rank, shard.row_band(shard.loss_rows(101, 2), rank, WORLD), [float(x) for x in out]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_shard_the_gradient_rows_and_sum_them():
+    """The sharded gradient (the one collective of the path): two gloo ranks take contiguous
+    bands of the loss level's rows and one all-reduce gives both the whole frame's results."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_adjoint_worker, args=(r, port, q)) for r in range(WORLD)]
+    for p in procs:
+        p.start()
+    try:
+        results = sorted(q.get(timeout=180) for _ in range(WORLD))
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert all(p.exitcode == 0 for p in procs)
+    (_, b0, o0), (_, b1, o1) = results
+    rows = 26  # 101 -> 51 -> 26
+    assert b0 == (0, 13) and b1 == (13, 26)
+    w = sum(r + 1 for r in range(rows))
+    assert o0 == o1 == [1.0 * w] + [(k + 2.0) * w for k in range(7)] + [9.0 * w, 10.0 * w]
+
+
 def test_single_process_needs_no_group():
     from specrel_b200 import shard
     assert shard.max_over_ranks(3.0) == 3.0

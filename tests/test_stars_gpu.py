@@ -61,7 +61,7 @@ def test_binned_batch_mixed_observers(engine, starfield):
 
 
 def test_full_starfield_matches_brute(engine):
-    """configs[4]'s 100k stars over the cube occluders at 640x400, observer at the target rapidity."""
+    """The 100k stars over the cube occluders at 640x400, observer at the target rapidity."""
     s = O.Scene(O.synth_params(5, 1, n_bodies=16, steps=16))
     assert int(s.info.n_stars) == 100000
     engine.upload(9, packed_from_oracle(s))
