@@ -109,6 +109,74 @@ __device__ int decide_split(const int* clo, const int* chi, const int (*blo)[4],
     return 0;
 }
 
+// decide_split computed by the 32 lanes of a warp, lane 8a + i holding bin i of axis a: the left
+// unions and counts of bins 0..i and the right ones of bins i+1..7 by segmented scans (min / max
+// and integer sums are exact in any order), then each candidate's cost by the same expression, and
+// the first strictly lowest cost in the serial order (axis 0..3, split 6..0) by a reduction whose
+// ties go to the earlier candidate. Every lane returns the decision.
+struct SplitChoice {
+    int leaf, axis;
+    float pos;
+};
+__device__ SplitChoice decide_split_warp(const int* clo, const int* chi, const int (*blo)[4], const int (*bhi)[4],
+                                         const uint32_t* bcnt, uint32_t lane) {
+    const int a = (int)(lane >> 3), i = (int)(lane & 7u);
+    const float amin = oval(clo[a]);
+    const float ext = oval(chi[a]) - amin;
+    const bool live = ext >= 1e-4f;
+    float l[8], r[8];
+    for (int k = 0; k < 4; ++k) {
+        l[k] = oval(blo[lane][k]);
+        l[4 + k] = oval(bhi[lane][k]);
+    }
+    uint32_t lc = bcnt[lane];
+    for (int k = 0; k < 8; ++k) r[k] = l[k];
+    uint32_t rc = lc;
+    for (int d = 1; d < 8; d <<= 1) {  // inclusive scans within the axis's 8 lanes
+        uint32_t up_c = __shfl_up_sync(0xFFFFFFFFu, lc, d, 8), dn_c = __shfl_down_sync(0xFFFFFFFFu, rc, d, 8);
+        for (int k = 0; k < 8; ++k) {
+            const float u = __shfl_up_sync(0xFFFFFFFFu, l[k], d, 8), v = __shfl_down_sync(0xFFFFFFFFu, r[k], d, 8);
+            if (i >= d) l[k] = k < 4 ? fminf(l[k], u) : fmaxf(l[k], u);
+            if (i + d < 8) r[k] = k < 4 ? fminf(r[k], v) : fmaxf(r[k], v);
+        }
+        if (i >= d) lc += up_c;
+        if (i + d < 8) rc += dn_c;
+    }
+    // The right side of split i is bins i+1..7: the next lane's suffix.
+    float rr[8];
+    for (int k = 0; k < 8; ++k) rr[k] = __shfl_down_sync(0xFFFFFFFFu, r[k], 1, 8);
+    const uint32_t rrc = __shfl_down_sync(0xFFFFFFFFu, rc, 1, 8);
+    float cost = INFINITY;
+    if (live && i < 7 && lc > 0 && rrc > 0)
+        cost = (float)lc * box_measure(l, l + 4) + (float)rrc * box_measure(rr, rr + 4);
+    int order = (cost < INFINITY) ? a * 8 + (6 - i) : 1 << 20;  // the serial loop's visiting order
+    if (!(cost < INFINITY)) cost = INFINITY;
+    for (int off = 16; off > 0; off >>= 1) {
+        const float oc = __shfl_xor_sync(0xFFFFFFFFu, cost, off);
+        const int oo = __shfl_xor_sync(0xFFFFFFFFu, order, off);
+        if (oc < cost || (oc == cost && oo < order)) {
+            cost = oc;
+            order = oo;
+        }
+    }
+    SplitChoice c{0, 0, 0.0f};
+    if (cost < INFINITY) {
+        const int ba = order >> 3, bi = 6 - (order & 7);
+        const float bmin = oval(clo[ba]), bext = oval(chi[ba]) - bmin;
+        c.axis = ba;
+        c.pos = bmin + ((float)(bi + 1) / 8.0f) * bext;
+        return c;
+    }
+    float me = -1.0f;
+    for (int x = 0; x < 4; ++x) {
+        const float e = oval(chi[x]) - oval(clo[x]);
+        if (e > me) { me = e; c.axis = x; }
+    }
+    if (me < 1e-5f) { c.leaf = 1; return c; }
+    c.pos = (oval(clo[c.axis]) + oval(chi[c.axis])) * 0.5f;
+    return c;
+}
+
 // Bin of centroid coordinate c: min(trunc((c - amin) * inv), 7), 0 for NaN or <= 0.
 __device__ __forceinline__ int bin_of(float c, float amin, float inv) {
     const float x = (c - amin) * inv;
@@ -355,10 +423,11 @@ struct SResult {
     uint32_t nodes, depth, max_leaf, bad;
 };
 
-__global__ void __launch_bounds__(256) k_small_build(const STask* tasks, const float4* box, const float4* cen,
-                                                    uint32_t* perm, SrGpuNode* out, SResult* res) {
+__global__ void __launch_bounds__(256) k_small_build(const STask* tasks, const uint32_t* ids, const float4* box,
+                                                    const float4* cen, uint32_t* perm, SrGpuNode* out, SResult* res) {
     extern __shared__ float4 sm[];
-    const STask tk = tasks[blockIdx.x];
+    const uint32_t task = ids[blockIdx.x];
+    const STask tk = tasks[task];
     const uint32_t n = tk.count;
     float4* slo = sm;
     float4* shi = sm + SMALL;
@@ -465,10 +534,11 @@ __global__ void __launch_bounds__(256) k_small_build(const STask* tasks, const f
             }
             __syncthreads();
         }
+        SplitChoice ch{1, 0, 0.0f};
+        if (!small_leaf && threadIdx.x < 32) ch = decide_split_warp(red + 8, red + 12, bl, bh, bc, threadIdx.x);
         if (threadIdx.x == 0) {
-            int leaf = small_leaf ? 1 : 0, axis = 0;
-            float pos = 0.0f;
-            if (!leaf) leaf = decide_split(red + 8, red + 12, bl, bh, bc, &axis, &pos);
+            int leaf = ch.leaf, axis = ch.axis;
+            const float pos = ch.pos;
             uint32_t mid = 0;
             if (!leaf) {
                 // The reference's partition pass.
@@ -517,7 +587,171 @@ __global__ void __launch_bounds__(256) k_small_build(const STask* tasks, const f
     }
     // The subtree's leaf order: the build indices in the final local order.
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) perm[tk.start + i] = sidx[ord[i]];
-    if (threadIdx.x == 0) res[blockIdx.x] = SResult{(uint32_t)node_count, (uint32_t)max_depth, (uint32_t)max_leaf, (uint32_t)bad};
+    if (threadIdx.x == 0) res[task] = SResult{(uint32_t)node_count, (uint32_t)max_depth, (uint32_t)max_leaf, (uint32_t)bad};
+}
+
+// The same build for subtrees of at most TINY primitives, one warp each (WARPS_TINY per block):
+// the same bounds, bins, decision and partition pass with warp synchronisation only, so a launch
+// of small chunks lasts about as many warp steps as its largest chunk has nodes.
+constexpr uint32_t TINY = 256;
+constexpr uint32_t WARPS_TINY = 4;
+struct TinyShared {
+    float4 lo[TINY], hi[TINY], cen[TINY];
+    uint32_t sidx[TINY];
+    uint16_t ord[TINY];
+    int bl[32][4], bh[32][4];
+    uint32_t bc[32];
+    int red[16];
+    uint32_t fs[64], fc[64], fpatch[64], fdepth[64];
+    uint32_t cur_s, cur_c, cur_patch, cur_depth;
+    int sp, node_count, max_depth, max_leaf, bad;
+};
+
+__global__ void __launch_bounds__(32 * WARPS_TINY) k_small_build_warp(const STask* tasks, const uint32_t* ids,
+                                                                      uint32_t n_ids, const float4* box,
+                                                                      const float4* cen, uint32_t* perm, SrGpuNode* out,
+                                                                      SResult* res) {
+    extern __shared__ float4 smw[];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t slot = blockIdx.x * WARPS_TINY + warp;
+    if (slot >= n_ids) return;  // whole warps leave together
+    TinyShared& w = reinterpret_cast<TinyShared*>(smw)[warp];
+    const uint32_t task = ids[slot];
+    const STask tk = tasks[task];
+    const uint32_t n = tk.count;
+    for (uint32_t i = lane; i < n; i += 32) {
+        const uint32_t e = perm[tk.start + i];
+        w.lo[i] = box[2ull * e];
+        w.hi[i] = box[2ull * e + 1];
+        w.cen[i] = cen[e];
+        w.sidx[i] = e;
+        w.ord[i] = (uint16_t)i;
+    }
+    if (lane == 0) {
+        w.fs[0] = 0; w.fc[0] = n; w.fpatch[0] = 0xFFFFFFFFu; w.fdepth[0] = 1;
+        w.sp = 1;
+        w.node_count = 0;
+        w.max_depth = 0;
+        w.max_leaf = 0;
+        w.bad = 0;
+    }
+    __syncwarp();
+    SrGpuNode* o = out + 2ull * tk.start;
+    while (true) {
+        if (lane == 0) {
+            if (w.sp > 0) {
+                --w.sp;
+                w.cur_s = w.fs[w.sp]; w.cur_c = w.fc[w.sp]; w.cur_patch = w.fpatch[w.sp]; w.cur_depth = w.fdepth[w.sp];
+            } else {
+                w.cur_c = 0;
+            }
+        }
+        __syncwarp();
+        const uint32_t s = w.cur_s, c = w.cur_c;
+        if (c == 0) break;
+        // Bounds and centroid bounds, reduced across the warp.
+        float v[16];
+        for (int k = 0; k < 4; ++k) { v[k] = INFINITY; v[4 + k] = -INFINITY; v[8 + k] = INFINITY; v[12 + k] = -INFINITY; }
+        for (uint32_t i = lane; i < c; i += 32) {
+            const uint32_t e = w.ord[s + i];
+            const float4 a = w.lo[e], b = w.hi[e], m = w.cen[e];
+            for (int k = 0; k < 4; ++k) {
+                v[k] = fminf(v[k], ax(a, k));
+                v[4 + k] = fmaxf(v[4 + k], ax(b, k));
+                v[8 + k] = fminf(v[8 + k], ax(m, k));
+                v[12 + k] = fmaxf(v[12 + k], ax(m, k));
+            }
+        }
+        for (int k = 0; k < 16; ++k) {
+            const bool mx = (k / 4) % 2 == 1;
+            float x = v[k];
+            for (int off = 16; off > 0; off >>= 1) {
+                const float y = __shfl_xor_sync(0xFFFFFFFFu, x, off);
+                x = mx ? fmaxf(x, y) : fminf(x, y);
+            }
+            v[k] = x;
+        }
+        if (lane == 0)
+            for (int k = 0; k < 16; ++k) w.red[k] = okey(v[k]);
+        for (uint32_t j = lane; j < 128; j += 32) { (&w.bl[0][0])[j] = okey(INFINITY); (&w.bh[0][0])[j] = okey(-INFINITY); }
+        w.bc[lane] = 0;
+        __syncwarp();
+        const bool small_leaf = c <= 3;
+        if (!small_leaf) {
+            float amin[4], inv[4];
+            bool live[4];
+            for (int a = 0; a < 4; ++a) {
+                amin[a] = oval(w.red[8 + a]);
+                const float ext = oval(w.red[12 + a]) - amin[a];
+                inv[a] = 8.0f / ext;
+                live[a] = ext >= 1e-4f;
+            }
+            for (uint32_t i = lane; i < c; i += 32) {
+                const uint32_t e = w.ord[s + i];
+                const float4 a = w.lo[e], b = w.hi[e], m = w.cen[e];
+                for (int x = 0; x < 4; ++x) {
+                    if (!live[x]) continue;
+                    const int bi = x * BINS + bin_of(ax(m, x), amin[x], inv[x]);
+                    for (int k = 0; k < 4; ++k) {
+                        atomicMin(&w.bl[bi][k], okey(ax(a, k)));
+                        atomicMax(&w.bh[bi][k], okey(ax(b, k)));
+                    }
+                    atomicAdd(&w.bc[bi], 1u);
+                }
+            }
+            __syncwarp();
+        }
+        SplitChoice ch{1, 0, 0.0f};
+        if (!small_leaf) ch = decide_split_warp(w.red + 8, w.red + 12, w.bl, w.bh, w.bc, lane);
+        if (lane == 0) {
+            int leaf = ch.leaf, axis = ch.axis;
+            const float pos = ch.pos;
+            uint32_t mid = 0;
+            if (!leaf) {
+                // The reference's partition pass.
+                for (uint32_t i = 0; i < c; ++i) {
+                    const uint16_t e = w.ord[s + i];
+                    if (ax(w.cen[e], axis) < pos) {
+                        w.ord[s + i] = w.ord[s + mid];
+                        w.ord[s + mid] = e;
+                        ++mid;
+                    }
+                }
+                if (mid == 0 || mid == c) {  // the reference selects by median here: not supported
+                    w.bad = 1;
+                    leaf = 1;
+                }
+            }
+            const int idx = w.node_count++;
+            SrGpuNode nd;
+            for (int k = 0; k < 4; ++k) { nd.min[k] = oval(w.red[k]); nd.max[k] = oval(w.red[4 + k]); }
+            if (leaf) {
+                nd.right_or_first = tk.start + s;
+                nd.count = c;
+                nd.left = 0;
+                if ((int)c > w.max_leaf) w.max_leaf = (int)c;
+            } else {
+                nd.right_or_first = 0;
+                nd.count = 0;
+                nd.left = (uint32_t)idx + 1;
+            }
+            nd.pad = 0;
+            o[idx] = nd;
+            if (w.cur_patch != 0xFFFFFFFFu) o[w.cur_patch].right_or_first = (uint32_t)idx;
+            if ((int)w.cur_depth > w.max_depth) w.max_depth = (int)w.cur_depth;
+            if (!leaf) {
+                if (w.sp + 2 > 64) {
+                    w.bad = 2;
+                } else {
+                    w.fs[w.sp] = s + mid; w.fc[w.sp] = c - mid; w.fpatch[w.sp] = (uint32_t)idx; w.fdepth[w.sp] = w.cur_depth + 1; ++w.sp;
+                    w.fs[w.sp] = s; w.fc[w.sp] = mid; w.fpatch[w.sp] = 0xFFFFFFFFu; w.fdepth[w.sp] = w.cur_depth + 1; ++w.sp;
+                }
+            }
+        }
+        __syncwarp();
+    }
+    for (uint32_t i = lane; i < n; i += 32) perm[tk.start + i] = w.sidx[w.ord[i]];
+    if (lane == 0) res[task] = SResult{(uint32_t)w.node_count, (uint32_t)w.max_depth, (uint32_t)w.max_leaf, (uint32_t)w.bad};
 }
 
 // Small subtree nodes into the final array at `base` (links made absolute).
@@ -761,9 +995,28 @@ cudaError_t gpu_bvh_build_forest(const float4* box, uint32_t n, const GpuSegment
         BK(dst.alloc(ns, st));
         BK(dres.alloc(ns, st));
         BK(cudaMemcpyAsync(dst.p, small.data(), ns * sizeof(STask), cudaMemcpyHostToDevice, st));
-        const size_t smem = 3 * SMALL * sizeof(float4) + SMALL * (sizeof(uint32_t) + sizeof(uint16_t));
-        BK(cudaFuncSetAttribute(k_small_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_small_build<<<ns, 256, smem, st>>>(dst.p, box, cen.p, perm.p, tmp.p, dres.p);
+        // Subtrees of at most TINY primitives one warp each, the others one block each.
+        std::vector<uint32_t> ids;
+        uint32_t n_tiny = 0;
+        for (uint32_t k = 0; k < ns; ++k)
+            if (small[k].count <= TINY) ids.push_back(k);
+        n_tiny = (uint32_t)ids.size();
+        for (uint32_t k = 0; k < ns; ++k)
+            if (small[k].count > TINY) ids.push_back(k);
+        Buf<uint32_t> dids;
+        BK(dids.alloc(ns, st));
+        BK(cudaMemcpyAsync(dids.p, ids.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        if (n_tiny) {
+            const size_t smem_w = WARPS_TINY * sizeof(TinyShared);
+            BK(cudaFuncSetAttribute(k_small_build_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_w));
+            k_small_build_warp<<<(n_tiny + WARPS_TINY - 1) / WARPS_TINY, 32 * WARPS_TINY, smem_w, st>>>(
+                dst.p, dids.p, n_tiny, box, cen.p, perm.p, tmp.p, dres.p);
+        }
+        if (ns > n_tiny) {
+            const size_t smem = 3 * SMALL * sizeof(float4) + SMALL * (sizeof(uint32_t) + sizeof(uint16_t));
+            BK(cudaFuncSetAttribute(k_small_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_small_build<<<ns - n_tiny, 256, smem, st>>>(dst.p, dids.p + n_tiny, box, cen.p, perm.p, tmp.p, dres.p);
+        }
         BK(cudaGetLastError());
         BK(cudaMemcpyAsync(res.data(), dres.p, ns * sizeof(SResult), cudaMemcpyDeviceToHost, st));
         BK(cudaStreamSynchronize(st));
