@@ -649,6 +649,30 @@ __global__ void __launch_bounds__(32 * WARPS_TINY) k_small_build_warp(const STas
         __syncwarp();
         const uint32_t s = w.cur_s, c = w.cur_c;
         if (c == 0) break;
+        const bool small_leaf = c <= 3;
+        if (small_leaf) {  // a leaf needs only its box: lane 0 takes the min / max of its few boxes
+            if (lane == 0) {
+                float lo[4] = {INFINITY, INFINITY, INFINITY, INFINITY}, hi[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+                for (uint32_t i = 0; i < c; ++i) {
+                    const uint32_t e = w.ord[s + i];
+                    const float4 a = w.lo[e], b = w.hi[e];
+                    for (int k = 0; k < 4; ++k) { lo[k] = fminf(lo[k], ax(a, k)); hi[k] = fmaxf(hi[k], ax(b, k)); }
+                }
+                const int idx = w.node_count++;
+                SrGpuNode nd;
+                for (int k = 0; k < 4; ++k) { nd.min[k] = lo[k]; nd.max[k] = hi[k]; }
+                nd.right_or_first = tk.start + s;
+                nd.count = c;
+                nd.left = 0;
+                nd.pad = 0;
+                if ((int)c > w.max_leaf) w.max_leaf = (int)c;
+                o[idx] = nd;
+                if (w.cur_patch != 0xFFFFFFFFu) o[w.cur_patch].right_or_first = (uint32_t)idx;
+                if ((int)w.cur_depth > w.max_depth) w.max_depth = (int)w.cur_depth;
+            }
+            __syncwarp();
+            continue;
+        }
         // Bounds and centroid bounds, reduced across the warp.
         float v[16];
         for (int k = 0; k < 4; ++k) { v[k] = INFINITY; v[4 + k] = -INFINITY; v[8 + k] = INFINITY; v[12 + k] = -INFINITY; }
@@ -676,8 +700,7 @@ __global__ void __launch_bounds__(32 * WARPS_TINY) k_small_build_warp(const STas
         for (uint32_t j = lane; j < 128; j += 32) { (&w.bl[0][0])[j] = okey(INFINITY); (&w.bh[0][0])[j] = okey(-INFINITY); }
         w.bc[lane] = 0;
         __syncwarp();
-        const bool small_leaf = c <= 3;
-        if (!small_leaf) {
+        {
             float amin[4], inv[4];
             bool live[4];
             for (int a = 0; a < 4; ++a) {
@@ -701,8 +724,7 @@ __global__ void __launch_bounds__(32 * WARPS_TINY) k_small_build_warp(const STas
             }
             __syncwarp();
         }
-        SplitChoice ch{1, 0, 0.0f};
-        if (!small_leaf) ch = decide_split_warp(w.red + 8, w.red + 12, w.bl, w.bh, w.bc, lane);
+        const SplitChoice ch = decide_split_warp(w.red + 8, w.red + 12, w.bl, w.bh, w.bc, lane);
         if (lane == 0) {
             int leaf = ch.leaf, axis = ch.axis;
             const float pos = ch.pos;
