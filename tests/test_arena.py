@@ -168,3 +168,35 @@ def test_single_chunk_root_and_nothing():
     assert nodes[0]["count"] == 0 and nodes[0]["left"] == 0 and nodes[0]["right_or_first"] == 0
     assert (nodes[0]["min"] > nodes[0]["max"]).all()
     assert W.in_tree(nodes, g, a) == []
+
+
+def test_validation_takes_the_reference_arena_arrays():
+    """The arrays the reference's dynamic flow uploads (an arena's, free room included) pass the
+    upload's checks; a root over nothing (an empty arena) is an empty tree; a real cycle is refused."""
+    sc = sr.synth_scene(1, 1, n_bodies=4, steps=8)
+    boxes, geoms, attrs, p = sc.build_inputs()
+    w = W.World(sc.tubes()[0], (boxes, geoms, attrs))
+    A = O.Arena()
+    for k in range(5):
+        drive(w, A, k)
+    nodes, g, a = A.arrays()
+    st, depth, msg = sr.validate(sr.PackedScene(nodes, g, a, p.materials, np.zeros(4, np.float32), 0))
+    assert st == 0 and depth > 3, msg
+    E = O.Arena()
+    E.begin()
+    E.finish()
+    en, eg, ea = E.arrays()
+    st, depth, msg = sr.validate(sr.PackedScene(en, eg, ea, p.materials, np.zeros(4, np.float32), 0))
+    assert st == 0 and depth == 1, msg
+    bad = nodes.copy()
+    bad[0]["min"] = bad[0]["max"]  # a real box: node 0 linking to itself is now a cycle
+    bad[0]["count"] = 0
+    bad[0]["left"] = 0
+    bad[0]["right_or_first"] = 0
+    st, _, msg = sr.validate(sr.PackedScene(bad, g, a, p.materials, np.zeros(4, np.float32), 0))
+    assert st != 0 and "twice" in msg
+
+
+def test_top_tree_needs_two_items():
+    with pytest.raises(sr.SrError):
+        sr.top_tree(np.zeros((1, 8), np.float32), np.zeros(1, np.uint32), np.ones(1, np.float32), 0)
