@@ -473,6 +473,29 @@ __global__ void __launch_bounds__(256) k_small_build(const STask* tasks, const u
         __syncthreads();
         if (cur_c == 0) break;
         const uint32_t s = cur_s, c = cur_c;
+        if (c <= 3) {  // a leaf needs only its box: thread 0 takes the min / max of its few boxes
+            if (threadIdx.x == 0) {
+                float lo[4] = {INFINITY, INFINITY, INFINITY, INFINITY}, hi[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+                for (uint32_t i = 0; i < c; ++i) {
+                    const uint32_t e = ord[s + i];
+                    const float4 a = slo[e], b = shi[e];
+                    for (int k = 0; k < 4; ++k) { lo[k] = fminf(lo[k], ax(a, k)); hi[k] = fmaxf(hi[k], ax(b, k)); }
+                }
+                const int idx = node_count++;
+                SrGpuNode nd;
+                for (int k = 0; k < 4; ++k) { nd.min[k] = lo[k]; nd.max[k] = hi[k]; }
+                nd.right_or_first = tk.start + s;
+                nd.count = c;
+                nd.left = 0;
+                nd.pad = 0;
+                if ((int)c > max_leaf) max_leaf = (int)c;
+                o[idx] = nd;
+                if (cur_patch != 0xFFFFFFFFu) o[cur_patch].right_or_first = (uint32_t)idx;
+                if ((int)cur_depth > max_depth) max_depth = (int)cur_depth;
+            }
+            __syncthreads();  // every thread has read this node before the next is popped
+            continue;
+        }
         // Bounds and centroid bounds.
         float v[16];
         for (int k = 0; k < 4; ++k) { v[k] = INFINITY; v[4 + k] = -INFINITY; v[8 + k] = INFINITY; v[12 + k] = -INFINITY; }
