@@ -1,22 +1,37 @@
 #!/usr/bin/env python
 """Headline benchmark: primary rays per second on the 7.9M-tetrahedron 1280x800 scene.
 
-Workload: 64 accelerated icospheres (subdivision 2) on Fermi-Walker
-worldlines, 128 time steps, ~7.9M tetrahedra; observers at t = 0 at the origin with rapidities
-|phi| <= 2; 1280x800; past light cone; Lorentz-invariant null shadows from a point light at
-(0, 50, 0); FP32 traversal. Synthetic, seeded (the reference ships no scenes for these configs).
+Workload: 64 accelerated icospheres (subdivision 2) on Fermi-Walker worldlines, 128 time steps,
+~7.9M tetrahedra; observers at t = 0 at the origin with rapidities |phi| <= 2; 1280x800; past
+light cone; Lorentz-invariant null shadows from a point light at (0, 50, 0); FP32 traversal.
+Synthetic, seeded (the reference ships no scenes for these configurations).
 
 One step renders a batch of B observers (B frames of 1,024,000 rays each) through the batched
 fast path with the FP64 camera (tetrad and event built in double on the GPU, rebased to the scene
 anchor). `value` is Mrays/s over all ranks (weak scaling: every rank renders its own batch of
-observers, no data-path collective). The plain single-frame path is timed on the same observers
-for comparison (`plain`), as is the end-to-end call through the C ABI with host buffers (`e2e`).
+observers, no data-path collective). The same line carries:
+
+  plain        the plain single-frame path on the same observers (batched over plain: the metric's
+               "batched vs plain");
+  parity       observer 0's frame against the all-FP64 oracle (scene built and rendered in double):
+               hit-id agreement (the metric's "hit-ID match % vs FP64"), lambda / tau / RGB errors;
+  e2e          the same batches through the C ABI with host buffers;
+  value_fresh  every step a new seeded set of observers, L2 flushed before each step;
+  config4      64 observers of mixed resolution and slice mode over the 147k-tet cube scene in one
+               batch, against looping the plain path;
+  config5      the image-loss gradient of one 1280x800 observer over 100k stars;
+  cpu_baseline the oracle (C++ restatement of the reference's CPU renderer) on the host cores.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+`--impl reference` times the reference's CPU renderer (its C++ restatement in oracle/: the Rust
+renderer cannot be built here) on the host cores, on the same scene (built by the oracle) and the
+same observers, each on a sample of every 8th row.
 """
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import os
 import subprocess
@@ -31,8 +46,9 @@ sys.path.insert(0, ROOT)
 
 W, H = 1280, 800
 RAYS_PER_FRAME = W * H
-METRIC = "Mrays/s on 1 B200, 1280x800 8M-tet scene (batched fast path); primary rays"
+METRIC = "Mrays/s on 1 B200, 1280×800 8M-tet scene, batched vs plain; hit-ID match % vs FP64"
 UNIT = "Mrays/s"
+ROW_STRIDE = 8  # the CPU arms render every 8th row of each frame
 
 
 def parse():
@@ -44,15 +60,33 @@ def parse():
     ap.add_argument("--batch", type=int, default=8, help="observers (1280x800 frames) per step per GPU")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the FP64-oracle parity block")
+    ap.add_argument("--no-extra", action="store_true", help="skip the config4 / config5 / fresh-observer legs")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch parameters")
     ap.add_argument("--bodies", type=int, default=64,
                     help="icospheres in the scene (64 is the workload; fewer only for small profiling captures)")
     ap.add_argument("--workload", choices=["config2", "config4", "config5"], default="config2",
-                    help="config2: the headline (8 observers of the 7.9M-tet scene per step); config4: 64 observers "
-                         "of mixed resolution and slice mode over the 147k-tet cube scene, batched against a loop "
-                         "of the plain single-frame path; config5: the image-loss gradient of one 1280x800 observer "
-                         "over 100k stars and the cube occluders")
+                    help="config2: the headline (8 observers of the 7.9M-tet scene per step, with the config4 and "
+                         "config5 legs as extra keys); config4 / config5 alone: see run_config4 / run_config5")
     return ap.parse_args()
+
+
+def load_shard():
+    """specrel_b200/shard.py (numpy only) loaded by path, so that the reference arm maps no engine code."""
+    spec = importlib.util.spec_from_file_location("sr_shard", os.path.join(ROOT, "specrel_b200", "shard.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_config(args, world):
+    """The `config` of both arms (identical, so the two lines describe the same workload)."""
+    return {"workload": "64 accelerated icospheres (subdiv 2), 128 steps, 7,864,320 tets, 1280x800, past light "
+                        "cone, Lorentz-invariant null shadows, light (0,50,0), FP32 traversal + FP64 camera",
+            "observers_per_step_per_gpu": args.batch, "seed": args.seed, "bodies": args.bodies,
+            "l2": "inputs larger than L2 (the scene is >2.6 GB on the device against a 126 MB L2); value_fresh "
+                  "also renders new observers every step with L2 flushed before each",
+            "parallelism": f"replicas x{world}, observers sharded"}
 
 
 class ClockSampler:
@@ -119,76 +153,235 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "trace_lean_config2.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            d = json.load(f)
-        return d.get("dram_bytes_per_launch"), d
-    return None, None
+def oracle_row_config(O, stride=ROW_STRIDE):
+    """Every `stride`-th row of the 1280x800 frame (1280 x 800/stride rays), shadows on."""
+    return O.make_config(W, H // stride, 0, 1, 0, full_height=H, row_stride=stride, row_offset=stride // 2)
 
 
-def cpu_baseline(packed, cam_rapidity, sample_stride=8):
+def cpu_baseline(packed, rapidities):
     """The reference CPU renderer (oracle/: the C++ restatement of renderer.rs, f32, rows over all
-    host threads, serial bloom) on a bounded sample of the same frame: every `sample_stride`-th row
-    of the 1280x800 frame (1280 x 100 rays), one warm-up then the median of 3."""
+    host threads, serial bloom) on a bounded sample of the same step: each observer's every 8th row
+    (1280 x 100 rays per observer), one warm-up then the median of 3 passes."""
     from oracle import oracle as O
     sc = O.Scene.from_packed(packed.nodes, packed.geoms, packed.attrs, packed.materials, packed.stars,
                              packed.num_stars, packed.light_pos)
-    cam = O.make_camera(rapidity=cam_rapidity)
-    rows = H // sample_stride
-    cfg = O.make_config(W, rows, 0, 1, 0, full_height=H, row_stride=sample_stride, row_offset=sample_stride // 2)
+    cams = [O.make_camera(rapidity=r) for r in rapidities]
+    cfg = oracle_row_config(O)
     threads = os.cpu_count() or 1
-    O.render(sc, cam, cfg, threads=threads, aux=False)
+    for c in cams:
+        O.render(sc, c, cfg, threads=threads, aux=False)
     ts = []
     for _ in range(3):
         t0 = time.perf_counter()
-        O.render(sc, cam, cfg, threads=threads, aux=False)
+        for c in cams:
+            O.render(sc, c, cfg, threads=threads, aux=False)
         ts.append(time.perf_counter() - t0)
     t = float(np.median(ts))
-    return {"value": W * rows / t / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"rows {sample_stride // 2}::{sample_stride} of the 1280x800 frame ({W}x{rows} rays, shadows "
-                      f"on, bloom on the sample), oracle C++ f32 restatement of render_frame, median of 3 after a "
-                      f"warm-up; {t * 1e3:.1f} ms per sample"}
+    rays = W * (H // ROW_STRIDE) * len(cams)
+    return {"value": rays / t / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"rows {ROW_STRIDE // 2}::{ROW_STRIDE} of each of the step's {len(cams)} observers' frames "
+                      f"({rays} rays, shadows on, bloom on the sample), oracle C++ f32 restatement of render_frame, "
+                      f"median of 3 after a warm-up; {t * 1e3:.1f} ms per pass"}
 
 
 def run_reference(args, rank, world):
-    """The reference arm: the reference's CPU renderer (Rust) cannot be built here (no cargo/rustc),
-    so its C++ restatement in oracle/ is timed on the host cores, on the engine arm's workload."""
+    """The reference arm. The reference's CPU renderer is Rust (renderer.rs:327-412) and cannot be
+    built here (no cargo / rustc), so its C++ restatement in oracle/ is timed on all host cores. The
+    scene is built by the oracle itself (the same arrays as the engine's scene builder produces),
+    and each step renders the engine arm's observers, each on every 8th row of its frame."""
     if rank != 0:
         return
-    import specrel_b200 as sr
     from oracle import oracle as O
-    scene = sr.synth_scene(2, args.seed)
-    p = scene.packed()
-    sc = O.Scene.from_packed(p.nodes, p.geoms, p.attrs, p.materials, p.stars, p.num_stars, p.light_pos)
-    rap = tuple(scene.info.cam_rapidity)
-    cam = O.make_camera(rapidity=rap)
-    stride = 8
-    rows = H // stride
-    cfg = O.make_config(W, rows, 0, 1, 0, full_height=H, row_stride=stride, row_offset=stride // 2)
+    shard = load_shard()
+    t0 = time.time()
+    sc = O.Scene(O.synth_params(2, args.seed, n_bodies=args.bodies))
+    build_s = time.time() - t0
+    raps = shard.observer_rapidities(args.seed, 0, args.batch, tuple(sc.info.cam_rapidity))
+    cams = [O.make_camera(rapidity=r) for r in raps]
+    cfg = oracle_row_config(O)
     threads = os.cpu_count() or 1
+
+    def step():
+        for c in cams:
+            O.render(sc, c, cfg, threads=threads, aux=False)
+
     for _ in range(args.warmup):
-        O.render(sc, cam, cfg, threads=threads, aux=False)
+        step()
     ts = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        O.render(sc, cam, cfg, threads=threads, aux=False)
+        step()
         ts.append(time.perf_counter() - t0)
     t = float(np.mean(ts))
-    v = W * rows / t / 1e6
+    rays = W * (H // ROW_STRIDE) * len(cams)
+    v = rays / t / 1e6
+    sample = (f"each step: rows {ROW_STRIDE // 2}::{ROW_STRIDE} of each of the {len(cams)} observers' 1280x800 frames "
+              f"({rays} rays), all {threads} host threads; the Rust renderer is not buildable here (no cargo/rustc), "
+              "so the oracle's C++ restatement of render_frame is timed")
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded accelerated-icosphere scene)", "impl": "reference",
-            "config": {"workload": "64 accelerated icospheres, 7.9M tets, 1280x800, null shadows",
-                       "sample": f"every {stride}th row ({W}x{rows} rays) per step"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"every {stride}th row of the 1280x800 frame, all host threads; the Rust "
-                                       "renderer is not buildable here (no cargo/rustc), so the oracle's C++ "
-                                       "restatement of render_frame is timed"},
+            "vs_baseline": None, "dtype": "f32", "impl": "reference",
+            "data": "synthetic (seeded accelerated-icosphere scene, built by the oracle)",
+            "config": workload_config(args, world), "rays_per_step": rays, "scene_build_s": round(build_s, 2),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def parity_fp64(args, eng, u0, cam0, rap0):
+    """Observer 0's frame on the fast path with the FP64 camera (the measured configuration)
+    against the all-FP64 oracle: the scene built and rendered in double, the whole 1280x800 frame
+    (bloom included), on the host cores."""
+    import specrel_b200 as sr
+    from oracle import oracle as O
+    t0 = time.time()
+    s64 = O.Scene(O.synth_params(2, args.seed, n_bodies=args.bodies), fp64=True)
+    ref = O.render(s64, O.make_camera(rapidity=rap0), O.make_config(W, H, 0, 1, 0), threads=os.cpu_count() or 1)
+    del s64
+    fr = eng.render(0, u0, path=sr.SR_PATH_FAST, aux=True, cam=cam0)
+    miss = 0xFFFFFFFF
+    gid, oid = fr.hit_id.astype(np.uint32), ref.orig.astype(np.uint32)
+    same = gid == oid
+    hit = same & (gid != miss)
+    lam = np.abs(fr.lam[hit].astype(np.float64) - ref.lam[hit]) / np.abs(ref.lam[hit])
+    tau = np.abs(fr.tau[hit].astype(np.float64) - ref.tau[hit]) / np.maximum(np.abs(ref.tau[hit]), 1.0)
+
+    def ch(x):
+        x = x.astype(np.uint32)
+        return np.stack([(x >> 16) & 255, (x >> 8) & 255, x & 255], -1).astype(np.int32)
+
+    d = np.abs(ch(fr.rgb) - ch(ref.rgb)).max(-1)
+    return {"reference": "all-FP64 oracle (scene built and rendered in double), observer 0, whole 1280x800 frame",
+            "pixels": int(same.size), "hit_id_match_pct": float(same.mean() * 100.0),
+            "hit_id_mismatches": int((~same).sum()),
+            "lambda_rel_max": float(lam.max()), "lambda_rel_median": float(np.median(lam)),
+            "tau_rel_max": float(tau.max()), "tau_rel_median": float(np.median(tau)),
+            "rgb8_max_abs": int(d.max()), "rgb8_max_abs_on_agreeing_hits": int(d[same].max()),
+            "rgb8_frac_gt1": float((d > 1).mean()), "seconds": round(time.time() - t0, 1)}
+
+
+def config4_measure(args, rank, world, local, dist, stream, eng, idx):
+    """The cube scene (64 inertial unit cubes, 147k tets) seen by 64 observers in one batch:
+    resolutions drawn from {320x200, 640x400, 1280x800, 1920x1200}, events t in [-50, 0] with
+    |x| <= 30, rapidities |phi| <= 3, half past light cone and half God's-eye slice. One step = the
+    whole batch through the batched fast path with FP64 cameras (one captured graph); `plain` loops
+    the plain single-frame path over the same observers. Observers are sharded over ranks."""
+    import torch
+    import specrel_b200 as sr
+    from specrel_b200 import shard
+    scene = sr.synth_scene(1, args.seed)
+    eng.upload(idx, scene)
+    draws = [o for i, o in enumerate(sr.observers(args.seed, 64)) if i % world == rank]
+    us, cams = [], []
+    for o in draws:
+        c = sr.camera(tuple(o["pos"]), 90.0, rapidity=o["rapidity"])
+        us.append(sr.uniforms(c, o["width"], o["height"], 0, 1 if o["slice_mode"] == 0 else 2, o["slice_mode"],
+                              num_nodes=scene.num_nodes, light_pos=scene.light_pos))
+        cams.append(sr.cam64(o["pos"], o["rapidity"]))
+    rays = sum(u.size[0] * u.size[1] for u in us)
+    out = torch.empty(max(rays, 1), dtype=torch.int32, device=f"cuda:{local}")
+    ptr = out.data_ptr()
+
+    def timed(fn, k):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return shard.max_over_ranks(e0.elapsed_time(e1) / k, dist, f"cuda:{local}")
+
+    def batch_step():
+        eng.render_batch(idx, us, ptr, rays, cams=cams, device_output=True)
+
+    def plain_step():
+        off = 0
+        for u in us:
+            eng.render_into(idx, u, ptr + 4 * off, path=sr.SR_PATH_PLAIN)
+            off += u.size[0] * u.size[1]
+
+    with torch.cuda.stream(stream):
+        if not args.no_autotune:
+            eng.autotune(idx, us[0], 2)
+        ms = timed(batch_step, args.steps)
+        plain_ms = timed(plain_step, max(2, args.steps // 2))
+        ph = eng.render_batch(idx, us, ptr, rays, cams=cams, device_output=True, phases=True)
+    total = rays
+    if dist is not None:
+        t = torch.tensor([rays], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t)
+        total = int(t.item())
+    sizes = {}
+    for o in draws:
+        key = f"{o['width']}x{o['height']}"
+        sizes[key] = sizes.get(key, 0) + 1
+    value = total / (ms / 1e3) / 1e6
+    plain_value = total / (plain_ms / 1e3) / 1e6
+    tuning = eng.tuning(idx)
+    res = {"metric": "Mrays/s, 64 observers of the 147k-tet cube scene in one batch; primary rays",
+           "value": value, "unit": UNIT, "ms_per_step": ms, "rays_per_step": total,
+           "workload": f"{scene.num_prims} tets, 64 observers (sizes {sizes}), past light cone and God's-eye "
+                       "slice 50/50, FP64 cameras; scene L2-resident",
+           "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms},
+           "speedup_batched_over_plain": value / plain_value,
+           "phases_ms": {"trace": ph.trace_ms, "shade": ph.shade_ms, "stars": ph.stars_ms, "bloom": ph.bloom_ms},
+           "tuning": {k: getattr(tuning, k)
+                      for k, _ in tuning._fields_}}
+    del out
+    return res
+
+
+def config5_measure(args, local, stream, eng, idx):
+    """100k inertial stars on a sphere of radius 1e3 over the cube scene, 1280x800, target rendered
+    at rapidity (0.8, -0.3, 0.5). Times, with CUDA events on the engine's stream: one forward frame
+    on the fast path (FP64 camera, binned stars) and one loss-and-gradient evaluation (sr_adjoint:
+    the forward frame recomputed, then the 7-vector of rapidity and event derivatives in f32 with
+    f64 sums) at loss level 0 (full resolution) and level 3, from rapidity 0."""
+    import torch
+    import specrel_b200 as sr
+    scene = sr.synth_scene(5, args.seed)
+    eng.upload(idx, scene)
+    star = (0.8, -0.3, 0.5)
+    u = sr.uniforms(sr.camera(), W, H, 0, 1, 0, num_nodes=scene.num_nodes, num_stars=scene.num_stars,
+                    light_pos=scene.light_pos)
+    ev = (0.0, 0.0, 0.0, 0.0)
+    out = torch.empty(W * H, dtype=torch.int32, device=f"cuda:{local}")
+    with torch.cuda.stream(stream):
+        tgt = eng.render(idx, u, path=sr.SR_PATH_FAST, hdr=True, cam=sr.cam64(ev, star)).hdr
+        tdev = torch.tensor(tgt, device=f"cuda:{local}").contiguous()
+        cam0 = sr.cam64(ev, (0.0, 0.0, 0.0))
+
+        def timed(fn, k):
+            for _ in range(max(1, args.warmup)):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(k):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / k
+
+        fwd = timed(lambda: eng.render_into(idx, u, out.data_ptr(), path=sr.SR_PATH_FAST, cam=cam0), args.steps)
+        g0 = timed(lambda: eng.adjoint(idx, u, cam0, tdev.data_ptr(), 0), args.steps)
+        g3 = timed(lambda: eng.adjoint(idx, u, cam0, tdev.data_ptr(), 3), args.steps)
+        r = eng.adjoint(idx, u, cam0, tdev.data_ptr(), 0)
+    res = {"metric": "ms per image-loss gradient, 100k stars over the cube scene, 1280x800",
+           "value": g0, "unit": "ms", "higher_is_better": False,
+           "workload": f"{scene.num_prims} tets, {scene.num_stars} stars, 1280x800, target at rapidity "
+                       "(0.8, -0.3, 0.5), gradient at rapidity 0",
+           "forward_frame_ms": fwd, "gradient_level3_ms": g3,
+           "gradient": {"loss": r.loss, "grad": list(r.grad), "star_terms": r.star_terms,
+                        "primal_mismatch": r.primal_mismatch}}
+    del tdev, out
+    return res
 
 
 def run_engine(args, rank, world, local):
@@ -224,6 +417,7 @@ def run_engine(args, rank, world, local):
     def max_over_ranks(x: float) -> float:
         return shard.max_over_ranks(x, dist, f"cuda:{local}")
 
+    extra = {}
     with torch.cuda.stream(stream):
         # Launch parameters for this scene, untimed.
         if not args.no_autotune:
@@ -289,7 +483,30 @@ def run_engine(args, rank, world, local):
         wall_e2e = (time.perf_counter() - t_e2e) / args.steps * 1e3
         e2e_ms = max_over_ranks(max(e0.elapsed_time(e1) / args.steps, wall_e2e))
 
-        # The dominant kernel (k_trace_batch: primary rays and the main light's shadow rays of all
+        # Fresh observers every step (new seeded rapidities, never rendered before), with L2 flushed
+        # (a 256 MiB write) before each step; only the batches are inside the events.
+        if not args.no_extra:
+            flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+            fresh = []
+            for k in range(args.steps):
+                rk = shard.observer_rapidities(args.seed + 1000 + k, rank, B)
+                fresh.append(([sr.uniforms(sr.camera(rapidity=r), W, H, 0, 1, 0, num_nodes=scene.num_nodes,
+                                           light_pos=scene.light_pos) for r in rk],
+                              [sr.cam64((0.0, 0.0, 0.0, 0.0), r) for r in rk]))
+            barrier()
+            torch.cuda.synchronize()
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(args.steps)]
+            for k, (fu, fc) in enumerate(fresh):
+                flush.fill_(k & 255)
+                evs[k][0].record(stream)
+                eng.render_batch(0, fu, ptr, B * RAYS_PER_FRAME, cams=fc, device_output=True)
+                evs[k][1].record(stream)
+            torch.cuda.synchronize()
+            fresh_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs) / args.steps)
+            del flush
+
+        # The dominant kernel (k_trace_lean: primary rays and the main light's shadow rays of all
         # B observers in one launch), timed with CUDA events the library records on the launching
         # stream around each phase of the same batch, then the traversal work of that batch
         # (counting variant).
@@ -304,7 +521,14 @@ def run_engine(args, rank, world, local):
         work = np.array([t.nodes_visited, t.leaves_visited, t.tets_tested, t.shadow_nodes_visited,
                          t.shadow_leaves_visited, t.shadow_tets_tested, t.shadow_rays], dtype=np.float64)
         tuning = eng.tuning(0)
-        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        stats = eng.stats(0)
+
+        if not args.no_extra:
+            extra["config4"] = config4_measure(args, rank, world, local, dist, stream, eng, 1)
+            if rank == 0:
+                extra["config5"] = config5_measure(args, local, stream, eng, 2)
+        if rank == 0 and world == 1 and not args.no_parity:
+            extra["parity"] = parity_fp64(args, eng, us[0], c64[0], raps[0])
 
     if dist is not None:
         dist.barrier()
@@ -325,40 +549,35 @@ def run_engine(args, rank, world, local):
     trace_s = float(np.median(trace_ms)) / 1e3
     achieved = trace_bytes / trace_s / 1e9
     peak, peak_kind = load_peaks()
-    traffic, traffic_src = load_traffic()
     clk = clocks.summary()
-    # The kernel is bound by instruction issue, not HBM (its working set stays in L1/L2): its
-    # warp instructions per launch (one-pass ncu capture of this launch, profiles/) against the
-    # issue peak of 4 warp instructions per SM per clock at the sampled SM clock.
-    issue = None
-    inst = (traffic_src or {}).get("warp_instructions_per_launch")
-    if inst and B == 8 and args.seed == 1 and args.bodies == 64:  # the captured workload
-        mhz = clk["sm_mhz"] or 1965.0
-        peak_issue = sms * 4 * mhz * 1e6 / 1e9
-        ach_issue = inst / trace_s / 1e9
-        issue = {"achieved": ach_issue, "peak": peak_issue, "unit": "G warp-instructions/s", "frac": ach_issue / peak_issue,
-                 "warp_instructions_per_launch": inst, "sms": sms, "sm_mhz": mhz}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded accelerated-icosphere scene: no dataset; the reference ships no such scene)",
-        "config": {"workload": "64 accelerated icospheres (subdiv 2), 128 steps, "
-                               f"{scene.num_prims} tets, 1280x800, past light cone, Lorentz-invariant null shadows, "
-                               "light (0,50,0), FP32 traversal + FP64 camera",
-                   "observers_per_step_per_gpu": B, "rays_per_step": total_rays, "seed": args.seed,
-                   "l2": "inputs larger than L2 (scene %.2f GB on the device vs 126 MB L2)" % (eng.stats(0).device_bytes / 1e9),
-                   "tuning": {k: (list(getattr(tuning, k)) if k == "reserved" else getattr(tuning, k))
-                              for k, _ in tuning._fields_},
-                   "scene_build_s": round(build_s, 2), "parallelism": f"replicas x{world}, observers sharded"},
+        "config": workload_config(args, world),
+        "rays_per_step": total_rays, "tets": scene.num_prims,
+        "footprint": {"scene_device_bytes": int(stats.device_bytes), "fast_nodes": int(stats.fast_nodes),
+                      "layout": "16 sign-octant box copies" if stats.fast_nodes else "plain"},
+        "tuning": {k: getattr(tuning, k)
+                   for k, _ in tuning._fields_},
+        "scene_build_s": round(build_s, 2),
         "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms,
                   "speedup_batched_over_plain": value / plain_value},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 768 * B + 80 * B,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": (768 + 80) * B,
                 "d2h_bytes_per_step": 4 * RAYS_PER_FRAME * B},
         # Kernels per step: camera, trace, shade, 6 bloom down, 5 bloom up, composite.
         "gpu_launches": int(args.steps * 15),
-        "roofline": {"bound": "hbm", "kernel": "k_trace_lean", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic, "issue": issue,
+        # The trace kernel is not bound by HBM: its working set (the light cone's share of the
+        # tree) is served from L1 and L2, so the byte model below (every node visit and test
+        # counted as if fetched) exceeds the HBM roof. What binds it is instruction issue and L1
+        # latency (ncu summaries in profiles/).
+        "roofline": {"bound": "issue", "kernel": "k_trace_lean", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "hbm_frac": achieved / peak, "peak_kind": peak_kind,
+                     "note": "achieved = algorithmic bytes (72 B per node visit, 80 B per tetrahedron test, 21 B "
+                             "written per ray) / trace-kernel time; these bytes are mostly served by L1/L2, so "
+                             "hbm_frac > 1 says the kernel is not HBM-bound. DRAM traffic and warp-instruction "
+                             "counts come from ncu captures (profiles/), not from this run.",
+                     "traffic": None,
                      "algorithmic_bytes_per_launch": trace_bytes, "frames_per_launch": B,
                      "trace_ms_per_launch": trace_s * 1e3,
                      "batch_ms": float(np.median(frame_ms)), "shade_ms": float(np.median(shade_ms)),
@@ -368,9 +587,14 @@ def run_engine(args, rank, world, local):
                                         "shadow_tet_tests": work[5] / B, "shadow_rays": work[6] / B}},
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
     }
+    if not args.no_extra:
+        line["value_fresh"] = {"value": total_rays / (fresh_ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": fresh_ms,
+                               "how": "a new seeded set of observers every step, L2 flushed (256 MiB write) before "
+                                      "each step, device time of the batches only"}
+    line.update(extra)
     if world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline(scene.packed(), tuple(scene.info.cam_rapidity))
+            line["cpu_baseline"] = cpu_baseline(scene.packed(), raps)
         except Exception as exc:  # the baseline is reported, not required for the GPU number
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                                     "sample": f"failed: {exc}"}
@@ -378,168 +602,39 @@ def run_engine(args, rank, world, local):
     eng.close()
 
 
-def run_config4(args, rank, world, local):
-    """The cube scene (64 inertial unit cubes, 147k tets) seen by 64 observers in one
-    batch: resolutions drawn from {320x200, 640x400, 1280x800, 1920x1200}, events t in [-50, 0]
-    with |x| <= 30, rapidities |phi| <= 3, half past light cone and half God's-eye slice (the
-    shared observer draw of the scene builder). One step = the whole batch through the batched fast
-    path with FP64 cameras (one captured graph); `plain` loops the plain single-frame path over the
-    same observers. Launch shape from the autotuner. Observers are sharded over ranks."""
+def _standalone(args, rank, world, local, fn):
+    """One of the extra legs as its own JSON line (config4: observers sharded over ranks)."""
     import torch
     import specrel_b200 as sr
-    from specrel_b200 import shard
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    scene = sr.synth_scene(1, args.seed)
     eng = sr.Engine(local)
-    eng.upload(0, scene)
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
-    draws = [o for i, o in enumerate(sr.observers(args.seed, 64)) if i % world == rank]
-    us, cams = [], []
-    for o in draws:
-        c = sr.camera(tuple(o["pos"]), 90.0, rapidity=o["rapidity"])
-        us.append(sr.uniforms(c, o["width"], o["height"], 0, 1 if o["slice_mode"] == 0 else 2, o["slice_mode"],
-                              num_nodes=scene.num_nodes, light_pos=scene.light_pos))
-        cams.append(sr.cam64(o["pos"], o["rapidity"]))
-    rays = sum(u.size[0] * u.size[1] for u in us)
-    out = torch.empty(max(rays, 1), dtype=torch.int32, device=f"cuda:{local}")
-    ptr = out.data_ptr()
-
-    def max_over_ranks(x: float) -> float:
-        return shard.max_over_ranks(x, dist, f"cuda:{local}")
-
-    def timed(fn, k):
-        for _ in range(max(1, args.warmup)):
-            fn()
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(k):
-            fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return max_over_ranks(e0.elapsed_time(e1) / k)
-
-    def batch_step():
-        eng.render_batch(0, us, ptr, rays, cams=cams, device_output=True)
-
-    def plain_step():
-        off = 0
-        for u in us:
-            eng.render_into(0, u, ptr + 4 * off, path=sr.SR_PATH_PLAIN)
-            off += u.size[0] * u.size[1]
-
-    with torch.cuda.stream(stream):
-        if not args.no_autotune:
-            eng.autotune(0, us[0], 2)
-        with ClockSampler(local) as clocks:
-            ms = timed(batch_step, args.steps)
-        plain_ms = timed(plain_step, max(2, args.steps // 2))
-        ph = eng.render_batch(0, us, ptr, rays, cams=cams, device_output=True, phases=True)
-        tuning = eng.tuning(0)
-    total = rays
+    with ClockSampler(local) as clocks:
+        if fn == "config4":
+            res = config4_measure(args, rank, world, local, dist, stream, eng, 0)
+        else:
+            res = config5_measure(args, local, stream, eng, 0) if rank == 0 else None
     if dist is not None:
-        t = torch.tensor([rays], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t)
-        total = int(t.item())
         dist.barrier()
         dist.destroy_process_group()
-    if rank != 0:
-        eng.close()
-        return
-    clk = clocks.summary()
-    value = total / (ms / 1e3) / 1e6
-    plain_value = total / (plain_ms / 1e3) / 1e6
-    sizes = {}
-    for o in draws:
-        key = f"{o['width']}x{o['height']}"
-        sizes[key] = sizes.get(key, 0) + 1
-    line = {
-        "metric": "Mrays/s on 1 B200, 64 observers of the 147k-tet cube scene in one batch; primary rays",
-        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded observers over the cube scene)",
-        "config": {"workload": f"{scene.num_prims} tets, 64 observers (sizes {sizes}), past light cone "
-                               "and God's-eye slice 50/50, FP64 cameras",
-                   "rays_per_step": total, "seed": args.seed,
-                   "l2": "scene L2-resident (%.1f MB on the device); every step renders 64 frames" %
-                         (eng.stats(0).device_bytes / 1e6),
-                   "tuning": {k: (list(getattr(tuning, k)) if k == "reserved" else getattr(tuning, k))
-                              for k, _ in tuning._fields_}},
-        "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms,
-                  "speedup_batched_over_plain": value / plain_value},
-        "phases_ms": {"trace": ph.trace_ms, "shade": ph.shade_ms, "stars": ph.stars_ms, "bloom": ph.bloom_ms},
-        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
-    }
-    print(json.dumps(line), flush=True)
     eng.close()
-
-
-def run_config5(args, rank, world, local):
-    """100k inertial stars on a sphere of radius 1e3 over the cube scene, 1280x800, target
-    rendered at rapidity (0.8, -0.3, 0.5). Times, with CUDA events on the engine's stream: one forward
-    frame on the fast path (FP64 camera, binned stars) and one loss-and-gradient evaluation
-    (sr_adjoint: the forward frame recomputed, then the 7-vector of rapidity and event derivatives in
-    f32 with f64 sums) at loss level 0 (full resolution) and level 3, from rapidity 0. One GPU."""
-    import torch
-    import specrel_b200 as sr
     if rank != 0:
         return
-    torch.cuda.set_device(local)
-    scene = sr.synth_scene(5, args.seed)
-    eng = sr.Engine(local)
-    eng.upload(0, scene)
-    stream = torch.cuda.Stream()
-    eng.set_stream(stream.cuda_stream)
-    star = (0.8, -0.3, 0.5)
-    u = sr.uniforms(sr.camera(), W, H, 0, 1, 0, num_nodes=scene.num_nodes, num_stars=scene.num_stars,
-                    light_pos=scene.light_pos)
-    ev = (0.0, 0.0, 0.0, 0.0)
-    out = torch.empty(W * H, dtype=torch.int32, device=f"cuda:{local}")
-    with torch.cuda.stream(stream):
-        tgt = eng.render(0, u, path=sr.SR_PATH_FAST, hdr=True, cam=sr.cam64(ev, star)).hdr
-        tdev = torch.tensor(tgt, device=f"cuda:{local}").contiguous()
-        cam0 = sr.cam64(ev, (0.0, 0.0, 0.0))
-
-        def timed(fn, k):
-            for _ in range(max(1, args.warmup)):
-                fn()
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(k):
-                fn()
-            e1.record(stream)
-            torch.cuda.synchronize()
-            return e0.elapsed_time(e1) / k
-
-        with ClockSampler(local) as clocks:
-            fwd = timed(lambda: eng.render_into(0, u, out.data_ptr(), path=sr.SR_PATH_FAST, cam=cam0), args.steps)
-            g0 = timed(lambda: eng.adjoint(0, u, cam0, tdev.data_ptr(), 0), args.steps)
-            g3 = timed(lambda: eng.adjoint(0, u, cam0, tdev.data_ptr(), 3), args.steps)
-        r = eng.adjoint(0, u, cam0, tdev.data_ptr(), 0)
     clk = clocks.summary()
-    line = {
-        "metric": "ms per image-loss gradient on 1 B200, 100k stars over the cube scene, 1280x800",
-        "value": g0, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": g0,
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 sums)",
-        "data": "synthetic (seeded stars and occluders)",
-        "config": {"workload": f"{scene.num_prims} tets, {scene.num_stars} stars, 1280x800, target at "
-                               "rapidity (0.8, -0.3, 0.5), gradient at rapidity 0", "seed": args.seed},
-        "forward_frame_ms": fwd, "gradient_level3_ms": g3,
-        "gradient": {"loss": r.loss, "grad": list(r.grad), "star_terms": r.star_terms},
-        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
-    }
+    ms = res.pop("ms_per_step", res["value"])  # config5's value is itself a time
+    line = {"metric": res.pop("metric"), "value": res.pop("value"), "unit": res.pop("unit"), "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": res.pop("higher_is_better", True), "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded)", "config": {"workload": res.pop("workload"), "seed": args.seed},
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}}
+    line.update(res)
     print(json.dumps(line), flush=True)
-    eng.close()
 
 
 def main():
@@ -549,10 +644,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
-    elif args.workload == "config4":
-        run_config4(args, rank, world, local)
-    elif args.workload == "config5":
-        run_config5(args, rank, world, local)
+    elif args.workload in ("config4", "config5"):
+        _standalone(args, rank, world, local, args.workload)
     else:
         run_engine(args, rank, world, local)
 

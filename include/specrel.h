@@ -419,13 +419,15 @@ sr_status sr_adjoint_rows(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* 
  * and its bloom pyramid) is one static device array of SR_NOALLOC_SCRATCH_BYTES that every GPU
  * which loads this library holds until the process exits.
  * - Frames above SR_NOALLOC_MAX_PIXELS pixels (e.g. 512x512 or 640x400 fit) are rejected with
- *   SR_ERR_INVALID_ARGUMENT.
- * - The first call on a device looks up the array's device address; make that first call before
- *   any stream capture.
+ *   SR_ERR_INVALID_ARGUMENT; that is the only size rule (the scratch holds the bloom pyramid of
+ *   every frame within it, one-row frames included).
+ * - Every call looks up the array's device address on the current device (cudaGetSymbolAddress; the
+ *   first call on a device also loads the library's device code there, if that has not happened).
  * - Every call uses the same array and leaves its contents behind (the counters are cleared at the
  *   start of each call). Calls that overlap on one GPU, from other streams or contexts of the
  *   process, race on it.
- * - The call waits for its frame (it reads the error flags back) and returns its status. */
+ * - The call waits for its frame (it copies the error flags back to the host and synchronizes the
+ *   context's stream), so it cannot be called while that stream is being captured into a graph. */
 #define SR_NOALLOC_SCRATCH_BYTES (8u << 20)
 #define SR_NOALLOC_MAX_PIXELS (1u << 18)
 sr_status sr_render_noalloc(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, const SrCameraF64* cam64,
@@ -442,7 +444,12 @@ typedef struct SrTuning {
     uint32_t leaf_batch;      /* lanes on a leaf before the warp tests leaves: 1..32 */
     uint32_t home_pct;        /* share of the tiles (0..100) split into one band per SM, which the
                                  warps on that SM take first; the rest go in frame order */
-    uint32_t reserved[3];     /* 0 */
+    uint32_t stack_smem;      /* traversal-stack entries per thread kept in shared memory, 0..64
+                                 (0: the whole stack in local memory); deeper entries go to local
+                                 memory, so the visiting order does not depend on it */
+    uint32_t top_levels;      /* levels of the wide tree staged in shared memory per block, 0..10
+                                 (0: none) */
+    uint32_t reserved;        /* 0 */
 } SrTuning;
 sr_status sr_get_tuning(const sr_ctx* ctx, uint32_t scene_idx, SrTuning* out);
 sr_status sr_set_tuning(sr_ctx* ctx, uint32_t scene_idx, const SrTuning* t);

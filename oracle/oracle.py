@@ -97,7 +97,7 @@ def lib():
         L.orc_gamma_lut.argtypes = [C.c_void_p]
         L.orc_bloom_pack.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
         L.orc_frozen_new.restype = C.c_void_p
-        L.orc_frozen_new.argtypes = [C.c_void_p, C.POINTER(Camera), C.POINTER(Config), C.c_int]
+        L.orc_frozen_new.argtypes = [C.c_void_p, C.POINTER(Camera), C.POINTER(Config), C.c_int, C.c_int]
         L.orc_frozen_free.argtypes = [C.c_void_p]
         L.orc_frozen_loss.restype = C.c_double
         L.orc_frozen_loss.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Camera), C.POINTER(Config), C.c_void_p,
@@ -340,9 +340,12 @@ class Frozen:
     stars passing the footprint cut), for evaluating the image loss at nearby observers with them
     held fixed: the FP64 reference for the engine's gradient (shaded, past light cone)."""
 
-    def __init__(self, scene: Scene, camera: Camera, cfg: Config, threads: int = 0):
+    def __init__(self, scene: Scene, camera: Camera, cfg: Config, threads: int = 0, binning: int = -1):
+        """`binning`: find each pixel's candidate stars by projecting the stars (-1: on star sets
+        above 4096, 0: never, 1: always); the recorded outcomes are the same either way."""
         self.scene, self.cfg = scene, cfg
-        self.h = lib().orc_frozen_new(scene.h, C.byref(camera), C.byref(cfg), threads or (os.cpu_count() or 1))
+        self.h = lib().orc_frozen_new(scene.h, C.byref(camera), C.byref(cfg), threads or (os.cpu_count() or 1),
+                                      binning)
         self._free = lib().orc_frozen_free
         if not self.h:
             raise RuntimeError("orc_frozen_new: only shaded past-light-cone frames")

@@ -407,7 +407,9 @@ double frozen_loss_t(const Scene<T>& scene, const FrozenFrame<T>& F, const OrcCa
 extern "C" {
 
 // Records the discrete outcomes of the frame (shaded, past light cone, no flashes or haze).
-void* orc_frozen_new(void* s, const OrcCamera* c, const OrcConfig* cf, int threads) {
+// `binning`: candidate stars per pixel found by projecting each star (-1: on large star sets,
+// 0: never, 1: always); the outcomes are the same either way.
+void* orc_frozen_new(void* s, const OrcCamera* c, const OrcConfig* cf, int threads, int binning) {
     auto* b = (SceneBox*)s;
     if (!cf || cf->mode != 0 || cf->slice_mode != 0 || cf->width == 0 || cf->height == 0) return nullptr;
     auto* fb = new FrozenBox();
@@ -418,12 +420,12 @@ void* orc_frozen_new(void* s, const OrcCamera* c, const OrcConfig* cf, int threa
         Camera4D<double> cam = camera_of<double>(c);
         FrameDynamics<double> dyn;
         Renderer<double> R{b->d->scene, cam, cfg, dyn};
-        fb->d = freeze(R, th);
+        fb->d = freeze(R, th, binning);
     } else {
         Camera4D<float> cam = camera_of<float>(c);
         FrameDynamics<float> dyn;
         Renderer<float> R{b->f->scene, cam, cfg, dyn};
-        fb->f = freeze(R, th);
+        fb->f = freeze(R, th, binning);
     }
     return fb;
 }

@@ -79,7 +79,9 @@ template <class T> inline bool sky_grid(const V4<T>& d) {
     return !(a.x == b.x && a.y == b.y && a.z == b.z);
 }
 
-template <class T> FrozenFrame<T> freeze(const Renderer<T>& R, unsigned threads) {
+// `binning`: -1 bins the stars per pixel on star sets above 4096, 0 never, 1 always (the tests
+// check that both give the same outcomes).
+template <class T> FrozenFrame<T> freeze(const Renderer<T>& R, unsigned threads, int binning = -1) {
     FrozenFrame<T> F;
     F.w = R.cfg.width;
     F.h = R.cfg.height;
@@ -89,6 +91,35 @@ template <class T> FrozenFrame<T> freeze(const Renderer<T>& R, unsigned threads)
     std::vector<char> ok(stars.size());
     std::vector<V4<T>> sd(stars.size()), su(stars.size());
     for (size_t i = 0; i < stars.size(); ++i) ok[i] = worldline_cone_event(stars[i], fr.ray_origin, fr.e0, fr.cone, &sd[i], &su[i]);
+    // Candidate stars per pixel, in increasing star order. A star passes a pixel's footprint cut
+    // only when the angle theta between its direction and the pixel's ray has tan(theta) < 2.4 *
+    // spread <= 2.4 * pixel pitch * c^1.5 (c: cosine of the pixel's view angle). On the image
+    // plane, where the pixel pitch is one pixel, that angle spans at most 2.4 / sqrt(c) pixels
+    // (radial magnification 1 / c^2), so a star is listed at the pixels within a radius of
+    // 1.25 * 2.4 / sqrt(c_min) + 2 pixels of where its direction projects; the exact test below
+    // decides, as in the full loop over all stars, which it replaces on large star sets.
+    std::vector<std::vector<uint32_t>> cand;
+    const bool binned = fr.draw_stars && (binning > 0 || (binning < 0 && stars.size() > 4096));
+    if (binned) {
+        cand.resize(F.w * F.h);
+        const double hw = (double)fr.half_w, hh = (double)fr.half_h;
+        const double c_min = 1.0 / std::sqrt(1.0 + hw * hw + hh * hh);
+        const int rad = (int)std::ceil(1.25 * 2.4 / std::sqrt(c_min)) + 2;
+        const Tetrad<T>& tet = R.camera.tetrad;
+        for (size_t i = 0; i < stars.size(); ++i) {
+            if (!ok[i]) continue;
+            T tau = -sd[i].mdot(fr.e0);
+            V4<T> r = sd[i] + fr.e0 * (-tau);
+            double x = (double)r.mdot(tet.e[1]), y = (double)r.mdot(tet.e[2]), z = (double)r.mdot(tet.e[3]);
+            double len = std::sqrt(x * x + y * y + z * z);
+            if (!(z > 0.25 * len)) continue;  // beyond 75 degrees of the axis: outside every view cone here
+            double px = (x / z / hw + 1.0) * 0.5 * (double)F.w - 0.5, py = (1.0 - y / z / hh) * 0.5 * (double)F.h - 0.5;
+            long x0 = std::max<long>(0, (long)std::floor(px) - rad), x1 = std::min<long>((long)F.w - 1, (long)std::ceil(px) + rad);
+            long y0 = std::max<long>(0, (long)std::floor(py) - rad), y1 = std::min<long>((long)F.h - 1, (long)std::ceil(py) + rad);
+            for (long yy = y0; yy <= y1; ++yy)
+                for (long xx = x0; xx <= x1; ++xx) cand[(size_t)yy * F.w + (size_t)xx].push_back((uint32_t)i);
+        }
+    }
     std::atomic<size_t> next{0};
     auto work = [&] {
         for (;;) {
@@ -121,7 +152,10 @@ template <class T> FrozenFrame<T> freeze(const Renderer<T>& R, unsigned threads)
                 T inv_len = T(1) / m_sqrt(sx * sx + sy * sy + T(1));
                 T spread = fr.pixel_pitch * inv_len * m_sqrt(inv_len);
                 V4<T> n = d - fr.e0 * fr.cone;
-                for (size_t i = 0; i < stars.size(); ++i) {
+                const std::vector<uint32_t>* list = binned ? &cand[py * F.w + px] : nullptr;
+                const size_t m = binned ? list->size() : stars.size();
+                for (size_t j = 0; j < m; ++j) {
+                    const size_t i = binned ? (*list)[j] : j;
                     if (!ok[i]) continue;
                     T tau = -sd[i].mdot(fr.e0);
                     V4<T> r = sd[i] + fr.e0 * (-tau);

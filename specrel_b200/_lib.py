@@ -132,7 +132,8 @@ class Tuning(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("tile_w", C.c_uint32),
                 ("tile_h", C.c_uint32), ("chunk_tiles", C.c_uint32), ("refill_lanes", C.c_uint32),
                 ("leaf_coop", C.c_uint32), ("leaf_batch", C.c_uint32),
-                ("home_pct", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("home_pct", C.c_uint32), ("stack_smem", C.c_uint32), ("top_levels", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class SynthParams(C.Structure):

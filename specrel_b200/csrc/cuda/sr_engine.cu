@@ -9,7 +9,6 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -766,12 +765,15 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
     float win_ms = INFINITY;
     // The schedules worth timing: whole-warp refills of single tiles were fastest on every scene
     // measured (wider chunks or partial refills spread the rays in flight over more of the tree).
+    // Per block shape and tile: cooperative leaf tests, or the lean kernel with the traversal
+    // stack in local memory or its first 8..16 entries in shared memory.
     const uint32_t shapes[][2] = {{128, 8}, {128, 11}, {256, 4}, {256, 6}, {512, 3}};
     const uint32_t tiles[][2] = {{8, 4}, {4, 8}};
+    const uint32_t stacks[] = {0, 8, 10, 12, 16};
     std::vector<SrTuning> cand;
     for (auto& sh : shapes)
         for (auto& tl : tiles)
-            for (uint32_t coop = 0; coop <= 1; ++coop) {
+            for (uint32_t v = 0; v <= sizeof(stacks) / sizeof(stacks[0]); ++v) {
                 SrTuning t = keep;
                 t.block_threads = sh[0];
                 t.blocks_per_sm = sh[1];
@@ -779,9 +781,11 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
                 t.tile_h = tl[1];
                 t.chunk_tiles = 1;
                 t.refill_lanes = 32;
-                t.leaf_coop = coop;
+                t.leaf_coop = v == 0 ? 1u : 0u;
                 t.leaf_batch = 1;
                 t.home_pct = 0;
+                t.stack_smem = v == 0 ? 0u : stacks[v - 1];
+                t.top_levels = 0;
                 if (fast_tuning_valid(ctx->fast, t)) cand.push_back(t);
             }
     for (const SrTuning& t : cand) {
@@ -866,24 +870,32 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[SR_NOALLOC_SCRA
 namespace {
 
 constexpr size_t NOALLOC_COUNTERS = 0, NOALLOC_CAM = 256, NOALLOC_HDR = 512;
-constexpr int NOALLOC_MAX_DEVICES = 64;
 
-std::mutex g_noalloc_mu;
-void* g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
-
-// The device address of g_noalloc_scratch on `device`, which must be current. In host code the
-// array's name only identifies the symbol; its address on each device comes from
-// cudaGetSymbolAddress, looked up once per device and kept.
-cudaError_t noalloc_base(int device, unsigned char** out) {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (device < 0 || device >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
-    if (!g_noalloc_base[device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_noalloc_base[device] = p;
+// Float4 entries of the HDR image and its bloom levels for a w x h frame (each level halves both
+// sides, rounding up).
+constexpr uint64_t noalloc_pyramid_len(uint64_t w, uint64_t h) {
+    uint64_t n = 0;
+    for (int k = 0; k <= SR_BLOOM_LEVELS; ++k) {
+        n += w * h;
+        w = (w + 1) / 2;
+        h = (h + 1) / 2;
     }
-    *out = static_cast<unsigned char*>(g_noalloc_base[device]);
+    return n;
+}
+// The largest pyramid of a frame within SR_NOALLOC_MAX_PIXELS is the one-row (or one-column) frame
+// of all of them: its levels shrink by 2 instead of 4.
+static_assert(NOALLOC_HDR + noalloc_pyramid_len(SR_NOALLOC_MAX_PIXELS, 1) * 16 <= SR_NOALLOC_SCRATCH_BYTES,
+              "the no-allocation scratch holds the pyramid of every frame within the pixel limit");
+
+// The device address of g_noalloc_scratch on the current device. In host code the array's name only
+// identifies the symbol; its address comes from cudaGetSymbolAddress, looked up on every call (a
+// host-side table lookup once the module is loaded), so no address outlives the context it came
+// from (a cudaDeviceReset by the application between calls included).
+cudaError_t noalloc_base(unsigned char** out) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    *out = static_cast<unsigned char*>(p);
     return cudaSuccess;
 }
 
@@ -903,11 +915,12 @@ sr_status sr_render_noalloc(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, c
     if (u->mode > 3 || u->shadow_mode > 2 || u->slice_mode > 3 || u->num_flashes > SR_MAX_FLASHES || u->num_haze > SR_MAX_HAZE_ORIGINS)
         return fail(ctx, SR_ERR_INVALID_ARGUMENT, "uniform block out of range");
     const Pyramid pyr = make_pyramid(u->size[0], u->size[1]);
+    // Defensive: the static_assert above shows every frame within the pixel limit fits.
     if (NOALLOC_HDR + (size_t)pyr.off[SR_BLOOM_LEVELS + 1] * sizeof(float4) > SR_NOALLOC_SCRATCH_BYTES)
         return fail(ctx, SR_ERR_INVALID_ARGUMENT, "frame's bloom pyramid exceeds the no-allocation scratch");
     CK(cudaSetDevice(ctx->device), "set device");
     unsigned char* base = nullptr;
-    CK(noalloc_base(ctx->device, &base), "no-allocation scratch address");
+    CK(noalloc_base(&base), "no-allocation scratch address");
     SceneSlot& s = *ctx->scenes[idx];
     FrameDev f{};
     f.hdr = reinterpret_cast<float4*>(base + NOALLOC_HDR);

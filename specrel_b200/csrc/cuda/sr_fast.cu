@@ -62,10 +62,18 @@ __global__ void k_wide_fill(const SrGpuNode* nodes, uint32_t n, const uint32_t* 
     refs[wid[i]] = make_uint2(ref[0], ref[1]);
 }
 
+static cudaError_t lean_kernel_attrs(int max_smem);
+bool lean_stack_supported(uint32_t s);
+
+// Dynamic shared memory of the lean kernel: S + 1 stack words per thread (S of them used).
+static size_t lean_stack_bytes(const SrTuning& t) {
+    return t.stack_smem ? (size_t)t.block_threads * (t.stack_smem + 1) * sizeof(uint2) : 0;
+}
+
 cudaError_t fast_init(FastCtx& c, const cudaDeviceProp& prop) {
     c.num_sms = prop.multiProcessorCount;
     c.max_smem = (int)prop.sharedMemPerBlockOptin;
-    return cudaSuccess;
+    return lean_kernel_attrs(c.max_smem);
 }
 
 void fast_release(FastCtx& c) {
@@ -143,12 +151,13 @@ SrTuning fast_default_tuning(const FastCtx& c) {
 }
 
 bool fast_tuning_valid(const FastCtx& c, const SrTuning& t) {
-    (void)c;
     bool bt = t.block_threads == 64 || t.block_threads == 128 || t.block_threads == 256 || t.block_threads == 512;
+    const size_t stack_bytes = lean_stack_bytes(t);
     return bt && t.blocks_per_sm >= 1 && t.blocks_per_sm <= 16 && t.tile_w >= 1 && t.tile_w * t.tile_h == 32 &&
            t.chunk_tiles >= 1 && t.chunk_tiles <= 64 && t.refill_lanes >= 1 && t.refill_lanes <= 32 &&
            t.leaf_coop <= 1 && t.leaf_batch >= 1 && t.leaf_batch <= 32 && t.home_pct <= 100 &&
-           t.reserved[0] == 0 && t.reserved[1] == 0 && t.reserved[2] == 0;
+           lean_stack_supported(t.stack_smem) && stack_bytes <= (size_t)c.max_smem && t.top_levels == 0 &&
+           t.reserved == 0;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -586,11 +595,18 @@ __device__ __forceinline__ uint32_t next_tile(const TraceBatchArgs& a, uint32_t 
     return ~0u;
 }
 
-template <bool COUNT>
+// SS > 0: the first SS entries of each thread's traversal stack live in dynamic shared memory
+// (SplitStack), the rest in local memory; SS == 0: all in local memory (LocalStack).
+template <bool COUNT, int SS>
 __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
     const uint32_t lane = threadIdx.x & 31u;
     Work wp{0, 0, 0}, wsh{0, 0, 0};
-    uint2 st[FAST_STACK];
+    uint2 lm[FAST_STACK];
+    extern __shared__ uint2 sm_stack[];
+    using Stack = typename std::conditional<(SS > 0), SplitStack<SS>, LocalStack>::type;
+    Stack st;
+    if constexpr (SS > 0) st = SplitStack<SS>{sm_stack + threadIdx.x * SplitStack<SS>::ROW, lm};
+    else st = LocalStack{lm};
     const uint32_t home = a.num_bands ? sm_id() % a.num_bands : 0u;
     uint32_t stage = a.num_bands ? 0u : 1u, steal = 0;
     for (;;) {
@@ -647,6 +663,41 @@ __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
         add_work(a.work, wp);
         add_work(a.work + 3, wsh);
     }
+}
+
+// The shared-memory stack depths the lean kernel is built for (SrTuning.stack_smem).
+#define SR_LEAN_STACKS(X) X(0) X(8) X(10) X(12) X(16)
+
+bool lean_stack_supported(uint32_t s) {
+#define SR_ONE(S) if (s == (S)) return true;
+    SR_LEAN_STACKS(SR_ONE)
+#undef SR_ONE
+    return false;
+}
+
+// The shared-memory stack of the lean kernel can exceed the 48 KB default of one block.
+static cudaError_t lean_kernel_attrs(int max_smem) {
+    cudaError_t e = cudaSuccess;
+#define SR_ONE(S)                                                                                                  \
+    if (e == cudaSuccess && (S) > 0)                                                                               \
+        e = cudaFuncSetAttribute(k_trace_lean<false, (S)>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem); \
+    if (e == cudaSuccess && (S) > 0)                                                                               \
+        e = cudaFuncSetAttribute(k_trace_lean<true, (S)>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+    SR_LEAN_STACKS(SR_ONE)
+#undef SR_ONE
+    return e;
+}
+
+static void launch_lean(uint32_t ss, bool count, uint32_t blocks, uint32_t threads, size_t smem, cudaStream_t st,
+                        const TraceBatchArgs& ta) {
+#define SR_ONE(S)                                                                         \
+    if (ss == (S)) {                                                                      \
+        if (count) k_trace_lean<true, (S)><<<blocks, threads, smem, st>>>(ta);           \
+        else k_trace_lean<false, (S)><<<blocks, threads, smem, st>>>(ta);                \
+        return;                                                                           \
+    }
+    SR_LEAN_STACKS(SR_ONE)
+#undef SR_ONE
 }
 
 struct ShadeBatchArgs {
@@ -922,8 +973,8 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
         const size_t smem = t.leaf_coop ? (size_t)(t.block_threads / 32) * COOP_SMEM_PER_WARP : 0;
         const bool lean = !t.leaf_coop && t.leaf_batch == 1 && t.refill_lanes == 32 && t.chunk_tiles == 1;
         if (lean) {
-            if (r.count_work) k_trace_lean<true><<<blocks, t.block_threads, 0, st>>>(ta);
-            else k_trace_lean<false><<<blocks, t.block_threads, 0, st>>>(ta);
+            const size_t ssm = lean_stack_bytes(t);
+            launch_lean(t.stack_smem, r.count_work, blocks, t.block_threads, ssm, st, ta);
         } else if (t.leaf_coop) {
             if (r.count_work) k_trace_batch<true, true><<<blocks, t.block_threads, smem, st>>>(ta);
             else k_trace_batch<false, true><<<blocks, t.block_threads, smem, st>>>(ta);

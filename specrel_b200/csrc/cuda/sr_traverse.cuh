@@ -289,6 +289,36 @@ __device__ __forceinline__ const float4* octant_boxes(const WideScene& s, float4
     return s.boxes + oct * s.oct_stride;
 }
 
+// The traversal stack of one thread for the lean forms (one 8-byte word per entry: reference,
+// entry-parameter bits). LocalStack keeps every entry in local memory. SplitStack<S> keeps entries
+// [0, S) in shared memory, thread t's in a row of S + 1 words at sm + t * (S + 1) (an odd row
+// length: when the lanes of a half-warp stand at the same depth, their 8-byte words fall in
+// distinct banks), and entries from S on in local memory. The traversal pushes and pops the same
+// entries either way.
+struct LocalStack {
+    uint2* lm;  // FAST_STACK entries
+    __device__ __forceinline__ void put(int i, uint2 e) const { lm[i] = e; }
+    __device__ __forceinline__ uint2 get(int i) const { return lm[i]; }
+    __device__ __forceinline__ void put_ref(int i, uint32_t r) const { lm[i].x = r; }
+    __device__ __forceinline__ uint32_t get_ref(int i) const { return lm[i].x; }
+};
+template <int S>
+struct SplitStack {
+    static constexpr int ROW = S + 1;  // words per thread in shared memory (S used)
+    uint2* sm;                         // this thread's row in shared memory
+    uint2* lm;                         // FAST_STACK entries in local memory (entries below S unused)
+    __device__ __forceinline__ void put(int i, uint2 e) const {
+        if (i < S) sm[i] = e;
+        else lm[i] = e;
+    }
+    __device__ __forceinline__ uint2 get(int i) const { return i < S ? sm[i] : lm[i]; }
+    __device__ __forceinline__ void put_ref(int i, uint32_t r) const {
+        if (i < S) sm[i].x = r;
+        else lm[i].x = r;
+    }
+    __device__ __forceinline__ uint32_t get_ref(int i) const { return i < S ? sm[i].x : lm[i].x; }
+};
+
 // Closest hit from node `cur` (the root, already tested against the ray). Returns the slot or
 // -1; `t_max` ends as the closest hit's parameter.
 //
@@ -297,9 +327,9 @@ __device__ __forceinline__ const float4* octant_boxes(const WideScene& s, float4
 // the longest leaf of the warp. A leaf in progress is its packed reference with the tested
 // primitives taken off the front. Each ray's own sequence of node visits and tests, and so its
 // result, is the same.
-template <bool COUNT>
+template <bool COUNT, class Stack>
 __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, float4 no, float4 d, float4 inv, float t_min,
-                                            float& t_max, GeomHit& best, uint2* st, uint32_t* err, Work& work) {
+                                            float& t_max, GeomHit& best, const Stack& st, uint32_t* err, Work& work) {
     const float4* ob = octant_boxes(s, inv);
     int slot = -1, sp = 0;
     uint32_t visits = 0;
@@ -339,7 +369,7 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
             const bool hr = exr >= enr;
             if (hl && hr) {
                 const bool ln = enl <= enr;
-                if (sp < FAST_STACK) st[sp++] = ln ? make_uint2(r.y, __float_as_uint(enr)) : make_uint2(r.x, __float_as_uint(enl));
+                if (sp < FAST_STACK) st.put(sp++, ln ? make_uint2(r.y, __float_as_uint(enr)) : make_uint2(r.x, __float_as_uint(enl)));
                 else atomicOr(err, ERR_BAD_INDEX);
                 cur = ln ? r.x : r.y;
                 if (COUNT && (cur & REF_LEAF)) ++work.leaves;
@@ -353,7 +383,7 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
         }
         bool found = false;
         while (sp > 0) {
-            const uint2 e = st[--sp];
+            const uint2 e = st.get(--sp);
             if (__uint_as_float(e.y) < t_max) {
                 cur = e.x;
                 if (COUNT && (cur & REF_LEAF)) ++work.leaves;
@@ -369,9 +399,9 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
 // Any hit in (t_min, t_max) from node `cur` (the root, already tested): left before right, no
 // culling (Bvh4D::is_occluded, bvh4d.rs:523-578). (The answer does not depend on the order;
 // nearer-first measured 7% slower on the 7.9M-tet scene.)
-template <bool COUNT>
+template <bool COUNT, class Stack>
 __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float4 no, float4 d, float4 inv, float t_min,
-                                         float t_max, uint2* st, uint32_t* err, Work& work) {
+                                         float t_max, const Stack& st, uint32_t* err, Work& work) {
     const float4* ob = octant_boxes(s, inv);
     int sp = 0;
     uint32_t visits = 0;
@@ -397,7 +427,7 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
             slab_octant(rnear, rfar, no, inv, t_min, t_max, &enr, &exr);
             const bool hl = exl >= enl, hr = exr >= enr;
             if (hl && hr) {
-                if (sp < FAST_STACK) st[sp++].x = r.y;
+                if (sp < FAST_STACK) st.put_ref(sp++, r.y);
                 else atomicOr(err, ERR_BAD_INDEX);
                 cur = r.x;
                 if (COUNT && (cur & REF_LEAF)) ++work.leaves;
@@ -410,7 +440,7 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
             }
         }
         if (sp == 0) return false;
-        cur = st[--sp].x;
+        cur = st.get_ref(--sp);
         if (COUNT && (cur & REF_LEAF)) ++work.leaves;
     }
 }

@@ -95,9 +95,47 @@ def test_every_schedule_gives_the_same_frames(engine, scene, tiling):
         off += n
 
 
+@pytest.mark.parametrize("stack,threads,blocks", [(8, 128, 11), (10, 128, 9), (12, 128, 9), (16, 256, 4),
+                                                   (12, 512, 3)])
+def test_shared_memory_stack_gives_the_same_frames_and_visits(engine, scene, stack, threads, blocks):
+    """The lean kernel with the first `stack` traversal-stack entries of each thread in shared
+    memory and the rest in local memory (8 entries: many rays go deeper, so both parts are used)
+    gives the plain path's frames, and visits exactly the nodes of the oracle's Bvh4D::trace."""
+    keep = engine.tuning(3)
+    t = engine.tuning(3)
+    t.tile_w, t.tile_h, t.chunk_tiles, t.refill_lanes, t.leaf_coop, t.leaf_batch, t.home_pct = 4, 8, 1, 32, 0, 1, 0
+    t.block_threads, t.blocks_per_sm, t.stack_smem = threads, blocks, stack
+    engine.set_tuning(3, t)
+    try:
+        obs, us, cams = _observers(14, 4, int(scene.info.n_nodes), scale=4)
+        out = _batch(engine, 3, us, cams)
+        cam = sr.camera((0.0, 0.0, 0.0, -10.0), 90.0, rapidity=(0.3, 0.1, -0.2))
+        u = sr.uniforms(cam, 256, 160, 0, 0, 0, num_nodes=int(scene.info.n_nodes))
+        fr = engine.render(3, u, count=True)
+    finally:
+        engine.set_tuning(3, keep)
+    off = 0
+    for u_, c in zip(us, cams):
+        n = u_.size[0] * u_.size[1]
+        assert (out[off:off + n] == engine.render(3, u_, path=sr.SR_PATH_PLAIN, cam=c).rgb).all()
+        off += n
+    base = O.render(scene, O.make_camera(pos=(0.0, 0.0, 0.0, -10.0), rapidity=(0.3, 0.1, -0.2)),
+                    O.make_config(256, 160), stats=True)
+    assert fr.timings.nodes_visited == int(base.stats[:, 0].sum())
+    assert fr.timings.tets_tested == int(base.stats[:, 2].sum())
+
+
 def test_invalid_tuning_rejected(engine, scene):
     t = engine.tuning(3)
     t.refill_lanes = 0
+    with pytest.raises(sr.SrError):
+        engine.set_tuning(3, t)
+    t = engine.tuning(3)
+    t.stack_smem = 9  # not one of the built depths
+    with pytest.raises(sr.SrError):
+        engine.set_tuning(3, t)
+    t = engine.tuning(3)
+    t.reserved = 1
     with pytest.raises(sr.SrError):
         engine.set_tuning(3, t)
 

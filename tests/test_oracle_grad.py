@@ -22,3 +22,17 @@ def test_frozen_frame_reproduces_the_render_and_is_smooth():
     assert np.abs(g4 - g6).max() <= 1e-3 * np.abs(g6).max()
     # A coarser loss level is smaller and still differentiable.
     assert F.loss(cam(th0), tgt, 3) < L0
+
+
+def test_binned_freeze_records_the_same_outcomes():
+    """Large star sets find each pixel's candidate stars by projection instead of testing every star;
+    the frozen image (every star that passed the footprint cut, in the same order) is the same."""
+    s = O.Scene(O.synth_params(5, 3, n_bodies=4, steps=8, n_stars=20000), fp64=True)
+    cfg = O.make_config(200, 125, 0, 1, 0)
+    th0 = np.array([0.3, -0.2, 0.1, 0.0, 0.05, 0.0, -0.02])
+    cam = O.make_camera(pos=tuple(th0[3:]), rapidity=tuple(th0[:3]))
+    tgt = np.zeros((200 * 125, 3))
+    L0, a = O.Frozen(s, cam, cfg, binning=0).loss(cam, tgt, hdr=True)
+    L1, b = O.Frozen(s, cam, cfg, binning=1).loss(cam, tgt, hdr=True)
+    ref = O.render(s, cam, cfg, hdr=True, aux=False).hdr
+    assert (a == ref).all() and (b == ref).all() and L0 == L1

@@ -17,13 +17,15 @@ pytestmark = pytest.mark.gpu
 PATHS = [sr.SR_PATH_PLAIN, sr.SR_PATH_FAST]
 
 
-def _assert_parity(rep, label, near_max=0.02):
+def _assert_parity(rep, label, near_pixels=0):
+    """The parity bar. The near-threshold mask (pixels exempt from the 1/255 check) is held to the
+    pixel count the oracle gives for the case (deterministic; measured on CPU), not to a share."""
     print(label, rep)
     assert rep.hit_match_nongrazing == 1.0, (label, str(rep))
     assert rep.hit_match >= 0.9999, (label, str(rep))
     assert rep.lam_max_rel <= 1e-5 and rep.tau_max_rel <= 1e-5, (label, str(rep))
     assert rep.rgb_max_unmasked <= 1, (label, str(rep))
-    assert rep.near_threshold_frac <= near_max, (label, str(rep))
+    assert round(rep.near_threshold_frac * rep.n) <= near_pixels, (label, str(rep))
     assert rep.frac_gt4 < 0.005, (label, str(rep))
 
 
@@ -59,6 +61,8 @@ def test_config1_320x200_matches_oracle(engine, cubes, path):
 MODES = [  # gpu.rs:1268-1278
     (0, 1, 0), (0, 2, 1), (1, 0, 0), (2, 0, 0), (3, 0, 0), (3, 0, 3), (0, 1, 2), (0, 2, 3), (1, 0, 2),
 ]
+# Pixels of the near-threshold mask per mode case (of 192x120), as the oracle gives them.
+MODE_NEAR = {(0, 1, 2): 1, (1, 0, 2): 1}
 
 
 @pytest.mark.parametrize("mode,shadow,slice_", MODES)
@@ -69,7 +73,8 @@ def test_modes_with_boosted_rotated_observer(engine, cubes, mode, shadow, slice_
     co = O.make_camera(pos=pos, fov_deg=65.0, **kw)
     ce = sr.camera(pos, 65.0, **kw)
     rep, fr, base = _render_both(engine, 0, cubes, co, ce, 192, 120, mode, shadow, slice_, path=path)
-    _assert_parity(rep, f"mode={mode} shadow={shadow} slice={slice_} path={path}", near_max=0.05)
+    _assert_parity(rep, f"mode={mode} shadow={shadow} slice={slice_} path={path}",
+                   near_pixels=MODE_NEAR.get((mode, shadow, slice_), 0))
 
 
 def test_flashes_haze_and_frontier(engine, cubes):
@@ -85,7 +90,7 @@ def test_flashes_haze_and_frontier(engine, cubes):
                                      uargs=dict(frontier=frontier, flashes=flashes, remote_origins=remote))
         # Flash colours reach the kernel premultiplied by intensity (gpu.rs:160-167), one rounding
         # away from the CPU's product; that can move a pixel by one level.
-        _assert_parity(rep, f"dynamics mode={mode} slice={slice_}", near_max=0.05)
+        _assert_parity(rep, f"dynamics mode={mode} slice={slice_}")
 
 
 @pytest.mark.parametrize("path", PATHS)
@@ -109,7 +114,7 @@ def test_stars_reduced(engine):
     for path in PATHS:
         rep, fr, base = _render_both(engine, 2, s, O.make_camera(rapidity=rap), sr.camera(rapidity=rap), 256, 160,
                                      path=path)
-        _assert_parity(rep, f"stars path={path}", near_max=0.05)
+        _assert_parity(rep, f"stars path={path}")
 
 
 def test_host_render_entry_point_equals_render_ex(engine, cubes):
