@@ -377,6 +377,31 @@ sr_status sr_render_batch(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* 
                           uint32_t n_observers, uint32_t* rgb_out, uint64_t rgb_len, uint32_t flags,
                           SrTimings* timings);
 
+/* ---- Ray queries ---------------------------------------------------------------------------
+ * Bvh4D::trace (bvh4d.rs:445-520) followed by Simplex4D::interpolate_hit (mesh4d.rs:382-425) for
+ * caller rays: the query the reference's scene probes (scene.rs:785-1053), picking and aiming make
+ * on the host, here on the device with the reference's traversal order. Ray i starts at event
+ * `origin` (double; rebased to the scene's FP64 anchor in double, then rounded to f32, so with no
+ * anchor it is the f32 origin) and runs along `dir` over (t_min, t_max). `hits` receives, per ray,
+ * the hit simplex (the caller's index through leaf_to_orig, else the leaf slot; 0xFFFFFFFF on a
+ * miss), its parameter lambda, the interpolated proper time, the event (the anchor added back in
+ * double), the tetrahedron barycentrics, the uv and the material. Host buffers; blocking. */
+typedef struct SrRay {
+    double origin[4];  /* (t, x, y, z) */
+    float dir[4];
+    float t_min, t_max;
+} SrRay;
+typedef struct SrRayHit {
+    uint32_t id;    /* the hit simplex in the caller's order, or 0xFFFFFFFF */
+    uint32_t slot;  /* its leaf slot, or 0xFFFFFFFF */
+    float lambda, proper_time;
+    double event[4];
+    float tet_bary[4];
+    float uv[2];
+    uint32_t material, pad;
+} SrRayHit;
+sr_status sr_trace_rays(sr_ctx* ctx, uint32_t scene_idx, const SrRay* rays, uint32_t n, SrRayHit* hits);
+
 /* ---- Gradient with respect to the observer ------------------------------------------------
  * New (the reference renders forward only). For one observer on the past light cone (mode 0,
  * slice mode 0, no flashes, no haze) on the fast path:
@@ -472,6 +497,7 @@ static_assert(sizeof(SrArenaPart) == 16 && sizeof(SrArenaStats) == 48, "arena st
 static_assert(sizeof(SrGpuMaterial) == 48, "GpuMaterial is 48 bytes (gpu.rs:96-100)");
 static_assert(sizeof(SrGpuUniforms) == 768, "GpuUniforms is 768 bytes (gpu.rs:122-144)");
 static_assert(sizeof(SrTuning) == 48, "SrTuning is 12 words");
+static_assert(sizeof(SrRay) == 56 && sizeof(SrRayHit) == 80, "ray query records");
 static_assert(offsetof(SrGpuUniforms, light_pos) == 80, "Uniforms.light_pos");
 static_assert(offsetof(SrGpuUniforms, num_nodes) == 124, "Uniforms.num_nodes");
 static_assert(offsetof(SrGpuUniforms, frontier_origin) == 128, "Uniforms.frontier_origin");

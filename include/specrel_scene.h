@@ -114,6 +114,21 @@ typedef struct SrFrameDynamics {
     uint32_t pad;
 } SrFrameDynamics;
 
+/* The flash list of FrameDynamics (renderer.rs:179, 228, 274-311), kept by the caller in an array
+ * of at least SR_MAX_FLASHES entries holding *n of them, oldest first:
+ * - sr_flash_emit: FrameDynamics::emit_flash (hit = 0: width 0.8, intensity 2.5, colour
+ *   (1, 0.9, 0.7)) or emit_hit_flash (hit != 0: width 0.5, intensity 3, colour (1, 0.35, 0.12))
+ *   at event `at`; the oldest is evicted when SR_MAX_FLASHES are held;
+ * - sr_flashes_retire: retire_flashes, keeps (in order) the flashes with now_t - at.t < 200 (the
+ *   shell radius beyond which they light nothing the renderers reach);
+ * - sr_flashes_shift_time: shift_time, adds dt to every flash's lab time. */
+sr_status sr_flash_emit(SrFlash* flashes, uint32_t* n, const float at[4], int hit);
+sr_status sr_flashes_retire(SrFlash* flashes, uint32_t* n, float now_t);
+sr_status sr_flashes_shift_time(SrFlash* flashes, uint32_t n, float dt);
+/* RenderConfig::step_prophecy_delta (renderer.rs:121-124, 172-175): prophecy_delta + steps * 0.5,
+ * clamped to [0.5, 20]. */
+sr_status sr_config_step_prophecy_delta(SrRenderConfig* cfg, float steps);
+
 /* GpuUniforms::build (gpu.rs:147-211). `dyn` may be NULL (FrameDynamics::default()). */
 sr_status sr_uniforms_build(const SrCamera* cam, const SrRenderConfig* cfg, const SrFrameDynamics* dyn,
                             uint32_t num_nodes, const float light_pos[4], uint32_t num_stars, SrGpuUniforms* out);

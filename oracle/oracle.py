@@ -89,6 +89,14 @@ def lib():
         L.orc_scene_from_packed.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                             C.c_uint32, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]
         L.orc_scene_info.argtypes = [C.c_void_p, C.POINTER(SceneInfo)]
+        L.orc_scene_demo.restype = C.c_void_p
+        L.orc_scene_demo.argtypes = [C.c_uint32, C.c_int]
+        L.orc_scene_demo_info.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        L.orc_light_clock_bounce_fraction.restype = C.c_float
+        L.orc_light_clock_bounce_fraction.argtypes = [C.c_float, C.c_float]
+        L.orc_material.argtypes = [C.c_uint32, C.c_void_p]
+        L.orc_tetrad_from_beta.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_scene_pack.argtypes = [C.c_void_p] + [C.c_void_p] * 6
         L.orc_render.argtypes = [C.c_void_p, C.POINTER(Camera), C.POINTER(Config), C.POINTER(Dynamics),
                                  C.c_int, C.c_int, C.POINTER(PixelOut)]
@@ -172,6 +180,30 @@ class Scene:
                                         num_stars, lp.ctypes.data)
         return cls(None, False, _handle=h)
 
+    @classmethod
+    def demo(cls, which: int, fp64: bool = False):
+        """One of the reference's demo scenes (scene.rs:283-720): DEMO_* below. Sets `window`
+        (t_min, t_max), `light` (x, y, z) and `initial_camera` (the scene's camera event)."""
+        h = lib().orc_scene_demo(which, 1 if fp64 else 0)
+        if not h:
+            raise ValueError(f"no demo scene {which}")
+        sc = cls(None, fp64, _handle=h)
+        d = np.zeros(5)
+        lib().orc_scene_demo_info(h, d.ctypes.data)
+        sc.window = (float(d[0]), float(d[1]))
+        sc.light = (float(d[2]), float(d[3]), float(d[4]))
+        sc.initial_camera = tuple(float(x) for x in sc.info.cam_pos)
+        return sc
+
+    def trace(self, rays) -> np.ndarray:
+        """Bvh4D::trace (bvh4d.rs:445-520) of rays (n x 10: origin t,x,y,z, direction, t_min, t_max)
+        and the interpolated hit: n x 18 (found, slot, original index, lambda, proper time,
+        event t,x,y,z, tet barycentrics (4), uv (2), material)."""
+        r = np.ascontiguousarray(np.atleast_2d(rays), np.float64)
+        out = np.zeros((len(r), 18))
+        lib().orc_trace(self.h, r.ctypes.data, len(r), out.ctypes.data)
+        return out
+
     def __del__(self):
         if getattr(self, "h", None):
             self._free(self.h)
@@ -191,6 +223,31 @@ class Scene:
         if rc != 0:
             raise RuntimeError("only float scenes pack")
         return nodes, geoms, attrs, mats, stars, order
+
+
+DEMO_TWIN_PARADOX, DEMO_BARN_AND_POLE, DEMO_TERRELL_PENROSE_STREET, DEMO_EINSTEIN_TRAIN, DEMO_CAROUSEL = range(5)
+PENROSE_SPHERE = 5  # the scene of scene.rs's Penrose silhouette test (not a demo scene)
+
+
+def tetrad_from_beta(beta) -> np.ndarray:
+    """Tetrad::from_beta in f32 (minkowski.rs:437-441): rows e0..e3, columns (t, x, y, z)."""
+    b = np.asarray(beta, np.float64)
+    out = np.zeros(16)
+    lib().orc_tetrad_from_beta(b.ctypes.data, out.ctypes.data)
+    return out.reshape(4, 4).astype(np.float32)
+
+
+def light_clock_bounce_fraction(proper_time: float, cavity_length: float) -> float:
+    """renderer.rs:988-996 in f32."""
+    return float(lib().orc_light_clock_bounce_fraction(proper_time, cavity_length))
+
+
+def material(i: int) -> dict:
+    """Material i of the scenes' table (scene.rs:181-275), as f32 values."""
+    v = np.zeros(9)
+    pattern = lib().orc_material(i, v.ctypes.data)
+    return dict(base=tuple(v[0:3]), emission=v[3], checker=tuple(v[4:7]), grid_scale=v[7], cavity_length=v[8],
+                pattern=pattern)
 
 
 @dataclass

@@ -5,6 +5,7 @@
 
 #include "oracle_arena.hpp"
 #include "oracle_grad.hpp"
+#include "oracle_demo.hpp"
 #include "oracle_scenes.hpp"
 
 using namespace orc;
@@ -91,7 +92,32 @@ struct SceneBox {
     bool fp64;
     std::unique_ptr<SynthOut<float>> f;
     std::unique_ptr<SynthOut<double>> d;
+    double t_window[2] = {0.0, 0.0};  // a demo scene's valid lab-time window
 };
+
+// Bvh4D::trace of one ray (origin, direction, t_min, t_max: 10 doubles converted to T) and the
+// interpolated hit: out = found, slot, original simplex index, lambda, proper time, event (4),
+// tet barycentrics (4), uv (2), material.
+template <class T> int trace_t(const SynthOut<T>& so, const double* r, double* out) {
+    const auto& bvh = so.scene.bvh;
+    V4<T> o((T)r[0], (T)r[1], (T)r[2], (T)r[3]), d((T)r[4], (T)r[5], (T)r[6], (T)r[7]);
+    HitRecord<T> h{};
+    int64_t slot = -1;
+    bool found = bvh.trace(o, d, (T)r[8], (T)r[9], &h, &slot, nullptr);
+    for (int k = 0; k < 18; ++k) out[k] = 0.0;
+    out[0] = found ? 1.0 : 0.0;
+    out[1] = (double)slot;
+    out[2] = found ? (double)bvh.order[(size_t)slot] : -1.0;
+    if (!found) return 0;
+    out[3] = (double)h.lambda;
+    out[4] = (double)h.proper_time;
+    out[5] = (double)h.event.t; out[6] = (double)h.event.x; out[7] = (double)h.event.y; out[8] = (double)h.event.z;
+    for (int k = 0; k < 4; ++k) out[9 + k] = (double)h.tet_bary[k];
+    out[13] = (double)h.uv_u;
+    out[14] = (double)h.uv_v;
+    out[15] = (double)h.material_id;
+    return 0;
+}
 
 template <class T> Tetrad<T> make_tetrad(const OrcCamera& c) {
     Tetrad<T> t = Tetrad<T>::rest();
@@ -212,6 +238,81 @@ void* orc_scene_new(const OrcSynthParams* p, int fp64) {
 }
 
 void orc_scene_free(void* s) { delete (SceneBox*)s; }
+
+// One of the reference's demo scenes (oracle_demo.hpp: 0 twin paradox, 1 barn and pole, 2
+// Terrell-Penrose street, 3 Einstein's train, 4 carousel; 5 the Penrose test's own sphere, scene.rs:985-996); its initial camera event is the info's
+// cam_pos, its lab-time window and light from orc_scene_demo_info.
+void* orc_scene_demo(uint32_t which, int fp64) {
+    if (which > 5) return nullptr;
+    auto* b = new SceneBox();
+    b->fp64 = fp64 != 0;
+    if (b->fp64) {
+        auto o = build_demo<double>(which);
+        b->t_window[0] = o.t_min;
+        b->t_window[1] = o.t_max;
+        b->d = std::make_unique<SynthOut<double>>(std::move(o.s));
+    } else {
+        auto o = build_demo<float>(which);
+        b->t_window[0] = o.t_min;
+        b->t_window[1] = o.t_max;
+        b->f = std::make_unique<SynthOut<float>>(std::move(o.s));
+    }
+    return b;
+}
+
+// A demo scene's lab-time window and light position: t_min, t_max, light x, y, z.
+int orc_scene_demo_info(void* s, double* out5) {
+    auto* b = (SceneBox*)s;
+    out5[0] = b->t_window[0];
+    out5[1] = b->t_window[1];
+    if (b->fp64) {
+        const auto& l = b->d->scene.light_pos;
+        out5[2] = l.x; out5[3] = l.y; out5[4] = l.z;
+    } else {
+        const auto& l = b->f->scene.light_pos;
+        out5[2] = l.x; out5[3] = l.y; out5[4] = l.z;
+    }
+    return 0;
+}
+
+// Rays through the scene's BVH (trace_t above): rays are 10 doubles each, out 18 doubles each.
+int orc_trace(void* s, const double* rays, uint32_t n, double* out) {
+    auto* b = (SceneBox*)s;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (b->fp64) trace_t(*b->d, rays + 10 * (size_t)i, out + 18 * (size_t)i);
+        else trace_t(*b->f, rays + 10 * (size_t)i, out + 18 * (size_t)i);
+    }
+    return 0;
+}
+
+// Tetrad::from_beta (minkowski.rs:437-441) in f32: e[a][k] into out16[4 * a + k].
+int orc_tetrad_from_beta(const double* beta3, double* out16) {
+    Tetrad<float> t = Tetrad<float>::from_beta(V3<float>((float)beta3[0], (float)beta3[1], (float)beta3[2]));
+    for (int a = 0; a < 4; ++a) {
+        out16[4 * a] = t.e[a].t;
+        out16[4 * a + 1] = t.e[a].x;
+        out16[4 * a + 2] = t.e[a].y;
+        out16[4 * a + 3] = t.e[a].z;
+    }
+    return 0;
+}
+
+// light_clock_bounce_fraction (renderer.rs:988-996) in f32.
+float orc_light_clock_bounce_fraction(float proper_time, float cavity_length) {
+    return light_clock_bounce_fraction<float>(proper_time, cavity_length);
+}
+
+// Material `i` of the demo scenes' table: base rgb, emission, checker rgb, grid scale, wire width,
+// pattern, cavity length.
+int orc_material(uint32_t i, double* out9) {
+    auto m = common_materials<float>();
+    if (i >= m.size()) return -1;
+    const auto& x = m[i];
+    double v[9] = {x.base_color.x, x.base_color.y, x.base_color.z, x.emission, x.checker_color.x, x.checker_color.y,
+                   x.checker_color.z, x.grid_scale, x.cavity_length};
+    for (int k = 0; k < 9; ++k) out9[k] = v[k];
+    return (int)x.pattern;
+}
 
 // A float scene from the reference's packed arrays (gpu.rs:44-119 layouts): the BVH nodes and hot
 // records as given, the cold attributes as leaf-ordered simplices (order = identity). Lets the

@@ -551,6 +551,20 @@ class Engine:
         _check(st, self.h, "adjoint")
         return r
 
+    def trace_rays(self, idx: int, rays) -> np.ndarray:
+        """sr_trace_rays: Bvh4D::trace and interpolate_hit of rays (n x 10: origin t, x, y, z as
+        doubles, direction, t_min, t_max) on the device. Returns a structured array of SrRayHit."""
+        r = np.atleast_2d(np.asarray(rays, np.float64))
+        n = len(r)
+        arr = (_lib.Ray * max(n, 1))()
+        for i in range(n):
+            arr[i].origin[:] = list(r[i, 0:4])
+            arr[i].dir[:] = list(np.float32(r[i, 4:8]))
+            arr[i].t_min, arr[i].t_max = float(np.float32(r[i, 8])), float(np.float32(r[i, 9]))
+        out = (_lib.RayHit * max(n, 1))()
+        _check(self.L.sr_trace_rays(self.h, idx, arr, n, out), self.h, "trace_rays")
+        return np.ctypeslib.as_array(out)[:n].copy()
+
     def tuning(self, idx: int) -> _lib.Tuning:
         t = _lib.Tuning()
         _check(self.L.sr_get_tuning(self.h, idx, C.byref(t)), self.h, "get_tuning")

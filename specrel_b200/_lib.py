@@ -35,6 +35,7 @@ SR_FLAG_ASYNC_OUTPUT = 16
 SR_NOALLOC_SCRATCH_BYTES = 8 << 20
 SR_ADJ_FROZEN = 1
 SR_NOALLOC_MAX_PIXELS = 1 << 18
+SR_MAX_FLASHES = 16
 
 # ---- packed layouts (gpu.rs:44-144) ------------------------------------------------------------
 NODE_DTYPE = np.dtype([("min", "<f4", 4), ("max", "<f4", 4), ("right_or_first", "<u4"), ("count", "<u4"),
@@ -46,6 +47,16 @@ MAT_DTYPE = np.dtype([("base", "<f4", 4), ("checker", "<f4", 4), ("params", "<f4
 TRI_DTYPE = np.dtype([("idx", "<u4", 3), ("uv", "<f4", (3, 2)), ("normal", "<f4", 3)])  # SrTubeTriangle
 SAMPLE_DTYPE = np.dtype([("center", "<f4", 4), ("tetrad", "<f4", (4, 4)), ("proper_time", "<f4"), ("phi", "<f4", 3),
                          ("accel", "<f4", 3), ("pad", "<f4")])  # SrTubeSample
+
+
+class Ray(C.Structure):  # SrRay
+    _fields_ = [("origin", C.c_double * 4), ("dir", C.c_float * 4), ("t_min", C.c_float), ("t_max", C.c_float)]
+
+
+class RayHit(C.Structure):  # SrRayHit
+    _fields_ = [("id", C.c_uint32), ("slot", C.c_uint32), ("lambda_", C.c_float), ("proper_time", C.c_float),
+                ("event", C.c_double * 4), ("tet_bary", C.c_float * 4), ("uv", C.c_float * 2), ("material", C.c_uint32),
+                ("pad", C.c_uint32)]
 
 
 class GpuUniforms(C.Structure):
@@ -216,6 +227,7 @@ SIGNATURES = {
                                C.c_uint32, C.c_uint32, C.POINTER(AdjointResult)]),
     "sr_adjoint_rows": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64), C.c_void_p,
                                     C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(AdjointResult)]),
+    "sr_trace_rays": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p]),
     "sr_render_noalloc": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64), C.c_void_p]),
     "sr_get_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),
     "sr_set_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),
@@ -232,6 +244,10 @@ SIGNATURES = {
     "sr_uniforms_build": (C.c_int32, [C.POINTER(Camera), C.POINTER(RenderConfig), C.POINTER(FrameDynamics),
                                       C.c_uint32, C.POINTER(C.c_float), C.c_uint32, C.POINTER(GpuUniforms)]),
     "sr_tables_build": (C.c_int32, [C.POINTER(C.c_uint32)]),
+    "sr_flash_emit": (C.c_int32, [C.POINTER(Flash), C.POINTER(C.c_uint32), C.POINTER(C.c_float), C.c_int]),
+    "sr_flashes_retire": (C.c_int32, [C.POINTER(Flash), C.POINTER(C.c_uint32), C.c_float]),
+    "sr_flashes_shift_time": (C.c_int32, [C.POINTER(Flash), C.c_uint32, C.c_float]),
+    "sr_config_step_prophecy_delta": (C.c_int32, [C.POINTER(RenderConfig), C.c_float]),
 }
 
 

@@ -627,6 +627,31 @@ sr_status sr_render(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_t*
     return sr_render_ex(ctx, idx, u, nullptr, &o, t);
 }
 
+sr_status sr_trace_rays(sr_ctx* ctx, uint32_t idx, const SrRay* rays, uint32_t n, SrRayHit* hits) {
+    if (!ctx || (n && (!rays || !hits))) return SR_ERR_INVALID_ARGUMENT;
+    if (idx >= ctx->scenes.size() || !ctx->scenes[idx] || !ctx->scenes[idx]->present)
+        return fail(ctx, SR_ERR_NO_SCENE, "scene " + std::to_string(idx) + " is not uploaded");
+    if (n == 0) return SR_OK;
+    CK(cudaSetDevice(ctx->device), "set device");
+    SceneSlot& s = *ctx->scenes[idx];
+    DevBuf din, dout;
+    CK(din.ensure((size_t)n * sizeof(SrRay)), "ray buffer");
+    CK(dout.ensure((size_t)n * sizeof(SrRayHit)), "hit buffer");
+    cudaStream_t sm = ctx->stream;
+    CK(cudaMemcpyAsync(din.p, rays, (size_t)n * sizeof(SrRay), cudaMemcpyHostToDevice, sm), "rays in");
+    CK(cudaMemsetAsync(ctx->counters.p, 0, 16, sm), "clear counters");
+    CK(launch_trace_rays(scene_dev(ctx, s), s.anchor, din.as<SrRay>(), n, dout.as<SrRayHit>(), ctx->counters.as<uint32_t>(),
+                         sm),
+       "ray kernel");
+    CK(cudaMemcpyAsync(hits, dout.p, (size_t)n * sizeof(SrRayHit), cudaMemcpyDeviceToHost, sm), "hits out");
+    uint32_t counters[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(counters, ctx->counters.p, 16, cudaMemcpyDeviceToHost, sm), "counters");
+    CK(cudaStreamSynchronize(sm), "ray sync");
+    if (counters[1] & ERR_TRAVERSAL_LIMIT) return fail(ctx, SR_ERR_TRAVERSAL_LIMIT, "a ray exceeded the traversal visit limit");
+    if (counters[1]) return fail(ctx, SR_ERR_BAD_SCENE, "device reported a bad index (flags " + std::to_string(counters[1]) + ")");
+    return SR_OK;
+}
+
 sr_status sr_render_batch(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, const SrCameraF64* cam64, uint32_t n,
                           uint32_t* rgb_out, uint64_t rgb_len, uint32_t flags, SrTimings* timings) {
     if (!ctx || (!u && n) || (!rgb_out && n)) return SR_ERR_INVALID_ARGUMENT;

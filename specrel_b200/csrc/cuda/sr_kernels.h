@@ -72,6 +72,10 @@ cudaError_t launch_render_plain(const SceneDev& s, const SrGpuUniforms& u, const
 // scene anchor, rounds to f32 and writes 6 float4 (event, e0..e3, frontier origin) to `cam_dev`.
 cudaError_t launch_camera_f64(const SrCameraF64& c, const double anchor[4], const SrGpuUniforms& u, float4* cam_dev,
                               cudaStream_t st);
+// Bvh4D::trace and interpolate_hit of caller rays (sr_trace_rays), the reference's traversal;
+// error flags into counters[1].
+cudaError_t launch_trace_rays(const SceneDev& s, const double anchor[4], const SrRay* rays, uint32_t n, SrRayHit* hits,
+                              uint32_t* counters, cudaStream_t st);
 // Bloom pyramid, composite, tone map and pack into f.rgb.
 cudaError_t launch_bloom(const FrameDev& f, const Pyramid& p, const uint32_t* tables, cudaStream_t st);
 

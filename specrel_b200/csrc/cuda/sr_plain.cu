@@ -157,4 +157,52 @@ cudaError_t launch_render_plain(const SceneDev& s, const SrGpuUniforms& u, const
     return cudaGetLastError();
 }
 
+// Caller rays (sr_trace_rays): one thread per ray, the reference's traversal, then the hit
+// record interpolated as the shading reads it.
+__global__ void k_trace_rays(SceneDev s, double a0, double a1, double a2, double a3, const SrRay* rays, uint32_t n,
+                             SrRayHit* hits, uint32_t* counters) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const SrRay r = rays[i];
+    const float4 o = v4((float)(r.origin[0] - a0), (float)(r.origin[1] - a1), (float)(r.origin[2] - a2),
+                        (float)(r.origin[3] - a3));
+    const float4 d = v4(r.dir[0], r.dir[1], r.dir[2], r.dir[3]);
+    SrRayHit out;
+    out.id = 0xFFFFFFFFu;
+    out.slot = 0xFFFFFFFFu;
+    out.lambda = out.proper_time = 0.0f;
+    for (int k = 0; k < 4; ++k) { out.event[k] = 0.0; out.tet_bary[k] = 0.0f; }
+    out.uv[0] = out.uv[1] = 0.0f;
+    out.material = out.pad = 0u;
+    GeomHit gh;
+    const int slot = trace_ref(s, o, d, r.t_min, r.t_max, &gh, counters + 1);
+    if (slot >= 0) {
+        Hit h;
+        interpolate(s.attrs + 12u * (uint32_t)slot, o, d, gh, &h);
+        out.slot = (uint32_t)slot;
+        out.id = s.leaf_to_orig ? __ldg(s.leaf_to_orig + slot) : (uint32_t)slot;
+        out.lambda = h.lambda;
+        out.proper_time = h.tau;
+        out.event[0] = (double)h.event.x + a0;
+        out.event[1] = (double)h.event.y + a1;
+        out.event[2] = (double)h.event.z + a2;
+        out.event[3] = (double)h.event.w + a3;
+        out.tet_bary[0] = h.b0;
+        out.tet_bary[1] = h.b1;
+        out.tet_bary[2] = h.b2;
+        out.tet_bary[3] = h.b3;
+        out.uv[0] = h.uv_u;
+        out.uv[1] = h.uv_v;
+        out.material = h.material;
+    }
+    hits[i] = out;
+}
+
+cudaError_t launch_trace_rays(const SceneDev& s, const double anchor[4], const SrRay* rays, uint32_t n, SrRayHit* hits,
+                              uint32_t* counters, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_trace_rays<<<(n + 127) / 128, 128, 0, st>>>(s, anchor[0], anchor[1], anchor[2], anchor[3], rays, n, hits, counters);
+    return cudaGetLastError();
+}
+
 }  // namespace srk

@@ -106,6 +106,51 @@ extern "C" sr_status sr_uniforms_build(const SrCamera* cam, const SrRenderConfig
     return SR_OK;
 }
 
+extern "C" sr_status sr_flash_emit(SrFlash* flashes, uint32_t* n, const float at[4], int hit) {
+    if (!flashes || !n || !at || *n > SR_MAX_FLASHES) return SR_ERR_INVALID_ARGUMENT;
+    // push_flash (renderer.rs:293-298): evict the oldest when every slot is taken.
+    if (*n >= SR_MAX_FLASHES) {
+        std::memmove(flashes, flashes + 1, (SR_MAX_FLASHES - 1) * sizeof(SrFlash));
+        *n = SR_MAX_FLASHES - 1;
+    }
+    SrFlash& f = flashes[(*n)++];
+    for (int k = 0; k < 4; ++k) f.at[k] = at[k];
+    if (hit) {  // emit_hit_flash (renderer.rs:283-291), HIT_FLASH_COLOR (renderer.rs:231)
+        f.width = 0.5f;
+        f.intensity = 3.0f;
+        f.color[0] = 1.0f; f.color[1] = 0.35f; f.color[2] = 0.12f;
+    } else {  // emit_flash (renderer.rs:274-281)
+        f.width = 0.8f;
+        f.intensity = 2.5f;
+        f.color[0] = 1.0f; f.color[1] = 0.9f; f.color[2] = 0.7f;
+    }
+    return SR_OK;
+}
+
+extern "C" sr_status sr_flashes_retire(SrFlash* flashes, uint32_t* n, float now_t) {
+    if (!n || (*n && !flashes)) return SR_ERR_INVALID_ARGUMENT;
+    const float max_radius = 200.0f;  // FLASH_MAX_RADIUS (renderer.rs:228)
+    uint32_t keep = 0;
+    for (uint32_t i = 0; i < *n; ++i)
+        if (now_t - flashes[i].at[0] < max_radius) flashes[keep++] = flashes[i];
+    *n = keep;
+    return SR_OK;
+}
+
+extern "C" sr_status sr_flashes_shift_time(SrFlash* flashes, uint32_t n, float dt) {
+    if (n && !flashes) return SR_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < n; ++i) flashes[i].at[0] += dt;
+    return SR_OK;
+}
+
+extern "C" sr_status sr_config_step_prophecy_delta(SrRenderConfig* cfg, float steps) {
+    if (!cfg) return SR_ERR_INVALID_ARGUMENT;
+    // PROPHECY_DELTA_MIN / MAX / STEP (renderer.rs:121-124); f32::clamp.
+    float v = cfg->prophecy_delta + steps * 0.5f;
+    cfg->prophecy_delta = v < 0.5f ? 0.5f : (v > 20.0f ? 20.0f : v);
+    return SR_OK;
+}
+
 static const uint8_t GLYPHS[14][7] = {
     {0b01110, 0b10001, 0b10011, 0b10101, 0b11001, 0b10001, 0b01110},  // 0
     {0b00100, 0b01100, 0b00100, 0b00100, 0b00100, 0b00100, 0b01110},  // 1
