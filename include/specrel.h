@@ -4,8 +4,9 @@
  * It replaces the wgpu backend `GpuRenderer` (src/gpu.rs:432-901) behind the same data split the
  * reference already uses: static scene arrays uploaded once (`PackedSceneGpuData`,
  * src/gpu.rs:232-315) and a 768-byte per-frame uniform block (`GpuUniforms`,
- * src/gpu.rs:122-212). A Rust caller binds these functions with `extern "C"` (see
- * INTEGRATION.md) and keeps `Scene4D::build`, `PackedSceneGpuData::from_scene` and
+ * src/gpu.rs:122-212). A Rust caller binds these functions with `extern "C"` and `#[repr(C)]`
+ * mirrors of the structs below (their sizes and offsets are fixed by the static_asserts at the
+ * end of this header) and keeps `Scene4D::build`, `PackedSceneGpuData::from_scene` and
  * `GpuUniforms::build` as they are.
  *
  * Conventions: every function returns an `sr_status` (no aborts); host buffers belong to the
@@ -434,6 +435,41 @@ sr_status sr_adjoint_rows(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* 
                           const float* target_hdr, uint32_t level, uint32_t flags, uint32_t row_begin,
                           uint32_t row_end, SrAdjointResult* out);
 
+/* ---- The gradient over a group of GPUs ------------------------------------------------------
+ * No counterpart in the reference (it renders on one device). One observer's gradient shards over
+ * `world` ranks, one GPU each, every rank holding the scene and the target image: each rank
+ * evaluates its band of the loss level's rows (sr_adjoint_rows) and the ten doubles of
+ * SrAdjointResult are summed over the group. The sum is the caller's collective, passed in as a
+ * function: an ncclAllReduce of doubles on the caller's communicator, an MPI_Allreduce, or
+ * sr_nccl_sum_f64 below. It returns 0 on success. */
+typedef int (*sr_sum_f64_fn)(double* values, size_t count, void* user);
+/* Rank `rank`'s band of the loss level's rows (`level` halvings of `height`, rounding up, as the
+ * loss takes them): [*row_begin, *row_end), contiguous, sizes differing by at most one, empty when
+ * the level has fewer rows than ranks. Host only. */
+sr_status sr_adjoint_band(uint32_t height, uint32_t level, uint32_t rank, uint32_t world, uint32_t* row_begin,
+                          uint32_t* row_end);
+/* Sums `r` (loss, gradient[7], primal mismatches, star terms) over the group in place through
+ * `sum`. Host only. */
+sr_status sr_adjoint_reduce(SrAdjointResult* r, sr_sum_f64_fn sum, void* user);
+/* sr_adjoint_rows over this rank's band, then sr_adjoint_reduce: every rank receives the whole
+ * frame's loss and gradient. Every rank of the group calls it (a rank with an empty band adds
+ * zeros), in the same order relative to the caller's other collectives. `flags` as sr_adjoint (a
+ * frozen evaluation follows this rank's previous gradient call). */
+sr_status sr_adjoint_group(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, const SrCameraF64* cam,
+                           const float* target_hdr, uint32_t level, uint32_t flags, uint32_t rank, uint32_t world,
+                           sr_sum_f64_fn sum, void* user, SrAdjointResult* out);
+/* A sum for sr_adjoint_reduce / sr_adjoint_group over NCCL: `user` points to an SrNcclSum. The
+ * library loads NCCL (libnccl.so.2) at the first call; the caller creates the communicator, one
+ * rank per GPU. The values go through `device_buf` (at least `count` doubles of device memory the
+ * caller owns) on `stream`, and the call waits for them. Returns the ncclResult_t, or -1 when
+ * NCCL cannot be loaded, -2 on a CUDA error. */
+typedef struct SrNcclSum {
+    void* comm;          /* ncclComm_t */
+    void* stream;        /* cudaStream_t (NULL: the legacy default stream) */
+    double* device_buf;
+} SrNcclSum;
+int sr_nccl_sum_f64(double* values, size_t count, void* user);
+
 /* ---- Rendering without device allocation -------------------------------------------------
  * No counterpart in the reference: an entry point for callers that cannot call cudaMalloc while
  * they render, for instance an application whose own allocator owns all device memory under a fixed
@@ -498,6 +534,7 @@ static_assert(sizeof(SrGpuMaterial) == 48, "GpuMaterial is 48 bytes (gpu.rs:96-1
 static_assert(sizeof(SrGpuUniforms) == 768, "GpuUniforms is 768 bytes (gpu.rs:122-144)");
 static_assert(sizeof(SrTuning) == 48, "SrTuning is 12 words");
 static_assert(sizeof(SrRay) == 56 && sizeof(SrRayHit) == 80, "ray query records");
+static_assert(sizeof(SrAdjointResult) == 80 && sizeof(SrCameraF64) == 80, "gradient records");
 static_assert(offsetof(SrGpuUniforms, light_pos) == 80, "Uniforms.light_pos");
 static_assert(offsetof(SrGpuUniforms, num_nodes) == 124, "Uniforms.num_nodes");
 static_assert(offsetof(SrGpuUniforms, frontier_origin) == 128, "Uniforms.frontier_origin");

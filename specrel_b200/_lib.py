@@ -189,6 +189,14 @@ assert C.sizeof(GpuUniforms) == 768 and C.sizeof(Timings) == 96
 _lib = None
 
 # Every function either header declares, with its ctypes signature.
+# sr_sum_f64_fn: the caller's sum over a group (0 on success).
+SUM_F64_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_size_t, C.c_void_p)
+
+
+class NcclSum(C.Structure):  # SrNcclSum
+    _fields_ = [("comm", C.c_void_p), ("stream", C.c_void_p), ("device_buf", C.c_void_p)]
+
+
 SIGNATURES = {
     "sr_create": (C.c_int32, [C.c_int, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
     "sr_destroy": (None, [C.c_void_p]),
@@ -228,6 +236,13 @@ SIGNATURES = {
     "sr_adjoint_rows": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64), C.c_void_p,
                                     C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(AdjointResult)]),
     "sr_trace_rays": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "sr_adjoint_band": (C.c_int32, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint32)]),
+    "sr_adjoint_reduce": (C.c_int32, [C.POINTER(AdjointResult), SUM_F64_FN, C.c_void_p]),
+    "sr_adjoint_group": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64), C.c_void_p,
+                                     C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, SUM_F64_FN, C.c_void_p,
+                                     C.POINTER(AdjointResult)]),
+    "sr_nccl_sum_f64": (C.c_int, [C.POINTER(C.c_double), C.c_size_t, C.c_void_p]),
     "sr_render_noalloc": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(CameraF64), C.c_void_p]),
     "sr_get_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),
     "sr_set_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),

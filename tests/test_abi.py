@@ -106,3 +106,69 @@ def test_validate_rejects_corrupt_scene(breakage):
     status, _, msg = sr.validate(p)
     assert status == sr._lib.SR_ERR_BAD_SCENE, breakage
     assert msg
+
+
+C_PROGRAM = r"""
+#include <stdio.h>
+#include <string.h>
+#include "specrel.h"
+#include "specrel_scene.h"
+
+/* A non-Python host: one leaf holding one tetrahedron, validated on the host, then a context. */
+int main(void) {
+    SrGpuNode node;
+    memset(&node, 0, sizeof node);
+    for (int k = 0; k < 4; ++k) { node.min[k] = -1.0f; node.max[k] = 1.0f; }
+    node.right_or_first = 0;
+    node.count = 1;
+    SrGpuGeom geom;
+    SrGpuAttr attr;
+    memset(&geom, 0, sizeof geom);
+    memset(&attr, 0, sizeof attr);
+    SrGpuMaterial mat;
+    memset(&mat, 0, sizeof mat);
+    SrSceneDesc d;
+    memset(&d, 0, sizeof d);
+    d.nodes = &node;
+    d.num_nodes = 1;
+    d.num_prims = 1;
+    d.geoms = &geom;
+    d.attrs = &attr;
+    d.materials = &mat;
+    d.num_materials = 1;
+    uint32_t depth = 0;
+    char err[256] = "";
+    sr_status v = sr_scene_validate(&d, &depth, err, sizeof err);
+    node.count = 2; /* a leaf past the records */
+    sr_status bad = sr_scene_validate(&d, NULL, err, sizeof err);
+    sr_ctx* ctx = NULL;
+    char cerr[256] = "";
+    sr_status c = sr_create(0, &ctx, cerr, sizeof cerr);
+    if (c == SR_OK) sr_destroy(ctx);
+    uint32_t r0 = 0, r1 = 0;
+    sr_status b = sr_adjoint_band(800, 3, 1, 4, &r0, &r1);
+    printf("%d %u %d %d %d %u %u\n", (int)v, depth, (int)bad, (int)c, (int)b, r0, r1);
+    return 0;
+}
+"""
+
+
+def test_c_host_compiles_links_and_calls_the_library(tmp_path):
+    """A C program built with gcc against include/specrel.h and include/specrel_scene.h (C99), linked
+    with libspecrel_cuda.so, calls the library as a Rust or C host would: host-side validation, a
+    context (SR_ERR_NO_DEVICE without a GPU) and the gradient's row bands."""
+    import subprocess
+    import specrel_b200._lib as L
+    src = tmp_path / "host.c"
+    src.write_text(C_PROGRAM)
+    exe = tmp_path / "host"
+    libdir = os.path.dirname(L.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", libdir, "-lspecrel_cuda", f"-Wl,-rpath,{libdir}"], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    v, depth, bad, c, b, r0, r1 = map(int, out)
+    assert v == L.SR_OK and depth == 1
+    assert bad == L.SR_ERR_BAD_SCENE
+    import torch
+    assert c == (L.SR_OK if torch.cuda.is_available() else L.SR_ERR_NO_DEVICE)
+    assert b == L.SR_OK and (r0, r1) == (25, 50)  # 800 rows halved 3 times: 100, rank 1 of 4

@@ -145,3 +145,54 @@ def test_gradient_descent_recovers_the_rapidity(engine):
                 break
     print("recovered", phi)
     assert np.abs(phi - np.array(STAR)).max() < 1e-4
+
+
+def test_group_gradient_through_the_c_abi(engine, setup):
+    """sr_adjoint_group, the path a non-Python host takes over several GPUs, run as three ranks in
+    turn on this GPU with a sum that records each rank's part: the parts sum to sr_adjoint's whole
+    frame. Then as a group of one over a real NCCL communicator through sr_nccl_sum_f64."""
+    import ctypes as C
+
+    import torch
+    from specrel_b200 import _lib as L
+    th = np.array((0.75, -0.25, 0.45, 0.0, 0.1, -0.05, 0.08))
+    u, cam, tp = setup["u"], _cam64(th), setup["tdev"].data_ptr()
+    whole = engine.adjoint(11, u, cam, tp, 2)
+    parts = []
+
+    @L.SUM_F64_FN
+    def record(values, count, user):
+        parts.append(np.ctypeslib.as_array(values, shape=(count,)).copy())
+        return 0
+
+    for rank in range(3):
+        r = L.AdjointResult()
+        assert engine.L.sr_adjoint_group(engine.h, 11, C.byref(u), C.byref(cam), tp, 2, 0, rank, 3, record, None,
+                                         C.byref(r)) == L.SR_OK
+    total = np.sum(parts, axis=0)
+    ref = np.array([whole.loss, *[whole.grad[k] for k in range(7)], whole.primal_mismatch, whole.star_terms])
+    assert len(parts) == 3
+    assert abs(total[0] - ref[0]) <= 1e-12 * ref[0]
+    assert np.abs(total[1:8] - ref[1:8]).max() <= 1e-12 * np.abs(ref[1:8]).max()
+    assert total[8] == ref[8] and total[9] == ref[9]
+
+    # A group of one over NCCL (the communicator made here through NCCL's own C API).
+    nccl = C.CDLL("libnccl.so.2")
+
+    class UniqueId(C.Structure):
+        _fields_ = [("internal", C.c_char * 128)]
+
+    uid = UniqueId()
+    assert nccl.ncclGetUniqueId(C.byref(uid)) == 0
+    comm = C.c_void_p()
+    assert nccl.ncclCommInitRank(C.byref(comm), 1, uid, 0) == 0
+    try:
+        buf = torch.zeros(10, dtype=torch.float64, device="cuda:0")
+        s = L.NcclSum(comm, None, buf.data_ptr())
+        nccl_sum = L.SUM_F64_FN(("sr_nccl_sum_f64", engine.L))
+        r = L.AdjointResult()
+        assert engine.L.sr_adjoint_group(engine.h, 11, C.byref(u), C.byref(cam), tp, 2, 0, 0, 1, nccl_sum, C.byref(s),
+                                         C.byref(r)) == L.SR_OK
+        assert r.loss == whole.loss and list(r.grad) == list(whole.grad)
+    finally:
+        nccl.ncclCommDestroy(comm)

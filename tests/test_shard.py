@@ -117,3 +117,73 @@ def test_single_process_needs_no_group():
     a = shard.observer_rapidities(5, 1, 4)
     assert a == shard.observer_rapidities(5, 1, 4)
     assert a != shard.observer_rapidities(5, 0, 4)
+
+
+def _c_reduce_worker(rank, port, q):
+    """The C-level path a non-Python host takes: sr_adjoint_band for the rank's rows, then
+    sr_adjoint_reduce with the caller's sum (here gloo's all-reduce behind a C function pointer)."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=WORLD, timeout=datetime.timedelta(seconds=60))
+    try:
+        from specrel_b200 import _lib as L
+        from specrel_b200 import shard
+        lib = L.lib()
+        bands = []
+        for level in (0, 3, 6):
+            r0, r1 = C.c_uint32(), C.c_uint32()
+            assert lib.sr_adjoint_band(800, level, rank, WORLD, C.byref(r0), C.byref(r1)) == L.SR_OK
+            bands.append((r0.value, r1.value, shard.row_band(shard.loss_rows(800, level), rank, WORLD)))
+        calls = []
+
+        @L.SUM_F64_FN
+        def gloo_sum(values, count, user):
+            t = torch.tensor(np.ctypeslib.as_array(values, shape=(count,)).copy())
+            dist.all_reduce(t)
+            for k in range(count):
+                values[k] = float(t[k])
+            calls.append(count)
+            return 0
+
+        part = L.AdjointResult()
+        part.loss = 1.5 + rank
+        for k in range(7):
+            part.grad[k] = (rank + 1) * (k - 3) * 0.25
+        part.primal_mismatch = 0.0
+        part.star_terms = 100.0 * (rank + 1)
+        assert lib.sr_adjoint_reduce(C.byref(part), gloo_sum, None) == L.SR_OK
+        q.put((rank, bands, part.loss, list(part.grad), part.primal_mismatch, part.star_terms, calls))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_reduce_the_gradient_through_the_c_abi():
+    """Two gloo ranks: the library's row bands equal the Python harness's, and sr_adjoint_reduce
+    sums the ten doubles of SrAdjointResult through the caller's sum function."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_c_reduce_worker, args=(r, port, q)) for r in range(WORLD)]
+    for p in procs:
+        p.start()
+    try:
+        results = sorted(q.get(timeout=180) for _ in range(WORLD))
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert all(p.exitcode == 0 for p in procs)
+    for rank, bands, loss, grad, pm, stars, calls in results:
+        for r0, r1, ref in bands:
+            assert (r0, r1) == ref
+        assert loss == 1.5 + 2.5
+        assert grad == [3 * (k - 3) * 0.25 for k in range(7)]
+        assert pm == 0.0 and stars == 300.0
+        assert calls == [10]
