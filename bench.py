@@ -483,6 +483,25 @@ def run_engine(args, rank, world, local):
         wall_e2e = (time.perf_counter() - t_e2e) / args.steps * 1e3
         e2e_ms = max_over_ranks(max(e0.elapsed_time(e1) / args.steps, wall_e2e))
 
+        # The compact node layout (one copy of the child boxes instead of 16 sign-octant copies) on
+        # the same batches: what the octant copies cost in memory and buy in speed.
+        compact = None
+        if not args.no_extra and eng.stats(0).box_copies == 16:
+            eng.set_layout(0, sr._lib.SR_LAYOUT_COMPACT)
+            compact_stats = eng.stats(0)
+            for _ in range(max(1, args.warmup)):
+                batch_step()
+            torch.cuda.synchronize()
+            barrier()
+            e0.record(stream)
+            for _ in range(args.steps):
+                batch_step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            compact_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+            eng.set_layout(0, sr._lib.SR_LAYOUT_AUTO)
+            compact = (compact_stats, compact_ms)
+
         # Fresh observers every step (new seeded rapidities, never rendered before), with L2 flushed
         # (a 256 MiB write) before each step; only the batches are inside the events.
         if not args.no_extra:
@@ -557,7 +576,8 @@ def run_engine(args, rank, world, local):
         "config": workload_config(args, world),
         "rays_per_step": total_rays, "tets": scene.num_prims,
         "footprint": {"scene_device_bytes": int(stats.device_bytes), "fast_nodes": int(stats.fast_nodes),
-                      "layout": "16 sign-octant box copies" if stats.fast_nodes else "plain"},
+                      "box_copies": int(stats.box_copies),
+                      "layout": "16 sign-octant box copies (SR_LAYOUT_AUTO)" if stats.box_copies == 16 else "compact"},
         "tuning": {k: getattr(tuning, k)
                    for k, _ in tuning._fields_},
         "scene_build_s": round(build_s, 2),
@@ -587,6 +607,12 @@ def run_engine(args, rank, world, local):
                                         "shadow_tet_tests": work[5] / B, "shadow_rays": work[6] / B}},
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
     }
+    if compact is not None:
+        cs, cms = compact
+        line["layout_compact"] = {"value": total_rays / (cms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": cms,
+                                  "scene_device_bytes": int(cs.device_bytes), "box_copies": int(cs.box_copies),
+                                  "how": "the same batches with SR_LAYOUT_COMPACT: one copy of the child boxes, "
+                                         "per-axis min / max in the traversal"}
     if not args.no_extra:
         line["value_fresh"] = {"value": total_rays / (fresh_ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": fresh_ms,
                                "how": "a new seeded set of observers every step, L2 flushed (256 MiB write) before "

@@ -352,8 +352,24 @@ typedef struct SrSceneStats {
     uint64_t device_bytes;
     uint32_t fast_nodes;   /* nodes of the B200 layout */
     uint32_t rindler_crossed; /* built from tubes, some vertex at some sample has 1 + a_local . p <= 0 */
+    uint32_t box_copies;   /* copies of the B200 layout's child boxes: 16 (octant) or 1 (compact) */
+    uint32_t pad;
 } SrSceneStats;
 sr_status sr_scene_stats(const sr_ctx* ctx, uint32_t scene_idx, SrSceneStats* out);
+
+/* The fast path's node layout. SR_LAYOUT_OCTANT keeps 16 copies of every wide node's child boxes,
+ * one per sign octant of a ray's inverse direction with each box's near corner first, so the slab
+ * test needs no per-axis min / max (1,024 bytes of boxes per internal node of the reference tree).
+ * SR_LAYOUT_COMPACT keeps one copy (64 bytes per internal node) and orders the corners per axis
+ * while traversing. SR_LAYOUT_AUTO, the default, takes the octant copies when the 15 extra copies
+ * need at most an eighth of the device's memory and all 16 fit in its free memory, else the
+ * compact layout. Hits, lambda, tau and the nodes visited are the same in every layout. The choice
+ * applies to the scene at `scene_idx` now (its layout is rebuilt) and to every later upload or
+ * build at that index. */
+#define SR_LAYOUT_AUTO 0u
+#define SR_LAYOUT_OCTANT 1u
+#define SR_LAYOUT_COMPACT 2u
+sr_status sr_set_layout(sr_ctx* ctx, uint32_t scene_idx, uint32_t layout);
 
 /* ---- Frames ------------------------------------------------------------------------------- */
 
@@ -508,8 +524,9 @@ typedef struct SrTuning {
     uint32_t stack_smem;      /* traversal-stack entries per thread kept in shared memory, 0..64
                                  (0: the whole stack in local memory); deeper entries go to local
                                  memory, so the visiting order does not depend on it */
-    uint32_t top_levels;      /* levels of the wide tree staged in shared memory per block, 0..10
-                                 (0: none) */
+    uint32_t top_levels;      /* levels of the wide tree staged in shared memory per block, 0..8
+                                 (0: none); with stack_smem 0 or 12; the compact layout
+                                 (sr_set_layout) stages none */
     uint32_t reserved;        /* 0 */
 } SrTuning;
 sr_status sr_get_tuning(const sr_ctx* ctx, uint32_t scene_idx, SrTuning* out);

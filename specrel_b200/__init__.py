@@ -470,6 +470,10 @@ class Engine:
                self.h, "update_scene")
         self.scenes[idx] = scene
 
+    def set_layout(self, idx: int, layout: int) -> None:
+        """sr_set_layout: SR_LAYOUT_AUTO / OCTANT / COMPACT for the scene at `idx` (rebuilt now if present)."""
+        _check(self.L.sr_set_layout(self.h, idx, layout), self.h, "set_layout")
+
     def stats(self, idx: int) -> _lib.SceneStats:
         s = _lib.SceneStats()
         _check(self.L.sr_scene_stats(self.h, idx, C.byref(s)), self.h, "scene_stats")

@@ -36,6 +36,7 @@ SR_NOALLOC_SCRATCH_BYTES = 8 << 20
 SR_ADJ_FROZEN = 1
 SR_NOALLOC_MAX_PIXELS = 1 << 18
 SR_MAX_FLASHES = 16
+SR_LAYOUT_AUTO, SR_LAYOUT_OCTANT, SR_LAYOUT_COMPACT = 0, 1, 2
 
 # ---- packed layouts (gpu.rs:44-144) ------------------------------------------------------------
 NODE_DTYPE = np.dtype([("min", "<f4", 4), ("max", "<f4", 4), ("right_or_first", "<u4"), ("count", "<u4"),
@@ -131,7 +132,7 @@ class RenderOpts(C.Structure):
 class SceneStats(C.Structure):
     _fields_ = [("num_nodes", C.c_uint32), ("num_prims", C.c_uint32), ("num_stars", C.c_uint32),
                 ("bvh_depth", C.c_uint32), ("device_bytes", C.c_uint64), ("fast_nodes", C.c_uint32),
-                ("rindler_crossed", C.c_uint32)]
+                ("rindler_crossed", C.c_uint32), ("box_copies", C.c_uint32), ("pad", C.c_uint32)]
 
 
 class AdjointResult(C.Structure):
@@ -225,6 +226,7 @@ SIGNATURES = {
     "sr_update_scene": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(SceneDesc), C.POINTER(Range), C.c_uint32,
                                     C.POINTER(Range), C.c_uint32]),
     "sr_scene_stats": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(SceneStats)]),
+    "sr_set_layout": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "sr_render": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.c_void_p, C.c_uint64,
                               C.POINTER(Timings)]),
     "sr_render_ex": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(GpuUniforms), C.POINTER(RenderOpts),

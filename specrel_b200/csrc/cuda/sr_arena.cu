@@ -770,6 +770,7 @@ sr_status sr_arena_finish(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d, SrAre
     s.has_l2o = false;
     s.empty_tree = items.empty();
     s.rindler_crossed = a.stats.rindler_crossed != 0;
+    s.fast.layout = ctx->layout_of(idx);
     CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, depth, s.num_prims, max_leaf, st),
        "build node layout");
     if (!was_live) s.tuning = fast_default_tuning(ctx->fast);

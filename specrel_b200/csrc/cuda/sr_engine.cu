@@ -223,6 +223,7 @@ sr_status sr_upload_scene(sr_ctx* ctx, uint32_t idx, const SrSceneDesc* d) {
         s.light_pos[k] = d->light_pos[k];
         s.anchor[k] = d->anchor ? d->anchor[k] : 0.0;
     }
+    s.fast.layout = ctx->layout_of(idx);
     CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.num_nodes, depth, s.num_prims, max_leaf_of(d),
                   ctx->stream),
        "build node layout");
@@ -396,6 +397,7 @@ sr_status sr_build_scene(sr_ctx* ctx, uint32_t idx, const SrBuildDesc* d) {
         CK(cudaMemcpyAsync(box.p, d->boxes, (size_t)n * 32, cudaMemcpyHostToDevice, st), "upload boxes");
         CK(cudaMemcpyAsync(gin.p, d->geoms, (size_t)n * sizeof(SrGpuGeom), cudaMemcpyHostToDevice, st), "upload geoms");
         CK(cudaMemcpyAsync(ain.p, d->attrs, (size_t)n * sizeof(SrGpuAttr), cudaMemcpyHostToDevice, st), "upload attrs");
+        slot->fast.layout = ctx->layout_of(idx);
         r = finish_build(ctx, *slot, box.as<float4>(), gin.as<SrGpuGeom>(), ain.as<SrGpuAttr>(), n, st);
         if (r != SR_OK) return r;
     }
@@ -436,6 +438,7 @@ sr_status sr_build_scene_tubes(sr_ctx* ctx, uint32_t idx, const SrTube* tubes, u
     } free_ex{&ex, st};
     CK(e, "extrude");
     if (ex.num_prims == 0) return fail(ctx, SR_ERR_INVALID_ARGUMENT, "the tubes hold no simplices");
+    slot->fast.layout = ctx->layout_of(idx);
     r = finish_build(ctx, *slot, ex.boxes, ex.geoms, ex.attrs, ex.num_prims, st);
     if (r != SR_OK) return r;
     slot->rindler_crossed = ex.rindler_bad != 0;
@@ -483,6 +486,21 @@ sr_status sr_scene_stats(const sr_ctx* ctx, uint32_t idx, SrSceneStats* o) {
     o->device_bytes = s.nodes.bytes + s.geoms.bytes + s.attrs.bytes + s.mats.bytes + s.stars.bytes + s.l2o.bytes + s.fast.bytes();
     o->fast_nodes = s.fast.num_wide;
     o->rindler_crossed = s.rindler_crossed ? 1u : 0u;
+    o->box_copies = s.fast.num_wide ? s.fast.copies : 0u;
+    return SR_OK;
+}
+
+sr_status sr_set_layout(sr_ctx* ctx, uint32_t idx, uint32_t layout) {
+    if (!ctx || layout > SR_LAYOUT_COMPACT || idx > 4096) return SR_ERR_INVALID_ARGUMENT;
+    if (ctx->layouts.size() <= idx) ctx->layouts.resize(idx + 1, SR_LAYOUT_AUTO);
+    ctx->layouts[idx] = layout;
+    if (idx >= ctx->scenes.size() || !ctx->scenes[idx] || !ctx->scenes[idx]->present) return SR_OK;
+    SceneSlot& s = *ctx->scenes[idx];
+    CK(cudaSetDevice(ctx->device), "set device");
+    s.fast.layout = layout;
+    CK(fast_build(ctx->fast, s.fast, s.nodes.as<SrGpuNode>(), s.empty_tree ? 0u : s.num_nodes, s.depth, s.num_prims,
+                  s.fast.max_leaf, ctx->stream),
+       "rebuild node layout");
     return SR_OK;
 }
 
@@ -794,7 +812,10 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
     // stack in local memory or its first 8..16 entries in shared memory.
     const uint32_t shapes[][2] = {{128, 8}, {128, 11}, {256, 4}, {256, 6}, {512, 3}};
     const uint32_t tiles[][2] = {{8, 4}, {4, 8}};
-    const uint32_t stacks[] = {0, 8, 10, 12, 16};
+    // With the stack in local memory or 12 entries in shared memory, also the top 4, 6 or 8 levels
+    // of the tree staged in shared memory.
+    const uint32_t stacks[][2] = {{0, 0}, {8, 0}, {10, 0}, {12, 0}, {16, 0}, {0, 4}, {0, 6}, {0, 8},
+                                  {12, 4}, {12, 6}, {12, 8}};
     std::vector<SrTuning> cand;
     for (auto& sh : shapes)
         for (auto& tl : tiles)
@@ -809,8 +830,8 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
                 t.leaf_coop = v == 0 ? 1u : 0u;
                 t.leaf_batch = 1;
                 t.home_pct = 0;
-                t.stack_smem = v == 0 ? 0u : stacks[v - 1];
-                t.top_levels = 0;
+                t.stack_smem = v == 0 ? 0u : stacks[v - 1][0];
+                t.top_levels = v == 0 ? 0u : stacks[v - 1][1];
                 if (fast_tuning_valid(ctx->fast, t)) cand.push_back(t);
             }
     for (const SrTuning& t : cand) {

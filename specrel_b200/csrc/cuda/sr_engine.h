@@ -79,6 +79,8 @@ struct sr_ctx {
     cudaEvent_t ev[8] = {};
     srk::FastCtx fast;
     sre::AsyncOutput async;
+    std::vector<uint32_t> layouts;  // per scene index: SR_LAYOUT_* (default SR_LAYOUT_AUTO)
+    uint32_t layout_of(uint32_t idx) const { return idx < layouts.size() ? layouts[idx] : SR_LAYOUT_AUTO; }
 };
 
 namespace sre {

@@ -31,35 +31,69 @@ using namespace srd;
 // ---------------------------------------------------------------------------------------------
 // Layout build.
 // ---------------------------------------------------------------------------------------------
-__global__ void k_wide_flags(const SrGpuNode* nodes, uint32_t n, uint32_t* flags) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) flags[i] = nodes[i].count == 0 ? 1u : 0u;
+// The internal nodes of the top TOP_LEVELS levels, breadth first, from an internal root (node 0):
+// topid[node] = its position + 1 (topid zeroed before), level_end[k] = nodes in levels 0..k. One
+// thread: at most TOP_NODES nodes, once per layout build.
+__global__ void k_top_levels(const SrGpuNode* nodes, uint32_t* topid, uint32_t* level_end) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    uint32_t q[TOP_NODES];
+    uint32_t m = 1, start = 0, end = 1;
+    q[0] = 0;
+    topid[0] = 1;
+    level_end[0] = 1;
+    for (uint32_t lv = 1; lv < TOP_LEVELS; ++lv) {
+        for (uint32_t i = start; i < end; ++i) {
+            const SrGpuNode& nd = nodes[q[i]];
+            const uint32_t c[2] = {nd.left, nd.right_or_first};
+            for (int k = 0; k < 2; ++k)
+                if (nodes[c[k]].count == 0 && m < TOP_NODES) {
+                    q[m] = c[k];
+                    topid[c[k]] = ++m;
+                }
+        }
+        start = end;
+        end = m;
+        level_end[lv] = m;
+    }
 }
 
-// One wide node: both children's boxes in each of the 16 sign-octant copies (near corner, far
-// corner; see WideScene) and the packed child references.
-__global__ void k_wide_fill(const SrGpuNode* nodes, uint32_t n, const uint32_t* wid, float4* boxes, size_t oct_stride,
-                            uint2* refs) {
+// Internal nodes below the top levels: they take the positions after the top levels' in the
+// reference's depth-first order.
+__global__ void k_wide_flags(const SrGpuNode* nodes, uint32_t n, const uint32_t* topid, uint32_t* flags) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flags[i] = nodes[i].count == 0 && topid[i] == 0 ? 1u : 0u;
+}
+
+__device__ __forceinline__ uint32_t wide_index(const uint32_t* topid, const uint32_t* wid, uint32_t n_top, uint32_t i) {
+    const uint32_t t = topid[i];
+    return t ? t - 1u : n_top + wid[i];
+}
+
+// One wide node: both children's boxes in each of the `copies` sign-octant copies (near corner,
+// far corner; see WideScene; copy 0 is the plain (min, max) layout) and the packed child references.
+__global__ void k_wide_fill(const SrGpuNode* nodes, uint32_t n, const uint32_t* topid, const uint32_t* wid,
+                            uint32_t n_top, float4* boxes, size_t oct_stride, uint32_t copies, uint2* refs) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || nodes[i].count != 0) return;
+    const uint32_t wi = wide_index(topid, wid, n_top, i);
     const SrGpuNode& nd = nodes[i];
     uint32_t c[2] = {nd.left, nd.right_or_first}, ref[2];
     for (int k = 0; k < 2; ++k) {
         const SrGpuNode& ch = nodes[c[k]];
-        for (uint32_t oct = 0; oct < 16; ++oct) {
+        for (uint32_t oct = 0; oct < copies; ++oct) {
             float nr[4], fr[4];
             for (int a = 0; a < 4; ++a) {
                 const bool neg = (oct >> a) & 1u;
                 nr[a] = neg ? ch.max[a] : ch.min[a];
                 fr[a] = neg ? ch.min[a] : ch.max[a];
             }
-            float4* b = boxes + oct * oct_stride + 4ull * wid[i];
+            float4* b = boxes + oct * oct_stride + 4ull * wi;
             b[2 * k] = make_float4(nr[0], nr[1], nr[2], nr[3]);
             b[2 * k + 1] = make_float4(fr[0], fr[1], fr[2], fr[3]);
         }
-        ref[k] = ch.count > 0 ? pack_leaf(ch.right_or_first, ch.count) : wid[c[k]];
+        ref[k] = ch.count > 0 ? pack_leaf(ch.right_or_first, ch.count) : wide_index(topid, wid, n_top, c[k]);
     }
-    refs[wid[i]] = make_uint2(ref[0], ref[1]);
+    refs[wi] = make_uint2(ref[0], ref[1]);
 }
 
 static cudaError_t lean_kernel_attrs(int max_smem);
@@ -95,6 +129,7 @@ cudaError_t fast_build(FastCtx& c, FastScene& s, const SrGpuNode* nodes, uint32_
     s.num_wide = 0;
     s.depth = depth;
     s.empty = n == 0;
+    s.max_leaf = max_leaf;
     s.usable = depth <= FAST_MAX_DEPTH && num_prims < MAX_PACKED_PRIMS && max_leaf <= MAX_LEAF_PRIMS;
     if (n == 0 || !s.usable) return cudaSuccess;
     SrGpuNode root;
@@ -110,25 +145,44 @@ cudaError_t fast_build(FastCtx& c, FastScene& s, const SrGpuNode* nodes, uint32_
         s.root_ref = pack_leaf(root.right_or_first, root.count);
         return cudaSuccess;
     }
-    s.root_ref = 0;  // internal root: wide node 0 (depth-first order)
+    s.root_ref = 0;  // internal root: wide node 0 (the top levels come first)
     size_t temp = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, temp, (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)n, st);
-    if ((e = s.scratch.ensure(2 * (size_t)n * 4 + temp + 512)) != cudaSuccess) return e;
+    if ((e = s.scratch.ensure(3 * (size_t)n * 4 + 64 + temp + 512)) != cudaSuccess) return e;
     uint32_t* flags = s.scratch.as<uint32_t>();
     uint32_t* wid = flags + n;
-    uintptr_t tp = reinterpret_cast<uintptr_t>(wid + n);
+    uint32_t* topid = wid + n;
+    uint32_t* level_end = topid + n;  // 16 words after topid
+    uintptr_t tp = reinterpret_cast<uintptr_t>(level_end + 16);
     void* tmp = reinterpret_cast<void*>((tp + 255) & ~uintptr_t(255));
-    k_wide_flags<<<(n + 255) / 256, 256, 0, st>>>(nodes, n, flags);
+    if ((e = cudaMemsetAsync(topid, 0, (size_t)n * 4 + 64, st)) != cudaSuccess) return e;
+    k_top_levels<<<1, 1, 0, st>>>(nodes, topid, level_end);
+    k_wide_flags<<<(n + 255) / 256, 256, 0, st>>>(nodes, n, topid, flags);
     if ((e = cub::DeviceScan::ExclusiveSum(tmp, temp, flags, wid, (int)n, st)) != cudaSuccess) return e;
     uint32_t last[2] = {0, 0};
     cudaMemcpyAsync(&last[0], wid + n - 1, 4, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(&last[1], flags + n - 1, 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(s.top_end, level_end, sizeof(s.top_end), cudaMemcpyDeviceToHost, st);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-    s.num_wide = last[0] + last[1];
-    if ((e = s.boxes.ensure_grow((size_t)s.num_wide * 64 * 16)) != cudaSuccess) return e;
+    const uint32_t n_top = s.top_end[TOP_LEVELS - 1];
+    s.num_wide = n_top + last[0] + last[1];
+    // Box copies: 16 sign-octant copies, or one (the compact layout) when asked for, or when the
+    // 15 extra copies would take more than an eighth of the device or not fit in free memory.
+    const uint32_t before = s.copies;
+    s.copies = 16;
+    if (s.layout == SR_LAYOUT_COMPACT) {
+        s.copies = 1;
+    } else if (s.layout == SR_LAYOUT_AUTO) {
+        size_t free_b = 0, total_b = 0;
+        if ((e = cudaMemGetInfo(&free_b, &total_b)) != cudaSuccess) return e;
+        const size_t one = (size_t)s.num_wide * 64;
+        if (15 * one > total_b / 8 || 16 * one > free_b + s.boxes.bytes) s.copies = 1;
+    }
+    if (before && before != s.copies) s.boxes.release();  // a layout change does not keep the old size
+    if ((e = s.boxes.ensure_grow((size_t)s.num_wide * 64 * s.copies)) != cudaSuccess) return e;
     if ((e = s.refs.ensure_grow((size_t)s.num_wide * 8)) != cudaSuccess) return e;
-    k_wide_fill<<<(n + 255) / 256, 256, 0, st>>>(nodes, n, wid, s.boxes.as<float4>(), 4ull * s.num_wide,
-                                                 s.refs.as<uint2>());
+    k_wide_fill<<<(n + 255) / 256, 256, 0, st>>>(nodes, n, topid, wid, n_top, s.boxes.as<float4>(), 4ull * s.num_wide,
+                                                 s.copies, s.refs.as<uint2>());
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     e = cudaStreamSynchronize(st);
     s.scratch.ensure(0);
@@ -156,8 +210,9 @@ bool fast_tuning_valid(const FastCtx& c, const SrTuning& t) {
     return bt && t.blocks_per_sm >= 1 && t.blocks_per_sm <= 16 && t.tile_w >= 1 && t.tile_w * t.tile_h == 32 &&
            t.chunk_tiles >= 1 && t.chunk_tiles <= 64 && t.refill_lanes >= 1 && t.refill_lanes <= 32 &&
            t.leaf_coop <= 1 && t.leaf_batch >= 1 && t.leaf_batch <= 32 && t.home_pct <= 100 &&
-           lean_stack_supported(t.stack_smem) && stack_bytes <= (size_t)c.max_smem && t.top_levels == 0 &&
-           t.reserved == 0;
+           lean_stack_supported(t.stack_smem) && t.top_levels <= TOP_LEVELS &&
+           (t.top_levels == 0 || t.stack_smem == 0 || t.stack_smem == 12) &&
+           stack_bytes + (t.top_levels ? ((size_t)1 << t.top_levels) * 72u : 0u) <= (size_t)c.max_smem && t.reserved == 0;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -221,6 +276,7 @@ struct TraceBatchArgs {
     uint32_t chunk_rays;    // rays a warp takes from the global counter at a time (a multiple of 32)
     uint32_t refill_lanes;  // idle lanes that make the warp fetch new rays
     uint32_t leaf_batch;    // lanes on a leaf before the warp tests leaves
+    uint32_t top_n;         // lean kernel: wide nodes staged in shared memory (the top levels)
     // Lean kernel tile order: SM band b holds tiles [b * band_tiles, (b + 1) * band_tiles) and is
     // taken through sched[b]; the shared pool, tiles [num_bands * band_tiles, total), through
     // sched[num_bands].
@@ -596,8 +652,11 @@ __device__ __forceinline__ uint32_t next_tile(const TraceBatchArgs& a, uint32_t 
 }
 
 // SS > 0: the first SS entries of each thread's traversal stack live in dynamic shared memory
-// (SplitStack), the rest in local memory; SS == 0: all in local memory (LocalStack).
-template <bool COUNT, int SS>
+// (SplitStack), the rest in local memory; SS == 0: all in local memory (LocalStack). OCT: the
+// scene has the 16 sign-octant box copies; otherwise the compact layout (one copy). TOP: the first
+// a.top_n wide nodes (the tree's top levels) are staged in shared memory after the stacks, their
+// (min, max) boxes then their references.
+template <bool COUNT, int SS, bool OCT, bool TOP>
 __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
     const uint32_t lane = threadIdx.x & 31u;
     Work wp{0, 0, 0}, wsh{0, 0, 0};
@@ -607,6 +666,15 @@ __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
     Stack st;
     if constexpr (SS > 0) st = SplitStack<SS>{sm_stack + threadIdx.x * SplitStack<SS>::ROW, lm};
     else st = LocalStack{lm};
+    TopStage top{nullptr, nullptr, 0u};
+    if constexpr (TOP) {
+        float4* tb = reinterpret_cast<float4*>(sm_stack + (SS > 0 ? blockDim.x * (uint32_t)SplitStack<SS>::ROW : 0u));
+        uint2* tr = reinterpret_cast<uint2*>(tb + 4u * a.top_n);
+        for (uint32_t i = threadIdx.x; i < 4u * a.top_n; i += blockDim.x) tb[i] = __ldg(a.ws.boxes + i);  // copy 0: (min, max)
+        for (uint32_t i = threadIdx.x; i < a.top_n; i += blockDim.x) tr[i] = __ldg(a.ws.refs + i);
+        __syncthreads();
+        top = TopStage{tb, tr, a.top_n};
+    }
     const uint32_t home = a.num_bands ? sm_id() % a.num_bands : 0u;
     uint32_t stage = a.num_bands ? 0u : 1u, steal = 0;
     for (;;) {
@@ -631,7 +699,8 @@ __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
             float en, ex;
             slab_interval(a.ws.root_min, a.ws.root_max, no, inv, 1e-3f, t_max, &en, &ex);
             if (ex >= en && en < t_max)  // else the ray misses the scene's box (bvh4d.rs:451)
-                slot = closest_lean<COUNT>(a.ws, a.ws.root_ref, no, d, inv, 1e-3f, t_max, best, st, a.err, wp);
+                slot = closest_lean<COUNT, OCT, TOP>(a.ws, a.ws.root_ref, no, d, inv, 1e-3f, t_max, best, st, a.err, wp,
+                                                     top);
         }
         a.hits[pix] = make_float4(best.lambda, best.u, best.v, best.w);
         a.slots[pix] = slot < 0 ? 0xFFFFFFFFu : (uint32_t)slot;
@@ -653,7 +722,9 @@ __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
                     const float s0 = 2e-3f, s1 = dist - 2e-3f;
                     float en, ex;
                     slab_interval(a.ws.root_min, a.ws.root_max, neg4(ev), sinv, s0, s1, &en, &ex);
-                    if (ex >= en && any_lean<COUNT>(a.ws, a.ws.root_ref, neg4(ev), tl, sinv, s0, s1, st, a.err, wsh)) sh = 2;
+                    if (ex >= en && any_lean<COUNT, OCT, TOP>(a.ws, a.ws.root_ref, neg4(ev), tl, sinv, s0, s1, st, a.err,
+                                                              wsh, top))
+                        sh = 2;
                 }
             }
         }
@@ -675,26 +746,62 @@ bool lean_stack_supported(uint32_t s) {
     return false;
 }
 
-// The shared-memory stack of the lean kernel can exceed the 48 KB default of one block.
+// The shared-memory stack and the staged top levels of the lean kernel can exceed the 48 KB
+// default of one block.
+template <bool COUNT, int SS, bool OCT, bool TOP>
+static cudaError_t lean_attr(int max_smem) {
+    return SS > 0 || TOP
+               ? cudaFuncSetAttribute(k_trace_lean<COUNT, SS, OCT, TOP>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)
+               : cudaSuccess;
+}
+
+template <int SS>
+static cudaError_t lean_attrs_ss(int max_smem) {
+    cudaError_t e = lean_attr<false, SS, true, false>(max_smem);
+    if (e == cudaSuccess) e = lean_attr<true, SS, true, false>(max_smem);
+    if (e == cudaSuccess) e = lean_attr<false, SS, false, false>(max_smem);
+    if (e == cudaSuccess) e = lean_attr<true, SS, false, false>(max_smem);
+    if constexpr (SS == 0 || SS == 12) {  // the depths built with staged top levels (octant layout)
+        if (e == cudaSuccess) e = lean_attr<false, SS, true, true>(max_smem);
+        if (e == cudaSuccess) e = lean_attr<true, SS, true, true>(max_smem);
+    }
+    return e;
+}
+
 static cudaError_t lean_kernel_attrs(int max_smem) {
     cudaError_t e = cudaSuccess;
-#define SR_ONE(S)                                                                                                  \
-    if (e == cudaSuccess && (S) > 0)                                                                               \
-        e = cudaFuncSetAttribute(k_trace_lean<false, (S)>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem); \
-    if (e == cudaSuccess && (S) > 0)                                                                               \
-        e = cudaFuncSetAttribute(k_trace_lean<true, (S)>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+#define SR_ONE(S) \
+    if (e == cudaSuccess) e = lean_attrs_ss<(S)>(max_smem);
     SR_LEAN_STACKS(SR_ONE)
 #undef SR_ONE
     return e;
 }
 
-static void launch_lean(uint32_t ss, bool count, uint32_t blocks, uint32_t threads, size_t smem, cudaStream_t st,
-                        const TraceBatchArgs& ta) {
-#define SR_ONE(S)                                                                         \
-    if (ss == (S)) {                                                                      \
-        if (count) k_trace_lean<true, (S)><<<blocks, threads, smem, st>>>(ta);           \
-        else k_trace_lean<false, (S)><<<blocks, threads, smem, st>>>(ta);                \
-        return;                                                                           \
+template <int SS>
+static void launch_lean_ss(bool count, bool oct, bool top, uint32_t blocks, uint32_t threads, size_t smem, cudaStream_t st,
+                           const TraceBatchArgs& ta) {
+    if constexpr (SS == 0 || SS == 12) {
+        if (top && oct) {
+            if (count) k_trace_lean<true, SS, true, true><<<blocks, threads, smem, st>>>(ta);
+            else k_trace_lean<false, SS, true, true><<<blocks, threads, smem, st>>>(ta);
+            return;
+        }
+    }
+    if (oct) {
+        if (count) k_trace_lean<true, SS, true, false><<<blocks, threads, smem, st>>>(ta);
+        else k_trace_lean<false, SS, true, false><<<blocks, threads, smem, st>>>(ta);
+    } else {
+        if (count) k_trace_lean<true, SS, false, false><<<blocks, threads, smem, st>>>(ta);
+        else k_trace_lean<false, SS, false, false><<<blocks, threads, smem, st>>>(ta);
+    }
+}
+
+static void launch_lean(uint32_t ss, bool count, bool oct, bool top, uint32_t blocks, uint32_t threads, size_t smem,
+                        cudaStream_t st, const TraceBatchArgs& ta) {
+#define SR_ONE(S)                                                             \
+    if (ss == (S)) {                                                          \
+        launch_lean_ss<(S)>(count, oct, top, blocks, threads, smem, st, ta);  \
+        return;                                                               \
     }
     SR_LEAN_STACKS(SR_ONE)
 #undef SR_ONE
@@ -943,6 +1050,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
                                                      anchor[0], anchor[1], anchor[2], anchor[3], c.cam.as<float4>());
         if (timed) cudaEventRecord(r.ev[0], st);
         TraceBatchArgs ta;
+        ta.top_n = 0;
         ta.ws = ws;
         ta.attrs = sd.attrs;
         ta.mats = sd.mats;
@@ -973,8 +1081,11 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
         const size_t smem = t.leaf_coop ? (size_t)(t.block_threads / 32) * COOP_SMEM_PER_WARP : 0;
         const bool lean = !t.leaf_coop && t.leaf_batch == 1 && t.refill_lanes == 32 && t.chunk_tiles == 1;
         if (lean) {
-            const size_t ssm = lean_stack_bytes(t);
-            launch_lean(t.stack_smem, r.count_work, blocks, t.block_threads, ssm, st, ta);
+            // Staged top levels need the octant layout (the compact layout's kernels stage none).
+            const bool oct = s.copies == 16, top = oct && t.top_levels > 0;
+            ta.top_n = top ? s.top_end[t.top_levels - 1] : 0u;
+            const size_t ssm = lean_stack_bytes(t) + (size_t)ta.top_n * 72u;
+            launch_lean(t.stack_smem, r.count_work, oct, top, blocks, t.block_threads, ssm, st, ta);
         } else if (t.leaf_coop) {
             if (r.count_work) k_trace_batch<true, true><<<blocks, t.block_threads, smem, st>>>(ta);
             else k_trace_batch<false, true><<<blocks, t.block_threads, smem, st>>>(ta);

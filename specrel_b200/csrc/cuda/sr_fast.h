@@ -33,6 +33,11 @@ struct DevMem {
         if (n <= bytes && p) return cudaSuccess;
         return ensure(p ? std::max(n, bytes + bytes / 4) : n);
     }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
     template <class T> T* as() const { return reinterpret_cast<T*>(p); }
 };
 
@@ -62,6 +67,10 @@ struct FastScene {
     uint32_t root_ref = 0;
     bool empty = true;
     bool usable = false;  // false: the scene renders on the plain path (see fast_build)
+    uint32_t layout = 0;  // SR_LAYOUT_* preference for the next build
+    uint32_t copies = 0;  // box copies built: 16 (one per sign octant) or 1 (compact)
+    uint32_t max_leaf = 0;  // most primitives in a leaf, as the last build saw
+    uint32_t top_end[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // wide nodes in the top k + 1 levels (breadth-first prefix)
     float root_min[4] = {0, 0, 0, 0}, root_max[4] = {0, 0, 0, 0};
     size_t bytes() const { return boxes.bytes + refs.bytes; }
 };

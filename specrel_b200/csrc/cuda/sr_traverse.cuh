@@ -8,7 +8,8 @@
 // A packed reference is either a leaf, bit 31 set, bits 25..30 the primitive count (1..63) and
 // bits 0..24 the first hot record; or an internal child, bit 31 clear, its wide-node index.
 // Boxes are 64-byte aligned, so one traversal step reads half a cache line plus 8 bytes instead
-// of the reference's three 48-byte node loads.
+// of the reference's three 48-byte node loads. Numbering: the internal nodes of the top
+// TOP_LEVELS levels first, breadth first, then the others in the reference's depth-first order.
 //
 // Traversal order: near child first, the far child pushed only when both are hit, with the
 // reference's culling (skip a node whose entry parameter is >= the closest hit so far). This is
@@ -35,6 +36,11 @@ constexpr uint32_t MAX_PACKED_PRIMS = 1u << REF_COUNT_SHIFT;
 constexpr uint32_t FAST_MAX_DEPTH = 60;
 constexpr uint32_t MAX_VISITS_FAST = 1u << 22;
 constexpr int FAST_STACK = 64;
+// The wide nodes of the tree's top TOP_LEVELS levels come first, level by level (breadth first),
+// so the top K levels are the prefix [0, top_end[K - 1]) for every K <= TOP_LEVELS; the lean
+// kernel can stage such a prefix in shared memory (SrTuning::top_levels).
+constexpr uint32_t TOP_LEVELS = 8;
+constexpr uint32_t TOP_NODES = (1u << TOP_LEVELS) - 1u;
 
 __host__ __device__ __forceinline__ uint32_t pack_leaf(uint32_t first, uint32_t count) {
     return REF_LEAF | (count << REF_COUNT_SHIFT) | first;
@@ -327,10 +333,21 @@ struct SplitStack {
 // the longest leaf of the warp. A leaf in progress is its packed reference with the tested
 // primitives taken off the front. Each ray's own sequence of node visits and tests, and so its
 // result, is the same.
-template <bool COUNT, class Stack>
+// The top levels of the tree staged in shared memory: wide nodes [0, n) with their (min, max)
+// boxes and packed references.
+struct TopStage {
+    const float4* boxes;
+    const uint2* refs;
+    uint32_t n;
+};
+
+// OCT: the scene has the 16 sign-octant box copies (else the compact layout, one (min, max)
+// copy). TOP: nodes below top.n are read from the shared-memory stage.
+template <bool COUNT, bool OCT, bool TOP, class Stack>
 __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, float4 no, float4 d, float4 inv, float t_min,
-                                            float& t_max, GeomHit& best, const Stack& st, uint32_t* err, Work& work) {
-    const float4* ob = octant_boxes(s, inv);
+                                            float& t_max, GeomHit& best, const Stack& st, uint32_t* err, Work& work,
+                                            const TopStage& top) {
+    const float4* ob = OCT ? octant_boxes(s, inv) : s.boxes;
     int slot = -1, sp = 0;
     uint32_t visits = 0;
     // The largest float below t_max (t_max > t_min > 0): with it as the exit bound, exit >= entry
@@ -359,12 +376,25 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
                 break;
             }
             if (COUNT) ++work.nodes;
-            const float4* b = ob + 4ull * cur;
-            const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
-            const uint2 r = __ldg(s.refs + cur);
             float enl, exl, enr, exr;
-            slab_octant(lnear, lfar, no, inv, t_min, t_below, &enl, &exl);
-            slab_octant(rnear, rfar, no, inv, t_min, t_below, &enr, &exr);
+            uint2 r;
+            if (TOP && cur < top.n) {  // a staged node: (min, max) boxes in shared memory
+                const float4* b = top.boxes + 4u * cur;
+                r = top.refs[cur];
+                slab_interval(b[0], b[1], no, inv, t_min, t_below, &enl, &exl);
+                slab_interval(b[2], b[3], no, inv, t_min, t_below, &enr, &exr);
+            } else {
+                const float4* b = ob + 4ull * cur;
+                const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
+                r = __ldg(s.refs + cur);
+                if (OCT) {
+                    slab_octant(lnear, lfar, no, inv, t_min, t_below, &enl, &exl);
+                    slab_octant(rnear, rfar, no, inv, t_min, t_below, &enr, &exr);
+                } else {  // compact layout: (min, max) boxes
+                    slab_interval(lnear, lfar, no, inv, t_min, t_below, &enl, &exl);
+                    slab_interval(rnear, rfar, no, inv, t_min, t_below, &enr, &exr);
+                }
+            }
             const bool hl = exl >= enl;  // and enl < t_max
             const bool hr = exr >= enr;
             if (hl && hr) {
@@ -399,10 +429,10 @@ __device__ __forceinline__ int closest_lean(const WideScene& s, uint32_t cur, fl
 // Any hit in (t_min, t_max) from node `cur` (the root, already tested): left before right, no
 // culling (Bvh4D::is_occluded, bvh4d.rs:523-578). (The answer does not depend on the order;
 // nearer-first measured 7% slower on the 7.9M-tet scene.)
-template <bool COUNT, class Stack>
+template <bool COUNT, bool OCT, bool TOP, class Stack>
 __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float4 no, float4 d, float4 inv, float t_min,
-                                         float t_max, const Stack& st, uint32_t* err, Work& work) {
-    const float4* ob = octant_boxes(s, inv);
+                                         float t_max, const Stack& st, uint32_t* err, Work& work, const TopStage& top) {
+    const float4* ob = OCT ? octant_boxes(s, inv) : s.boxes;
     int sp = 0;
     uint32_t visits = 0;
     if (COUNT && (cur & REF_LEAF)) ++work.leaves;
@@ -419,12 +449,25 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
                 return false;
             }
             if (COUNT) ++work.nodes;
-            const float4* b = ob + 4ull * cur;
-            const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
-            const uint2 r = __ldg(s.refs + cur);
             float enl, exl, enr, exr;
-            slab_octant(lnear, lfar, no, inv, t_min, t_max, &enl, &exl);
-            slab_octant(rnear, rfar, no, inv, t_min, t_max, &enr, &exr);
+            uint2 r;
+            if (TOP && cur < top.n) {
+                const float4* b = top.boxes + 4u * cur;
+                r = top.refs[cur];
+                slab_interval(b[0], b[1], no, inv, t_min, t_max, &enl, &exl);
+                slab_interval(b[2], b[3], no, inv, t_min, t_max, &enr, &exr);
+            } else {
+                const float4* b = ob + 4ull * cur;
+                const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
+                r = __ldg(s.refs + cur);
+                if (OCT) {
+                    slab_octant(lnear, lfar, no, inv, t_min, t_max, &enl, &exl);
+                    slab_octant(rnear, rfar, no, inv, t_min, t_max, &enr, &exr);
+                } else {
+                    slab_interval(lnear, lfar, no, inv, t_min, t_max, &enl, &exl);
+                    slab_interval(rnear, rfar, no, inv, t_min, t_max, &enr, &exr);
+                }
+            }
             const bool hl = exl >= enl, hr = exr >= enr;
             if (hl && hr) {
                 if (sp < FAST_STACK) st.put_ref(sp++, r.y);

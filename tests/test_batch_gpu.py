@@ -214,3 +214,72 @@ def test_async_output_overlaps_and_equals_the_blocking_batch(engine, scene):
     with pytest.raises(sr.SrError):
         engine.render_batch(3, us, outs[0].data_ptr(), total, cams=cams, device_output=False, async_output=True,
                             timing=True)
+
+
+@pytest.mark.parametrize("stack", [0, 12])
+def test_compact_layout_gives_the_same_frames_and_visits(engine, scene, stack):
+    """The compact node layout (one copy of the child boxes instead of 16 sign-octant copies) gives
+    the same frames and visits the same nodes; it takes 15 x 64 bytes less per internal node."""
+    from specrel_b200 import _lib as L
+    obs, us, cams = _observers(15, 4, int(scene.info.n_nodes), scale=4)
+    keep = engine.tuning(3)
+    t = engine.tuning(3)
+    t.tile_w, t.tile_h, t.chunk_tiles, t.refill_lanes, t.leaf_coop, t.leaf_batch, t.home_pct = 4, 8, 1, 32, 0, 1, 0
+    t.stack_smem, t.top_levels = stack, 0
+    cam = sr.camera((0.0, 0.0, 0.0, -10.0), 90.0, rapidity=(0.3, 0.1, -0.2))
+    u = sr.uniforms(cam, 256, 160, 0, 0, 0, num_nodes=int(scene.info.n_nodes))
+    engine.set_tuning(3, t)
+    try:
+        wide = engine.stats(3)
+        assert wide.box_copies == 16
+        ref = _batch(engine, 3, us, cams)
+        ref_work = engine.render(3, u, count=True).timings
+        engine.set_layout(3, L.SR_LAYOUT_COMPACT)
+        compact = engine.stats(3)
+        assert compact.box_copies == 1 and compact.fast_nodes == wide.fast_nodes
+        assert wide.device_bytes - compact.device_bytes == 15 * 64 * wide.fast_nodes
+        out = _batch(engine, 3, us, cams)
+        work = engine.render(3, u, count=True).timings
+    finally:
+        engine.set_layout(3, L.SR_LAYOUT_AUTO)
+        engine.set_tuning(3, keep)
+    assert engine.stats(3).box_copies == 16
+    assert (out == ref).all()
+    assert (work.nodes_visited, work.tets_tested, work.leaves_visited) == \
+        (ref_work.nodes_visited, ref_work.tets_tested, ref_work.leaves_visited)
+
+
+@pytest.mark.parametrize("stack,top", [(0, 4), (0, 8), (12, 6), (12, 8)])
+def test_staged_top_levels_give_the_same_frames_and_visits(engine, scene, stack, top):
+    """The top `top` levels of the tree read from shared memory (staged per block) instead of
+    global memory: the plain path's frames and the oracle's node visits, unchanged."""
+    keep = engine.tuning(3)
+    t = engine.tuning(3)
+    t.tile_w, t.tile_h, t.chunk_tiles, t.refill_lanes, t.leaf_coop, t.leaf_batch, t.home_pct = 4, 8, 1, 32, 0, 1, 0
+    t.block_threads, t.blocks_per_sm, t.stack_smem, t.top_levels = 128, 8, stack, top
+    engine.set_tuning(3, t)
+    try:
+        obs, us, cams = _observers(16, 4, int(scene.info.n_nodes), scale=4)
+        out = _batch(engine, 3, us, cams)
+        cam = sr.camera((0.0, 0.0, 0.0, -10.0), 90.0, rapidity=(0.3, 0.1, -0.2))
+        u = sr.uniforms(cam, 256, 160, 0, 0, 0, num_nodes=int(scene.info.n_nodes))
+        fr = engine.render(3, u, count=True)
+    finally:
+        engine.set_tuning(3, keep)
+    off = 0  # the batch's frames have shadows on: shadow rays read the staged levels too
+    for u_, c in zip(us, cams):
+        n = u_.size[0] * u_.size[1]
+        assert (out[off:off + n] == engine.render(3, u_, path=sr.SR_PATH_PLAIN, cam=c).rgb).all()
+        off += n
+    base = O.render(scene, O.make_camera(pos=(0.0, 0.0, 0.0, -10.0), rapidity=(0.3, 0.1, -0.2)),
+                    O.make_config(256, 160), stats=True)
+    assert fr.timings.nodes_visited == int(base.stats[:, 0].sum())
+    assert fr.timings.tets_tested == int(base.stats[:, 2].sum())
+
+
+def test_invalid_top_levels_rejected(engine, scene):
+    for stack, top in ((8, 4), (0, 9), (16, 2)):
+        t = engine.tuning(3)
+        t.stack_smem, t.top_levels = stack, top
+        with pytest.raises(sr.SrError):
+            engine.set_tuning(3, t)
