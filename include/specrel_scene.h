@@ -44,7 +44,18 @@ typedef struct SrSynthInfo {
     double cam_rapidity[3];  /* the workload's observer rapidity */
     double anchor[4];        /* FP64 anchor of the f32 coordinates */
     double build_seconds;
+    uint32_t median_splits;  /* nodes split at the centroid median (bvh4d.rs:418-424): the SAH split
+                                left one side empty; sr_build_scene does not take such scenes */
+    uint32_t pad;
 } SrSynthInfo;
+
+/* Bvh4D::build (bvh4d.rs:123-141, 287-427) on the host from the simplices' boxes in build order (8
+ * floats each: min then max, (t, x, y, z)); centroids are the box centres. `nodes` (at least 2n - 1)
+ * receives the node array, `order` (n) the leaf order (leaf slot -> build index), `median_splits`
+ * (optional) the number of nodes split at the centroid median, which selects as Rust's
+ * slice::select_nth_unstable_by does. `threads`: worker threads for large subtrees. */
+sr_status sr_bvh_build_host(const float* boxes, uint32_t n, uint32_t threads, SrGpuNode* nodes, uint32_t nodes_cap,
+                            uint32_t* order, uint32_t* num_nodes, uint32_t* median_splits);
 
 /* Builds the workload (threads: params->threads). */
 sr_status sr_scene_synth(const SrSynthParams* params, sr_scene** out, char* err, size_t errlen);

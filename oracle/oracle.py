@@ -36,7 +36,8 @@ class SceneInfo(C.Structure):
                 ("n_star_vec4", C.c_uint64), ("n_materials", C.c_uint64), ("depth", C.c_uint32),
                 ("rindler_ok", C.c_int32), ("superluminal", C.c_int32), ("clamped_accel", C.c_uint32),
                 ("cam_pos", C.c_double * 4), ("cam_rapidity", C.c_double * 3),
-                ("bounds_min", C.c_double * 4), ("bounds_max", C.c_double * 4)]
+                ("bounds_min", C.c_double * 4), ("bounds_max", C.c_double * 4), ("median_splits", C.c_uint32),
+                ("pad", C.c_uint32)]
 
 
 class Camera(C.Structure):
@@ -97,6 +98,9 @@ def lib():
         L.orc_light_clock_bounce_fraction.argtypes = [C.c_float, C.c_float]
         L.orc_material.argtypes = [C.c_uint32, C.c_void_p]
         L.orc_tetrad_from_beta.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_bvh_from_boxes.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32),
+                                         C.POINTER(C.c_uint32)]
+        L.orc_select_nth.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32]
         L.orc_scene_pack.argtypes = [C.c_void_p] + [C.c_void_p] * 6
         L.orc_render.argtypes = [C.c_void_p, C.POINTER(Camera), C.POINTER(Config), C.POINTER(Dynamics),
                                  C.c_int, C.c_int, C.POINTER(PixelOut)]
@@ -235,6 +239,25 @@ def tetrad_from_beta(beta) -> np.ndarray:
     out = np.zeros(16)
     lib().orc_tetrad_from_beta(b.ctypes.data, out.ctypes.data)
     return out.reshape(4, 4).astype(np.float32)
+
+
+def bvh_from_boxes(boxes):
+    """Bvh4D::build over boxes (n x 8: min then max, (t, x, y, z)): (nodes, order, median splits)."""
+    b = np.ascontiguousarray(boxes, np.float32).reshape(-1, 8)
+    n = len(b)
+    nodes = np.zeros(max(1, 2 * n - 1), NODE_DTYPE)
+    order = np.zeros(max(1, n), np.uint32)
+    nn, med = C.c_uint32(), C.c_uint32()
+    lib().orc_bvh_from_boxes(b.ctypes.data, n, nodes.ctypes.data, order.ctypes.data, C.byref(nn), C.byref(med))
+    return nodes[:nn.value], order[:n], med.value
+
+
+def select_nth(keys, k):
+    """The oracle's slice::select_nth_unstable_by on float keys: (keys, original positions) after."""
+    v = np.ascontiguousarray(keys, np.float32).copy()
+    idx = np.arange(len(v), dtype=np.uint32)
+    lib().orc_select_nth(v.ctypes.data, idx.ctypes.data, len(v), k)
+    return v, idx
 
 
 def light_clock_bounce_fraction(proper_time: float, cavity_length: float) -> float:

@@ -31,6 +31,8 @@ struct OrcSceneInfo {
     double cam_pos[4];
     double cam_rapidity[3];
     double bounds_min[4], bounds_max[4];
+    uint32_t median_splits;  // nodes split at the centroid median (bvh4d.rs:418-424)
+    uint32_t pad;
 };
 
 struct OrcCamera {
@@ -207,6 +209,7 @@ template <class T> void info_t(const SynthOut<T>& s, OrcSceneInfo* o) {
     o->n_star_vec4 = s.scene.stars.size() + 3 * segs;
     o->n_materials = s.scene.materials.size();
     o->depth = s.scene.bvh.depth();
+    o->median_splits = s.scene.bvh.median_splits;
     o->rindler_ok = s.rindler_ok;
     o->superluminal = s.superluminal;
     o->clamped_accel = s.clamped_accel;
@@ -294,6 +297,48 @@ int orc_tetrad_from_beta(const double* beta3, double* out16) {
         out16[4 * a + 2] = t.e[a].y;
         out16[4 * a + 3] = t.e[a].z;
     }
+    return 0;
+}
+
+// Bvh4D::build over boxes (8 floats each: min then max, (t, x, y, z); centroids their centres),
+// as the tree of simplices with those boxes: the node array (2n - 1 GpuNode slots), the leaf order
+// and the number of median splits.
+int orc_bvh_from_boxes(const float* boxes, uint32_t n, void* nodes_out, uint32_t* order, uint32_t* n_nodes,
+                       uint32_t* median) {
+    using B = Bvh<float>;
+    std::vector<B::Ref> refs(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        Aabb<float> a;
+        a.min = V4<float>(boxes[8 * i], boxes[8 * i + 1], boxes[8 * i + 2], boxes[8 * i + 3]);
+        a.max = V4<float>(boxes[8 * i + 4], boxes[8 * i + 5], boxes[8 * i + 6], boxes[8 * i + 7]);
+        refs[i] = {a, a.center(), i};
+    }
+    std::vector<BvhNode<float>> nodes;
+    std::atomic<uint32_t> med{0};
+    if (n) B::build_recursive(nodes, refs.data(), n, 0, 6, &med);
+    auto* pn = (PNode*)nodes_out;
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        v4f(pn[i].min, nodes[i].aabb.min);
+        v4f(pn[i].max, nodes[i].aabb.max);
+        pn[i].right_or_first = nodes[i].right_or_first;
+        pn[i].count = nodes[i].count;
+        pn[i].left = nodes[i].left;
+        pn[i].pad = 0;
+    }
+    for (uint32_t i = 0; i < n; ++i) order[i] = refs[i].index;
+    *n_nodes = (uint32_t)nodes.size();
+    *median = med.load();
+    return 0;
+}
+
+// select_nth_unstable_by on floats (by value, `partial_cmp` order) carrying their indices: the
+// oracle's restatement of Rust's selection, for the tests.
+int orc_select_nth(float* keys, uint32_t* idx, uint32_t n, uint32_t k) {
+    struct KI { float key; uint32_t i; };
+    std::vector<KI> v(n);
+    for (uint32_t j = 0; j < n; ++j) v[j] = {keys[j], idx[j]};
+    select_nth_unstable(v.data(), n, k, [](const KI& a, const KI& b) { return a.key < b.key; });
+    for (uint32_t j = 0; j < n; ++j) { keys[j] = v[j].key; idx[j] = v[j].i; }
     return 0;
 }
 

@@ -18,6 +18,7 @@
 #include <utility>
 #include <vector>
 
+#include "oracle_select.hpp"
 #include "oracle_math.hpp"
 
 namespace orc {
@@ -469,6 +470,7 @@ template <class T> struct Bvh {
     std::vector<Geom<T>> hot;       // leaf order
     std::vector<uint32_t> order;    // leaf slot -> index into `simplices`
     std::vector<Simplex<T>> simplices;  // build order
+    uint32_t median_splits = 0;         // nodes split at the centroid median (bvh4d.rs:418-424)
 
     struct Ref { Aabb<T> aabb; V4<T> centroid; uint32_t index; };
 
@@ -479,10 +481,12 @@ template <class T> struct Bvh {
         size_t n = simplices.size();
         std::vector<Ref> refs(n);
         for (size_t i = 0; i < n; ++i) refs[i] = {simplices[i].aabb, simplices[i].aabb.center(), (uint32_t)i};
+        std::atomic<uint32_t> med{0};
         if (n > 0) {
             b.nodes.reserve(n);
-            build_recursive(b.nodes, refs.data(), refs.size(), 0);
+            build_recursive(b.nodes, refs.data(), refs.size(), 0, 6, &med);
         }
+        b.median_splits = med.load();
         b.order.resize(n);
         b.hot.resize(n);
         for (size_t i = 0; i < n; ++i) {
@@ -498,11 +502,11 @@ template <class T> struct Bvh {
     // first order (left subtree, then right), which gives the serial build's array exactly: the
     // two subtrees own disjoint ranges of `refs`.
     static uint32_t build_recursive(std::vector<BvhNode<T>>& nodes, Ref* refs, size_t count, size_t first,
-                                    int spawn_depth = 6) {
+                                    int spawn_depth, std::atomic<uint32_t>* med) {
         uint32_t node_idx = (uint32_t)nodes.size();
         Aabb<T> bounds;
         size_t mid;
-        bool leaf = !split(refs, count, &bounds, &mid);
+        bool leaf = !split(refs, count, &bounds, &mid, med);
         if (leaf) {
             BvhNode<T> nd;
             nd.aabb = bounds;
@@ -517,8 +521,8 @@ template <class T> struct Bvh {
         nodes.push_back(nd);
         if (spawn_depth > 0 && count >= 65536) {
             std::vector<BvhNode<T>> ln, rn;
-            auto fl = std::async(std::launch::async, [&] { build_recursive(ln, refs, mid, first, spawn_depth - 1); });
-            build_recursive(rn, refs + mid, count - mid, first + mid, spawn_depth - 1);
+            auto fl = std::async(std::launch::async, [&] { build_recursive(ln, refs, mid, first, spawn_depth - 1, med); });
+            build_recursive(rn, refs + mid, count - mid, first + mid, spawn_depth - 1, med);
             fl.get();
             const uint32_t lbase = node_idx + 1, rbase = lbase + (uint32_t)ln.size();
             for (auto* part : {&ln, &rn}) {
@@ -534,14 +538,14 @@ template <class T> struct Bvh {
             nodes[node_idx].right_or_first = rbase;
             return node_idx;
         }
-        build_recursive(nodes, refs, mid, first, 0);
-        uint32_t right_idx = build_recursive(nodes, refs + mid, count - mid, first + mid, 0);
+        build_recursive(nodes, refs, mid, first, 0, med);
+        uint32_t right_idx = build_recursive(nodes, refs + mid, count - mid, first + mid, 0, med);
         nodes[node_idx].right_or_first = right_idx;
         return node_idx;
     }
 
     // bvh4d.rs:307-427. Returns false for a leaf.
-    static bool split(Ref* refs, size_t count, Aabb<T>* bounds_out, size_t* mid_out) {
+    static bool split(Ref* refs, size_t count, Aabb<T>* bounds_out, size_t* mid_out, std::atomic<uint32_t>* med) {
         Aabb<T> bounds, cb;
         for (size_t i = 0; i < count; ++i) {
             bounds = bounds.unite(refs[i].aabb);
@@ -611,11 +615,12 @@ template <class T> struct Bvh {
         size_t mid = 0;
         for (size_t i = 0; i < count; ++i)
             if (refs[i].centroid.axis(best_axis) < best_split_pos) { std::swap(refs[i], refs[mid]); ++mid; }
-        if (mid == 0 || mid == count) {
+        if (mid == 0 || mid == count) {  // bvh4d.rs:418-424
             mid = count / 2;
-            std::nth_element(refs, refs + mid, refs + count, [best_axis](const Ref& a, const Ref& b) {
-                return a.centroid.axis(best_axis) < b.centroid.axis(best_axis);
+            select_nth_unstable(refs, count, mid, [best_axis](const Ref& a, const Ref& b) {
+                return a.centroid.axis(best_axis) < b.centroid.axis(best_axis);  // partial_cmp == Less
             });
+            if (med) med->fetch_add(1);
         }
         *mid_out = mid;
         return true;

@@ -157,7 +157,8 @@ class SynthParams(C.Structure):
 class SynthInfo(C.Structure):
     _fields_ = [("bvh_depth", C.c_uint32), ("rindler_ok", C.c_int32), ("clamped_accel", C.c_uint32),
                 ("max_leaf", C.c_uint32), ("cam_pos", C.c_double * 4), ("cam_rapidity", C.c_double * 3),
-                ("anchor", C.c_double * 4), ("build_seconds", C.c_double)]
+                ("anchor", C.c_double * 4), ("build_seconds", C.c_double), ("median_splits", C.c_uint32),
+                ("pad", C.c_uint32)]
 
 
 class ObserverDraw(C.Structure):
@@ -252,6 +253,8 @@ SIGNATURES = {
                                 C.POINTER(C.c_float)]),
     "sr_scene_synth": (C.c_int32, [C.POINTER(SynthParams), C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
     "sr_scene_free": (None, [C.c_void_p]),
+    "sr_bvh_build_host": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                      C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "sr_scene_desc": (C.c_int32, [C.c_void_p, C.POINTER(SceneDesc)]),
     "sr_scene_info": (C.c_int32, [C.c_void_p, C.POINTER(SynthInfo)]),
     "sr_observers_synth": (C.c_int32, [C.c_uint64, C.c_uint32, C.POINTER(ObserverDraw)]),

@@ -11,6 +11,7 @@
 // and BVH subtrees of at least 4096 primitives are built concurrently and spliced depth-first,
 // so the arrays are identical to a serial build's.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstring>
 #include <functional>
@@ -23,6 +24,7 @@
 
 #include "../../../include/specrel_scene.h"
 #include "sr_math.hpp"
+#include "rust_select.hpp"
 #include "tube_build.hpp"
 
 using namespace srh;
@@ -244,6 +246,7 @@ inline float box_measure(const Box& b) {  // bvh4d.rs:8-13
 
 struct Builder {
     unsigned spawn_depth;  // subtrees above this recursion depth may build their halves concurrently
+    std::atomic<uint32_t>* median = nullptr;  // counts the splits that fell back to the median
 
     static inline uint64_t sat_usize(float x) { return (std::isnan(x) || x <= 0.0f) ? 0 : (uint64_t)x; }
 
@@ -333,9 +336,12 @@ struct Builder {
         size_t mid = 0;
         for (size_t i = 0; i < n; ++i)
             if (r[i].c.ax(best_axis) < best_pos) { std::swap(r[i], r[mid]); ++mid; }
-        if (mid == 0 || mid == n) {
+        if (mid == 0 || mid == n) {  // bvh4d.rs:418-424: select_nth_unstable_by on the centroid
             mid = n / 2;
-            std::nth_element(r, r + mid, r + n, [best_axis](const Ref& a, const Ref& b) { return a.c.ax(best_axis) < b.c.ax(best_axis); });
+            sr_select::select_nth_unstable(r, n, mid, [best_axis](const Ref& a, const Ref& b) {
+                return a.c.ax(best_axis) < b.c.ax(best_axis);  // partial_cmp == Less (no NaN centroids)
+            });
+            if (median) median->fetch_add(1, std::memory_order_relaxed);
         }
         *mid_out = mid;
         return true;
@@ -628,8 +634,10 @@ extern "C" sr_status sr_scene_synth(const SrSynthParams* p, sr_scene** out, char
     for (size_t i = 0; i < n; ++i) refs[i] = {tets[i].box, (tets[i].box.lo + tets[i].box.hi) * 0.5f, (uint32_t)i};
     unsigned sd = 0;
     while ((1u << sd) < threads * 4) ++sd;
-    Builder bld{sd};
+    std::atomic<uint32_t> median{0};
+    Builder bld{sd, &median};
     std::vector<Node> nodes = n ? bld.build_sub(refs.data(), n, 0, 0) : std::vector<Node>();
+    sc->info.median_splits = median.load();
     sc->nodes.resize(nodes.size());
     for (size_t i = 0; i < nodes.size(); ++i) {
         SrGpuNode& g = sc->nodes[i];
@@ -669,6 +677,38 @@ extern "C" sr_status sr_scene_synth(const SrSynthParams* p, sr_scene** out, char
 }
 
 extern "C" void sr_scene_free(sr_scene* s) { delete s; }
+
+extern "C" sr_status sr_bvh_build_host(const float* boxes, uint32_t n, uint32_t threads, SrGpuNode* nodes,
+                                       uint32_t nodes_cap, uint32_t* order, uint32_t* num_nodes,
+                                       uint32_t* median_splits) {
+    if ((n && (!boxes || !nodes || !order)) || !num_nodes) return SR_ERR_INVALID_ARGUMENT;
+    if (n && (uint64_t)nodes_cap < 2ull * n - 1) return SR_ERR_INVALID_ARGUMENT;
+    std::vector<Ref> refs(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        Box b;
+        b.lo = V4f(boxes[8 * i], boxes[8 * i + 1], boxes[8 * i + 2], boxes[8 * i + 3]);
+        b.hi = V4f(boxes[8 * i + 4], boxes[8 * i + 5], boxes[8 * i + 6], boxes[8 * i + 7]);
+        refs[i] = {b, (b.lo + b.hi) * 0.5f, i};
+    }
+    unsigned sd = 0;
+    while ((1u << sd) < std::max(1u, threads) * 4) ++sd;
+    std::atomic<uint32_t> median{0};
+    Builder bld{sd, &median};
+    std::vector<Node> out = n ? bld.build_sub(refs.data(), n, 0, 0) : std::vector<Node>();
+    for (size_t i = 0; i < out.size(); ++i) {
+        SrGpuNode& g = nodes[i];
+        put4(g.min, out[i].box.lo);
+        put4(g.max, out[i].box.hi);
+        g.right_or_first = out[i].right_or_first;
+        g.count = out[i].count;
+        g.left = out[i].left;
+        g.pad = 0;
+    }
+    for (uint32_t i = 0; i < n; ++i) order[i] = refs[i].index;
+    *num_nodes = (uint32_t)out.size();
+    if (median_splits) *median_splits = median.load();
+    return SR_OK;
+}
 
 extern "C" sr_status sr_scene_desc(const sr_scene* s, SrSceneDesc* d) {
     if (!s || !d) return SR_ERR_INVALID_ARGUMENT;

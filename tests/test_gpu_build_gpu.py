@@ -123,3 +123,17 @@ def test_dynamic_scale_update_and_rebuild(engine):
     assert (engine.render(25, u, path=sr.SR_PATH_FAST).rgb == ref).all()
     print(f"{scene.num_prims} simplices: dirty-range update {np.median(ts_up) * 1e3:.2f} ms, "
           f"rebuild from worldtubes on the device {np.median(ts_build) * 1e3:.2f} ms (medians of 10)")
+
+
+def test_device_build_reports_the_median_split(engine):
+    """A node whose SAH split leaves one side empty is split at the centroid median by the reference
+    (Rust's select_nth_unstable_by); the device build does not restate that selection and returns
+    SR_ERR_UNSUPPORTED, so such a scene is built on the host (sr_bvh_build_host flags it)."""
+    from test_median_split import degenerate_boxes, host_build
+    boxes = degenerate_boxes()
+    n = len(boxes)
+    mats = sr.synth_scene(1, 1, n_bodies=2, steps=2).packed().materials
+    with pytest.raises(sr.SrError) as e:
+        engine.build(22, boxes, np.zeros(n, sr.GEOM_DTYPE), np.zeros(n, sr.ATTR_DTYPE), mats)
+    assert e.value.status == sr._lib.SR_ERR_UNSUPPORTED
+    assert host_build(boxes)[2] == 1
