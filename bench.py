@@ -308,7 +308,7 @@ def config4_measure(args, rank, world, local, dist, stream, eng, idx):
 
     with torch.cuda.stream(stream):
         if not args.no_autotune:
-            eng.autotune(idx, us[0], 2)
+            eng.autotune(idx, us[0], 8)
         ms = timed(batch_step, args.steps)
         plain_ms = timed(plain_step, max(2, args.steps // 2))
         ph = eng.render_batch(idx, us, ptr, rays, cams=cams, device_output=True, phases=True)
@@ -421,7 +421,7 @@ def run_engine(args, rank, world, local):
     with torch.cuda.stream(stream):
         # Launch parameters for this scene, untimed.
         if not args.no_autotune:
-            eng.autotune(0, us[0], 2)
+            eng.autotune(0, us[0], B)
 
         def batch_step():
             eng.render_batch(0, us, ptr, B * RAYS_PER_FRAME, cams=c64, device_output=True)

@@ -531,7 +531,10 @@ typedef struct SrTuning {
 } SrTuning;
 sr_status sr_get_tuning(const sr_ctx* ctx, uint32_t scene_idx, SrTuning* out);
 sr_status sr_set_tuning(sr_ctx* ctx, uint32_t scene_idx, const SrTuning* t);
-/* Times candidate SrTuning values on `n` frames and keeps the fastest for this scene. */
+/* Times candidate SrTuning values on a batch of `n` copies of the observer `u` (the batched path,
+ * replayed from its captured graph after a warm-up batch), in two sweeps taking each candidate's
+ * better time, and keeps the fastest for this scene; the current tuning stays unless a candidate
+ * is at least 1% faster. `best_ms`: the winner's time per frame. */
 sr_status sr_autotune(sr_ctx* ctx, uint32_t scene_idx, const SrGpuUniforms* u, uint32_t n, SrTuning* best,
                       float* best_ms);
 

@@ -1207,6 +1207,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
     key = mix(key, ((uint64_t)t.chunk_tiles << 40) | ((uint64_t)t.refill_lanes << 24) | ((uint64_t)t.leaf_batch << 8) |
                        t.leaf_coop);
     key = mix(key, t.home_pct);
+    key = mix(key, ((uint64_t)t.stack_smem << 32) | t.top_levels);
     key = mix(key, binned ? 0x5354ull : 0ull);
     key = mix(key, simple ? 0x51ull : 0ull);
     for (auto& o : sh.obs) key = mix(key, ((uint64_t)o.width << 32) | o.height);
