@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch parameters")
     ap.add_argument("--bodies", type=int, default=64,
                     help="icospheres in the scene (64 is the workload; fewer only for small profiling captures)")
-    ap.add_argument("--workload", choices=["config2", "config4", "config5"], default="config2",
+    ap.add_argument("--workload", choices=["config2", "config4", "config5", "tunings"], default="config2",
                     help="config2: the headline (8 observers of the 7.9M-tet scene per step, with the config4 and "
                          "config5 legs as extra keys); config4 / config5 alone: see run_config4 / run_config5")
     return ap.parse_args()
@@ -663,6 +663,63 @@ def _standalone(args, rank, world, local, fn):
     print(json.dumps(line), flush=True)
 
 
+def run_tunings(args, local):
+    """Trace-kernel time per 8-frame batch of the headline workload under launch settings and node
+    layouts (SrTuning fields, sr_set_layout), each timed with the library's CUDA events around the
+    kernel outside the captured graph, three rounds interleaved across the settings, medians
+    printed as one JSON line. Not a bench line: the comparison behind the default settings."""
+    import torch
+    import specrel_b200 as sr
+    from specrel_b200 import shard
+    torch.cuda.set_device(local)
+    scene = sr.synth_scene(2, args.seed, n_bodies=args.bodies, threads=os.cpu_count() or 1)
+    eng = sr.Engine(local)
+    eng.upload(0, scene)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    B = args.batch
+    raps = shard.observer_rapidities(args.seed, 0, B, scene.info.cam_rapidity)
+    us = [sr.uniforms(sr.camera(rapidity=r), W, H, 0, 1, 0, num_nodes=scene.num_nodes, light_pos=scene.light_pos)
+          for r in raps]
+    c64 = [sr.cam64((0.0,) * 4, r) for r in raps]
+    out = torch.empty(B * RAYS_PER_FRAME, dtype=torch.int32, device=f"cuda:{local}")
+
+    def tune(threads, blocks, stack, top):
+        t = eng.tuning(0)
+        t.block_threads, t.blocks_per_sm, t.stack_smem, t.top_levels = threads, blocks, stack, top
+        t.tile_w, t.tile_h, t.chunk_tiles, t.refill_lanes, t.leaf_coop, t.leaf_batch, t.home_pct = 4, 8, 1, 32, 0, 1, 0
+        eng.set_tuning(0, t)
+
+    def trace_ms(k=5):
+        ts = []
+        with torch.cuda.stream(stream):
+            eng.render_batch(0, us, out.data_ptr(), B * RAYS_PER_FRAME, cams=c64, device_output=True)
+            for _ in range(k):
+                ts.append(eng.render_batch(0, us, out.data_ptr(), B * RAYS_PER_FRAME, cams=c64, device_output=True,
+                                           phases=True).trace_ms)
+        return float(np.median(ts))
+
+    L = sr._lib
+    cands = [("octant", 128, 11, 0, 0), ("octant", 128, 9, 0, 0), ("octant", 128, 11, 12, 0), ("octant", 128, 9, 12, 0),
+             ("octant", 128, 8, 12, 0), ("octant", 128, 9, 10, 0), ("octant", 128, 9, 16, 0), ("octant", 128, 9, 8, 0),
+             ("octant", 128, 9, 0, 4), ("octant", 128, 9, 0, 6), ("octant", 128, 9, 0, 8), ("octant", 128, 8, 12, 4),
+             ("octant", 128, 8, 12, 6), ("octant", 128, 8, 12, 8), ("compact", 128, 9, 0, 0), ("compact", 128, 9, 10, 0)]
+    res = {c: [] for c in cands}
+    for _ in range(3):
+        for layout in ("octant", "compact"):
+            eng.set_layout(0, L.SR_LAYOUT_OCTANT if layout == "octant" else L.SR_LAYOUT_COMPACT)
+            for c in cands:
+                if c[0] == layout:
+                    tune(*c[1:])
+                    res[c].append(trace_ms())
+    eng.set_layout(0, L.SR_LAYOUT_AUTO)
+    rows = [{"layout": c[0], "block_threads": c[1], "blocks_per_sm": c[2], "stack_smem": c[3], "top_levels": c[4],
+             "trace_ms": float(np.median(v)), "runs": v} for c, v in res.items()]
+    print(json.dumps({"what": f"trace-kernel ms per {B}-frame batch, {scene.num_prims} tets, 1280x800", "rows": rows}),
+          flush=True)
+    eng.close()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -670,6 +727,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload == "tunings":
+        if rank == 0:
+            run_tunings(args, local)
     elif args.workload in ("config4", "config5"):
         _standalone(args, rank, world, local, args.workload)
     else:
