@@ -46,7 +46,7 @@ def test_fp64_rebase_matches_fp64_oracle(engine, fp64_oracle):
         print(path, reports[path])
         assert same.mean() >= 0.9999
         assert lam_rel.max() <= 1e-5 and tau_rel.max() <= 1e-5
-        assert (d > 1).mean() <= 0.002
+        assert d.max() <= 1  # every pixel within 1/255 of the FP64 oracle (measured: max 1)
     # The two engine paths agree with each other exactly.
     assert reports[0] == reports[1]
 
