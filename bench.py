@@ -384,6 +384,65 @@ def config5_measure(args, local, stream, eng, idx):
     return res
 
 
+def coherent_roof(sr, eng, scene, ptr, B, seed, work, trace_ms):
+    """The trace kernel's ceiling on this GPU, measured in this run: batches in which every pixel of
+    a frame traces that frame's centre ray (half_wh = 0), so the 32 lanes of a warp take the same
+    nodes and tests in step, no lane idles, and every load after a warp's first is an L1 hit. The
+    kernel's time on such batches, least squares (non-negative) over per-launch, per-node-visit,
+    per-tetrahedron-test and per-shadow-ray costs, gives the time the same kernel would take on the
+    real batch's work if its rays were coherent: the roof. frac = roof time / measured time.
+    Centre rays vary by observer rapidity, yaw and pitch, slice (past cone, God's-eye, future
+    cone) and shadows on / off, so the work mix varies across the fitted batches.
+    Only for scenes without stars (the binned-star set-up divides by the pixel pitch)."""
+    from scipy.optimize import nnls
+    rng = np.random.default_rng(seed * 31 + 7)
+    X, y = [], []
+    for slice_mode in (0, 1, 2):
+        for shadow in (1, 0):
+            for _ in range(4):
+                while True:
+                    r = rng.uniform(-1.0, 1.0, 3)
+                    if r @ r < 1.0:
+                        break
+                r = tuple(float(v) for v in 2.0 * r)
+                yaw, pitch = float(rng.uniform(-0.5, 0.5)), float(rng.uniform(-0.35, 0.35))
+                u = sr.uniforms(sr.camera(rapidity=r), W, H, 0, shadow, slice_mode, num_nodes=scene.num_nodes,
+                                light_pos=scene.light_pos)
+                u.half_wh[0] = 0.0
+                u.half_wh[1] = 0.0
+                c = sr.cam64((0.0, 0.0, 0.0, 0.0), r, yaw, pitch)
+                ub, cb = [u] * B, [c] * B
+                eng.render_batch(0, ub, ptr, B * RAYS_PER_FRAME, cams=cb, device_output=True)
+                ts = [eng.render_batch(0, ub, ptr, B * RAYS_PER_FRAME, cams=cb, device_output=True,
+                                       phases=True).trace_ms for _ in range(3)]
+                t = eng.render_batch(0, ub, ptr, B * RAYS_PER_FRAME, cams=cb, device_output=True, count=True)
+                X.append([1.0, float(t.nodes_visited + t.shadow_nodes_visited),
+                          float(t.tets_tested + t.shadow_tets_tested), float(t.shadow_rays)])
+                y.append(float(np.median(ts)))
+    X, y = np.array(X), np.array(y)
+    scale = np.maximum(X.max(axis=0), 1.0)
+    coef, _ = nnls(X / scale, y)
+    coef = coef / scale
+    fit = X @ coef
+    real = np.array([1.0, work[0] + work[3], work[2] + work[5], work[6]])
+    roof_ms = float(real @ coef)
+    rays = B * RAYS_PER_FRAME
+    return {
+        "achieved": rays / (trace_ms / 1e3) / 1e6, "peak": rays / (roof_ms / 1e3) / 1e6, "unit": "Mrays/s",
+        "frac": roof_ms / trace_ms, "roof_ms_per_launch": roof_ms,
+        "peak_kind": "measured in this run: the same kernel on warp-coherent batches (every pixel of a frame on "
+                     "its centre ray), its per-launch, per-node-visit, per-test and per-shadow-ray costs fitted "
+                     "and applied to this batch's counted work",
+        "coherent_fit": {"batches": int(len(y)), "ms_per_launch": float(coef[0]),
+                         "ns_per_node_visit": float(coef[1] * 1e6), "ns_per_tet_test": float(coef[2] * 1e6),
+                         "ns_per_shadow_ray": float(coef[3] * 1e6),
+                         "max_rel_residual": float(np.max(np.abs(fit - y) / y)),
+                         "trace_ms_range": [float(y.min()), float(y.max())],
+                         "node_visits_per_launch_range": [float(X[:, 1].min()), float(X[:, 1].max())],
+                         "tet_tests_per_launch_range": [float(X[:, 2].min()), float(X[:, 2].max())]},
+    }
+
+
 def run_engine(args, rank, world, local):
     import torch
     import specrel_b200 as sr
@@ -541,6 +600,9 @@ def run_engine(args, rank, world, local):
                          t.shadow_leaves_visited, t.shadow_tets_tested, t.shadow_rays], dtype=np.float64)
         tuning = eng.tuning(0)
         stats = eng.stats(0)
+        roof = None
+        if scene.num_stars == 0:
+            roof = coherent_roof(sr, eng, scene, ptr, B, args.seed, work, float(np.median(trace_ms)))
 
         if not args.no_extra:
             extra["config4"] = config4_measure(args, rank, world, local, dist, stream, eng, 1)
@@ -590,13 +652,21 @@ def run_engine(args, rank, world, local):
         # The trace kernel is not bound by HBM: its working set (the light cone's share of the
         # tree) is served from L1 and L2, so the byte model below (every node visit and test
         # counted as if fetched) exceeds the HBM roof. What binds it is instruction issue and L1
-        # latency (ncu summaries in profiles/).
-        "roofline": {"bound": "issue", "kernel": "k_trace_lean", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "hbm_frac": achieved / peak, "peak_kind": peak_kind,
-                     "note": "achieved = algorithmic bytes (72 B per node visit, 80 B per tetrahedron test, 21 B "
-                             "written per ray) / trace-kernel time; these bytes are mostly served by L1/L2, so "
-                             "hbm_frac > 1 says the kernel is not HBM-bound. DRAM traffic and warp-instruction "
-                             "counts come from ncu captures (profiles/), not from this run.",
+        # latency (ncu summaries in profiles/); its roof is the same kernel's speed on
+        # warp-coherent rays, measured in this run (coherent_roof).
+        "roofline": {"bound": "issue", "kernel": "k_trace_lean",
+                     **(roof if roof is not None else
+                        {"achieved": None, "peak": None, "unit": "Mrays/s", "frac": None,
+                         "peak_kind": "not measured (scene with stars)"}),
+                     "hbm_achieved_gbs": achieved, "hbm_peak_gbs": peak, "hbm_frac": achieved / peak,
+                     "hbm_peak_kind": peak_kind,
+                     "note": "frac = the trace kernel's time on this batch's counted work at warp-coherent speed "
+                             "(fitted on coherent batches in this run) / its measured time: what divergence and "
+                             "cache misses cost. hbm_achieved_gbs = algorithmic bytes (72 B per node visit, 80 B "
+                             "per tetrahedron test, 21 B written per ray) / trace-kernel time; these bytes are "
+                             "mostly served by L1/L2, so hbm_frac > 1 says the kernel is not HBM-bound. DRAM "
+                             "traffic and warp-instruction counts come from ncu captures (profiles/), not from "
+                             "this run.",
                      "traffic": None,
                      "algorithmic_bytes_per_launch": trace_bytes, "frames_per_launch": B,
                      "trace_ms_per_launch": trace_s * 1e3,
