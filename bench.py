@@ -754,9 +754,9 @@ def run_tunings(args, local):
     c64 = [sr.cam64((0.0,) * 4, r) for r in raps]
     out = torch.empty(B * RAYS_PER_FRAME, dtype=torch.int32, device=f"cuda:{local}")
 
-    def tune(threads, blocks, stack, top):
+    def tune(threads, blocks, stack, top, packet=0):
         t = eng.tuning(0)
-        t.block_threads, t.blocks_per_sm, t.stack_smem, t.top_levels = threads, blocks, stack, top
+        t.block_threads, t.blocks_per_sm, t.stack_smem, t.top_levels, t.packet = threads, blocks, stack, top, packet
         t.tile_w, t.tile_h, t.chunk_tiles, t.refill_lanes, t.leaf_coop, t.leaf_batch, t.home_pct = 4, 8, 1, 32, 0, 1, 0
         eng.set_tuning(0, t)
 
@@ -773,7 +773,9 @@ def run_tunings(args, local):
     cands = [("octant", 128, 11, 0, 0), ("octant", 128, 9, 0, 0), ("octant", 128, 11, 12, 0), ("octant", 128, 9, 12, 0),
              ("octant", 128, 8, 12, 0), ("octant", 128, 9, 10, 0), ("octant", 128, 9, 16, 0), ("octant", 128, 9, 8, 0),
              ("octant", 128, 9, 0, 4), ("octant", 128, 9, 0, 6), ("octant", 128, 9, 0, 8), ("octant", 128, 8, 12, 4),
-             ("octant", 128, 8, 12, 6), ("octant", 128, 8, 12, 8), ("compact", 128, 9, 0, 0), ("compact", 128, 9, 10, 0)]
+             ("octant", 128, 8, 12, 6), ("octant", 128, 8, 12, 8), ("compact", 128, 9, 0, 0), ("compact", 128, 9, 10, 0),
+             ("octant", 128, 8, 0, 0, 1), ("octant", 256, 4, 0, 0, 1), ("octant", 64, 16, 0, 0, 1),
+             ("octant", 128, 6, 0, 0, 1), ("compact", 128, 8, 0, 0, 1)]
     res = {c: [] for c in cands}
     for _ in range(3):
         for layout in ("octant", "compact"):
@@ -784,7 +786,7 @@ def run_tunings(args, local):
                     res[c].append(trace_ms())
     eng.set_layout(0, L.SR_LAYOUT_AUTO)
     rows = [{"layout": c[0], "block_threads": c[1], "blocks_per_sm": c[2], "stack_smem": c[3], "top_levels": c[4],
-             "trace_ms": float(np.median(v)), "runs": v} for c, v in res.items()]
+             "packet": c[5] if len(c) > 5 else 0, "trace_ms": float(np.median(v)), "runs": v} for c, v in res.items()]
     print(json.dumps({"what": f"trace-kernel ms per {B}-frame batch, {scene.num_prims} tets, 1280x800", "rows": rows}),
           flush=True)
     eng.close()

@@ -145,7 +145,7 @@ class Tuning(C.Structure):
                 ("tile_h", C.c_uint32), ("chunk_tiles", C.c_uint32), ("refill_lanes", C.c_uint32),
                 ("leaf_coop", C.c_uint32), ("leaf_batch", C.c_uint32),
                 ("home_pct", C.c_uint32), ("stack_smem", C.c_uint32), ("top_levels", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("packet", C.c_uint32)]
 
 
 class SynthParams(C.Structure):

@@ -808,9 +808,9 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
     SrTuning keep = s.tuning;
     // The schedules worth timing: whole-warp refills of single tiles were fastest on every scene
     // measured (wider chunks or partial refills spread the rays in flight over more of the tree).
-    // Per block shape and tile: cooperative leaf tests, or the lean kernel with the traversal
-    // stack in local memory or its first 8..16 entries in shared memory.
-    const uint32_t shapes[][2] = {{128, 8}, {128, 9}, {128, 11}, {256, 4}, {256, 6}, {512, 3}};
+    // Per block shape and tile: the packet traversal, cooperative leaf tests, or the lean kernel
+    // with the traversal stack in local memory or its first 8..16 entries in shared memory.
+    const uint32_t shapes[][2] = {{128, 8}, {128, 9}, {128, 11}, {256, 4}, {256, 6}, {512, 3}, {64, 16}};
     const uint32_t tiles[][2] = {{8, 4}, {4, 8}};
     // With the stack in local memory or 12 entries in shared memory, also the top 4, 6 or 8 levels
     // of the tree staged in shared memory.
@@ -819,7 +819,8 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
     std::vector<SrTuning> cand{keep};
     for (auto& sh : shapes)
         for (auto& tl : tiles)
-            for (uint32_t v = 0; v <= sizeof(stacks) / sizeof(stacks[0]); ++v) {
+            for (uint32_t v = 0; v <= sizeof(stacks) / sizeof(stacks[0]) + 1; ++v) {
+                const bool packet = v == sizeof(stacks) / sizeof(stacks[0]) + 1;
                 SrTuning t = keep;
                 t.block_threads = sh[0];
                 t.blocks_per_sm = sh[1];
@@ -830,8 +831,9 @@ sr_status sr_autotune(sr_ctx* ctx, uint32_t idx, const SrGpuUniforms* u, uint32_
                 t.leaf_coop = v == 0 ? 1u : 0u;
                 t.leaf_batch = 1;
                 t.home_pct = 0;
-                t.stack_smem = v == 0 ? 0u : stacks[v - 1][0];
-                t.top_levels = v == 0 ? 0u : stacks[v - 1][1];
+                t.stack_smem = v == 0 || packet ? 0u : stacks[v - 1][0];
+                t.top_levels = v == 0 || packet ? 0u : stacks[v - 1][1];
+                t.packet = packet ? 1u : 0u;
                 if (fast_tuning_valid(ctx->fast, t)) cand.push_back(t);
             }
     auto time_batch = [&](const SrTuning& t, float* ms) -> sr_status {

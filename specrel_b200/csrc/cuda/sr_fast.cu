@@ -70,9 +70,12 @@ __device__ __forceinline__ uint32_t wide_index(const uint32_t* topid, const uint
 }
 
 // One wide node: both children's boxes in each of the `copies` sign-octant copies (near corner,
-// far corner; see WideScene; copy 0 is the plain (min, max) layout) and the packed child references.
+// far corner; see WideScene; copy 0 is the plain (min, max) layout), the packed child references,
+// and the up links of its children (an internal child's in `up`, a leaf child's records' in
+// `leafpar`: this node's index, bit 31 set for the right child).
 __global__ void k_wide_fill(const SrGpuNode* nodes, uint32_t n, const uint32_t* topid, const uint32_t* wid,
-                            uint32_t n_top, float4* boxes, size_t oct_stride, uint32_t copies, uint2* refs) {
+                            uint32_t n_top, float4* boxes, size_t oct_stride, uint32_t copies, uint2* refs, uint32_t* up,
+                            uint32_t* leafpar) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || nodes[i].count != 0) return;
     const uint32_t wi = wide_index(topid, wid, n_top, i);
@@ -92,6 +95,11 @@ __global__ void k_wide_fill(const SrGpuNode* nodes, uint32_t n, const uint32_t* 
             b[2 * k + 1] = make_float4(fr[0], fr[1], fr[2], fr[3]);
         }
         ref[k] = ch.count > 0 ? pack_leaf(ch.right_or_first, ch.count) : wide_index(topid, wid, n_top, c[k]);
+        const uint32_t link = wi | ((uint32_t)k << 31);
+        if (ch.count > 0)
+            for (uint32_t p = ch.right_or_first; p < ch.right_or_first + ch.count; ++p) leafpar[p] = link;
+        else
+            up[ref[k]] = link;
     }
     refs[wi] = make_uint2(ref[0], ref[1]);
 }
@@ -181,8 +189,12 @@ cudaError_t fast_build(FastCtx& c, FastScene& s, const SrGpuNode* nodes, uint32_
     if (before && before != s.copies) s.boxes.release();  // a layout change does not keep the old size
     if ((e = s.boxes.ensure_grow((size_t)s.num_wide * 64 * s.copies)) != cudaSuccess) return e;
     if ((e = s.refs.ensure_grow((size_t)s.num_wide * 8)) != cudaSuccess) return e;
+    if ((e = s.up.ensure_grow((size_t)s.num_wide * 4)) != cudaSuccess) return e;
+    if ((e = s.leafpar.ensure_grow((size_t)num_prims * 4 + 4)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(s.up.p, 0xFF, (size_t)s.num_wide * 4, st)) != cudaSuccess) return e;  // the root: ~0
     k_wide_fill<<<(n + 255) / 256, 256, 0, st>>>(nodes, n, topid, wid, n_top, s.boxes.as<float4>(), 4ull * s.num_wide,
-                                                 s.copies, s.refs.as<uint2>());
+                                                 s.copies, s.refs.as<uint2>(), s.up.as<uint32_t>(),
+                                                 s.leafpar.as<uint32_t>());
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     e = cudaStreamSynchronize(st);
     s.scratch.ensure(0);
@@ -193,7 +205,7 @@ SrTuning fast_default_tuning(const FastCtx& c) {
     (void)c;
     SrTuning t{};
     t.block_threads = 128;
-    t.blocks_per_sm = 11;
+    t.blocks_per_sm = 8;  // the packet kernel's 64 registers leave room for 8 blocks of 128
     t.tile_w = 4;
     t.tile_h = 8;
     t.chunk_tiles = 1;
@@ -201,6 +213,7 @@ SrTuning fast_default_tuning(const FastCtx& c) {
     t.leaf_coop = 0;
     t.leaf_batch = 1;
     t.home_pct = 0;
+    t.packet = 1;
     return t;
 }
 
@@ -212,7 +225,9 @@ bool fast_tuning_valid(const FastCtx& c, const SrTuning& t) {
            t.leaf_coop <= 1 && t.leaf_batch >= 1 && t.leaf_batch <= 32 && t.home_pct <= 100 &&
            lean_stack_supported(t.stack_smem) && t.top_levels <= TOP_LEVELS &&
            (t.top_levels == 0 || t.stack_smem == 0 || t.stack_smem == 12) &&
-           stack_bytes + (t.top_levels ? ((size_t)1 << t.top_levels) * 72u : 0u) <= (size_t)c.max_smem && t.reserved == 0;
+           stack_bytes + (t.top_levels ? ((size_t)1 << t.top_levels) * 72u : 0u) <= (size_t)c.max_smem && t.packet <= 1 &&
+           (t.packet == 0 || (t.stack_smem == 0 && t.top_levels == 0 && !t.leaf_coop && t.leaf_batch == 1 &&
+                              t.refill_lanes == 32 && t.chunk_tiles == 1));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -655,9 +670,11 @@ __device__ __forceinline__ uint32_t next_tile(const TraceBatchArgs& a, uint32_t 
 // (SplitStack), the rest in local memory; SS == 0: all in local memory (LocalStack). OCT: the
 // scene has the 16 sign-octant box copies; otherwise the compact layout (one copy). TOP: the first
 // a.top_n wide nodes (the tree's top levels) are staged in shared memory after the stacks, their
-// (min, max) boxes then their references.
-template <bool COUNT, int SS, bool OCT, bool TOP>
+// (min, max) boxes then their references. PKT: each warp walks its tile's primary rays as one
+// packet (closest_packet; built with SS == 0, no staging and no counting).
+template <bool COUNT, int SS, bool OCT, bool TOP, bool PKT>
 __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
+    static_assert(!PKT || (!COUNT && SS == 0 && !TOP), "the packet form is built alone");
     const uint32_t lane = threadIdx.x & 31u;
     Work wp{0, 0, 0}, wsh{0, 0, 0};
     uint2 lm[FAST_STACK];
@@ -683,13 +700,14 @@ __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
         tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
         if (tile == ~0u) break;
         const uint32_t base = tile << 5;
-        uint32_t obs, px, py, pix;
-        if (!ray_pixel(a, base + lane, &obs, &px, &py, &pix)) continue;
-        const Cam cam = cam_of(a.cam, obs);
-        const SrGpuUniforms& U = a.U[obs];
-        float4 o, d;
-        float sx, sy;
-        camera_ray(U, cam, px, py, &o, &d, &sx, &sy);
+        uint32_t obs = 0, px = 0, py = 0, pix = 0;
+        const bool valid = ray_pixel(a, base + lane, &obs, &px, &py, &pix);
+        if (!PKT && !valid) continue;  // the packet form keeps every lane in the warp's traversal
+        float4 o = v4(0.0f, 0.0f, 0.0f, 0.0f), d = v4(0.0f, 0.0f, 1.0f, 0.0f);
+        if (valid) {
+            float sx, sy;
+            camera_ray(a.U[obs], cam_of(a.cam, obs), px, py, &o, &d, &sx, &sy);
+        }
         const float4 no = neg4(o);  // the traversal and the hit event use the negated origin only
         const float4 inv = v4(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z), safe_inv(d.w));
         float t_max = 180.0f;
@@ -698,10 +716,17 @@ __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
         if (!a.ws.empty) {
             float en, ex;
             slab_interval(a.ws.root_min, a.ws.root_max, no, inv, 1e-3f, t_max, &en, &ex);
-            if (ex >= en && en < t_max)  // else the ray misses the scene's box (bvh4d.rs:451)
+            const bool in = valid && ex >= en && en < t_max;  // else the ray misses the scene's box (bvh4d.rs:451)
+            if constexpr (PKT) {
+                if (__any_sync(0xFFFFFFFFu, in))
+                    slot = closest_packet<OCT>(a.ws, in, no, d, inv, 1e-3f, t_max, best, st, a.err);
+            } else if (in) {
                 slot = closest_lean<COUNT, OCT, TOP>(a.ws, a.ws.root_ref, no, d, inv, 1e-3f, t_max, best, st, a.err, wp,
                                                      top);
+            }
         }
+        if (!valid) continue;
+        const SrGpuUniforms& U = a.U[obs];
         a.hits[pix] = make_float4(best.lambda, best.u, best.v, best.w);
         a.slots[pix] = slot < 0 ? 0xFFFFFFFFu : (uint32_t)slot;
         uint8_t sh = 0;
@@ -751,7 +776,8 @@ bool lean_stack_supported(uint32_t s) {
 template <bool COUNT, int SS, bool OCT, bool TOP>
 static cudaError_t lean_attr(int max_smem) {
     return SS > 0 || TOP
-               ? cudaFuncSetAttribute(k_trace_lean<COUNT, SS, OCT, TOP>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)
+               ? cudaFuncSetAttribute(k_trace_lean<COUNT, SS, OCT, TOP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      max_smem)
                : cudaSuccess;
 }
 
@@ -782,22 +808,29 @@ static void launch_lean_ss(bool count, bool oct, bool top, uint32_t blocks, uint
                            const TraceBatchArgs& ta) {
     if constexpr (SS == 0 || SS == 12) {
         if (top && oct) {
-            if (count) k_trace_lean<true, SS, true, true><<<blocks, threads, smem, st>>>(ta);
-            else k_trace_lean<false, SS, true, true><<<blocks, threads, smem, st>>>(ta);
+            if (count) k_trace_lean<true, SS, true, true, false><<<blocks, threads, smem, st>>>(ta);
+            else k_trace_lean<false, SS, true, true, false><<<blocks, threads, smem, st>>>(ta);
             return;
         }
     }
     if (oct) {
-        if (count) k_trace_lean<true, SS, true, false><<<blocks, threads, smem, st>>>(ta);
-        else k_trace_lean<false, SS, true, false><<<blocks, threads, smem, st>>>(ta);
+        if (count) k_trace_lean<true, SS, true, false, false><<<blocks, threads, smem, st>>>(ta);
+        else k_trace_lean<false, SS, true, false, false><<<blocks, threads, smem, st>>>(ta);
     } else {
-        if (count) k_trace_lean<true, SS, false, false><<<blocks, threads, smem, st>>>(ta);
-        else k_trace_lean<false, SS, false, false><<<blocks, threads, smem, st>>>(ta);
+        if (count) k_trace_lean<true, SS, false, false, false><<<blocks, threads, smem, st>>>(ta);
+        else k_trace_lean<false, SS, false, false, false><<<blocks, threads, smem, st>>>(ta);
     }
 }
 
-static void launch_lean(uint32_t ss, bool count, bool oct, bool top, uint32_t blocks, uint32_t threads, size_t smem,
-                        cudaStream_t st, const TraceBatchArgs& ta) {
+// packet: the warp-packet traversal of primary rays (counting runs always take the per-lane order,
+// whose work counts are the reference traversal's).
+static void launch_lean(uint32_t ss, bool count, bool oct, bool top, bool packet, uint32_t blocks, uint32_t threads,
+                        size_t smem, cudaStream_t st, const TraceBatchArgs& ta) {
+    if (packet && !count) {
+        if (oct) k_trace_lean<false, 0, true, false, true><<<blocks, threads, smem, st>>>(ta);
+        else k_trace_lean<false, 0, false, false, true><<<blocks, threads, smem, st>>>(ta);
+        return;
+    }
 #define SR_ONE(S)                                                             \
     if (ss == (S)) {                                                          \
         launch_lean_ss<(S)>(count, oct, top, blocks, threads, smem, st, ta);  \
@@ -1029,6 +1062,8 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
     ws.boxes = s.boxes.as<float4>();
     ws.oct_stride = 4ull * s.num_wide;
     ws.refs = s.refs.as<uint2>();
+    ws.up = s.up.as<uint32_t>();
+    ws.leafpar = s.leafpar.as<uint32_t>();
     ws.geoms = sd.geoms;
     ws.root_min = make_float4(s.root_min[0], s.root_min[1], s.root_min[2], s.root_min[3]);
     ws.root_max = make_float4(s.root_max[0], s.root_max[1], s.root_max[2], s.root_max[3]);
@@ -1085,7 +1120,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
             const bool oct = s.copies == 16, top = oct && t.top_levels > 0;
             ta.top_n = top ? s.top_end[t.top_levels - 1] : 0u;
             const size_t ssm = lean_stack_bytes(t) + (size_t)ta.top_n * 72u;
-            launch_lean(t.stack_smem, r.count_work, oct, top, blocks, t.block_threads, ssm, st, ta);
+            launch_lean(t.stack_smem, r.count_work, oct, top, t.packet != 0, blocks, t.block_threads, ssm, st, ta);
         } else if (t.leaf_coop) {
             if (r.count_work) k_trace_batch<true, true><<<blocks, t.block_threads, smem, st>>>(ta);
             else k_trace_batch<false, true><<<blocks, t.block_threads, smem, st>>>(ta);
@@ -1208,6 +1243,7 @@ cudaError_t fast_render_batch(FastCtx& c, const FastScene& s, const SrTuning& t,
                        t.leaf_coop);
     key = mix(key, t.home_pct);
     key = mix(key, ((uint64_t)t.stack_smem << 32) | t.top_levels);
+    key = mix(key, t.packet);
     key = mix(key, binned ? 0x5354ull : 0ull);
     key = mix(key, simple ? 0x51ull : 0ull);
     for (auto& o : sh.obs) key = mix(key, ((uint64_t)o.width << 32) | o.height);

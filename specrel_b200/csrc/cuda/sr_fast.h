@@ -62,6 +62,8 @@ struct HostMem {  // pinned host staging
 // The B200 node layout of one scene (see sr_traverse.cuh).
 struct FastScene {
     DevMem boxes, refs, scratch;
+    // Up links for the packet traversal's ordering of equal-lambda hits (WideScene::up / leafpar).
+    DevMem up, leafpar;
     uint32_t num_wide = 0;
     uint32_t depth = 0;
     uint32_t root_ref = 0;
@@ -72,7 +74,7 @@ struct FastScene {
     uint32_t max_leaf = 0;  // most primitives in a leaf, as the last build saw
     uint32_t top_end[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // wide nodes in the top k + 1 levels (breadth-first prefix)
     float root_min[4] = {0, 0, 0, 0}, root_max[4] = {0, 0, 0, 0};
-    size_t bytes() const { return boxes.bytes + refs.bytes; }
+    size_t bytes() const { return boxes.bytes + refs.bytes + up.bytes + leafpar.bytes; }
 };
 
 // Per-observer description of a batch (device copy in BatchCtx::obs).

@@ -55,6 +55,11 @@ struct WideScene {
     size_t oct_stride;    // float4 count of one copy (4 per wide node)
     const uint2* refs;    // packed (left, right)
     const float4* geoms;  // 5 float4 per hot record
+    // Up links, for ordering two hits of equal lambda the way the reference's traversal meets them
+    // (packet traversal only): up[w] = parent wide node of wide node w | side << 31 (side 1: the
+    // right child), ~0u for the root; leafpar[k] = the same for the leaf holding hot record k.
+    const uint32_t* up;
+    const uint32_t* leafpar;
     float4 root_min, root_max;
     uint32_t root_ref;    // packed reference of the root (a leaf, or wide node 0)
     uint32_t empty;       // no geometry at all
@@ -486,6 +491,180 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
         cur = st.get_ref(--sp);
         if (COUNT && (cur & REF_LEAF)) ++work.leaves;
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Packet traversal: the closest-hit queries of a warp's 32 lanes (the primary rays of one tile of
+// neighbouring pixels) walked as one. The warp steps through one node sequence. At an internal node
+// every lane that takes part tests both child boxes against its own ray, bounded by its own
+// closest hit so far; a child is entered when some lane enters it, and when lanes enter both, the
+// child that more of them enter first goes first (the left one on a tie), the other pushed with each
+// lane's entry parameter (+inf where the lane misses it) and taken again when some lane still
+// enters it before its closest hit. At a leaf every lane that takes part tests the records in
+// order. Rays of neighbouring pixels walk nearly the same nodes (on the 7.9M-tet workload the union
+// of a 4x8 tile's node visits is 6% above one ray's), so the warp runs one instruction stream with
+// warp-wide loads of one node or record, where the per-lane order runs the node and record code
+// side by side over lanes standing at different nodes.
+//
+// The result of each lane is closest_lean's. The closest hit so far is never nearer than the
+// reference's final one, so no box the reference enters on the way to its hit is culled, and that
+// hit is tested; no nearer hit exists among the records tested; of hits at equal lambda the lane
+// keeps the one the reference's near-first order meets first (packet_precedes). This holds as long
+// as every hit lies inside the entry parameter of its leaf's box as computed (the build pads every
+// record's box by 1e-4, far above the rounding of the slab and hit arithmetic).
+// ---------------------------------------------------------------------------------------------
+
+// Whether hot record a comes before hot record b in the reference's visiting order for this ray
+// (a != b): at their lowest common ancestor the near child (smaller entry parameter, the left one on
+// equal entries) is entered first; within one leaf, records in index order.
+template <bool OCT>
+__device__ __noinline__ bool packet_precedes(const WideScene& s, uint32_t a, uint32_t b, float4 no, float4 inv, float t_min,
+                                             uint32_t* err) {
+    if (s.root_ref & REF_LEAF) return a < b;
+    const uint32_t pa = __ldg(s.leafpar + a), pb = __ldg(s.leafpar + b);
+    if (pa == pb) return a < b;
+    constexpr uint32_t NODE = 0x7FFFFFFFu;
+    uint32_t na = pa & NODE, nb = pb & NODE, sa = pa >> 31, sb = pb >> 31;
+    uint32_t da = 0, db = 0;
+    for (uint32_t w = na; da <= FAST_MAX_DEPTH; ++da) {
+        const uint32_t u = __ldg(s.up + w);
+        if (u == ~0u) break;
+        w = u & NODE;
+    }
+    for (uint32_t w = nb; db <= FAST_MAX_DEPTH; ++db) {
+        const uint32_t u = __ldg(s.up + w);
+        if (u == ~0u) break;
+        w = u & NODE;
+    }
+    if (da > FAST_MAX_DEPTH || db > FAST_MAX_DEPTH) {
+        atomicOr(err, ERR_BAD_INDEX);
+        return a < b;
+    }
+    // Climb to equal depth, then together to the first common node; (n, s): the branch towards the
+    // record is child s of node n.
+    for (; da > db; --da) {
+        const uint32_t u = __ldg(s.up + na);
+        sa = u >> 31;
+        na = u & NODE;
+    }
+    for (; db > da; --db) {
+        const uint32_t u = __ldg(s.up + nb);
+        sb = u >> 31;
+        nb = u & NODE;
+    }
+    for (; na != nb; --da) {
+        if (da == 0) {
+            atomicOr(err, ERR_BAD_INDEX);
+            return a < b;
+        }
+        const uint32_t ua = __ldg(s.up + na), ub = __ldg(s.up + nb);
+        sa = ua >> 31;
+        na = ua & NODE;
+        sb = ub >> 31;
+        nb = ub & NODE;
+    }
+    const float4* bx = (OCT ? octant_boxes(s, inv) : s.boxes) + 4ull * na;
+    const float4 b0 = __ldg(bx), b1 = __ldg(bx + 1), b2 = __ldg(bx + 2), b3 = __ldg(bx + 3);
+    const float big = 3.0e38f;  // the entry parameters do not depend on the exit bound
+    float enl, exl, enr, exr;
+    if (OCT) {
+        slab_octant(b0, b1, no, inv, t_min, big, &enl, &exl);
+        slab_octant(b2, b3, no, inv, t_min, big, &enr, &exr);
+    } else {
+        slab_interval(b0, b1, no, inv, t_min, big, &enl, &exl);
+        slab_interval(b2, b3, no, inv, t_min, big, &enr, &exr);
+    }
+    const bool left_first = enl <= enr;
+    return sa == 0 ? left_first : !left_first;
+}
+
+// The packet form of closest_lean for the whole warp (all 32 lanes call it together, converged).
+// `in`: this lane's ray enters the scene's box (the others take no part). Returns the slot or -1;
+// `t_max` ends as the closest hit's parameter.
+template <bool OCT, class Stack>
+__device__ __forceinline__ int closest_packet(const WideScene& s, bool in, float4 no, float4 d, float4 inv, float t_min,
+                                              float& t_max, GeomHit& best, const Stack& st, uint32_t* err) {
+    constexpr uint32_t FULL = 0xFFFFFFFFu;
+    const float none = __uint_as_float(0x7F800000u);  // +inf: the lane does not enter the pushed child
+    const float4* ob = OCT ? octant_boxes(s, inv) : s.boxes;
+    int slot = -1, sp = 0;
+    uint32_t visits = 0;
+    float t_below = __uint_as_float(__float_as_uint(t_max) - 1u);
+    uint32_t cur = s.root_ref;
+    for (;;) {
+        if (cur & REF_LEAF) {
+            const uint32_t k = cur & REF_FIRST_MASK;
+            if (in) {
+                GeomHit gh;
+                // Hits up to and including t_max, so that a hit at the closest hit's lambda is seen.
+                if (intersect_lean(s.geoms + 5u * k, no, d, t_min, __uint_as_float(__float_as_uint(t_max) + 1u), &gh)) {
+                    if (gh.lambda < t_max) {
+                        t_max = gh.lambda;
+                        t_below = __uint_as_float(__float_as_uint(t_max) - 1u);
+                        best = gh;
+                        slot = (int)k;
+                    } else if (slot >= 0 && packet_precedes<OCT>(s, k, (uint32_t)slot, no, inv, t_min, err)) {
+                        best = gh;
+                        slot = (int)k;
+                    }
+                }
+            }
+            cur += REF_NEXT_PRIM;
+            if (cur & REF_COUNT_MASK) continue;
+        } else {
+            if (++visits > MAX_VISITS_FAST) {
+                atomicOr(err, ERR_TRAVERSAL_LIMIT);
+                break;
+            }
+            const uint2 r = __ldg(s.refs + cur);
+            bool hl = false, hr = false;
+            float enl = none, enr = none;
+            if (in) {
+                const float4* b = ob + 4ull * cur;
+                const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
+                float exl, exr;
+                if (OCT) {
+                    slab_octant(lnear, lfar, no, inv, t_min, t_below, &enl, &exl);
+                    slab_octant(rnear, rfar, no, inv, t_min, t_below, &enr, &exr);
+                } else {
+                    slab_interval(lnear, lfar, no, inv, t_min, t_below, &enl, &exl);
+                    slab_interval(rnear, rfar, no, inv, t_min, t_below, &enr, &exr);
+                }
+                hl = exl >= enl;  // and enl < t_max
+                hr = exr >= enr;
+            }
+            const uint32_t ml = __ballot_sync(FULL, hl), mr = __ballot_sync(FULL, hr);
+            if (ml && mr) {
+                const uint32_t nl = __popc(__ballot_sync(FULL, hl && (!hr || enl <= enr)));
+                const bool left_first = 2u * nl >= (uint32_t)__popc(ml | mr);
+                if (sp < FAST_STACK)
+                    st.put(sp++, left_first ? make_uint2(r.y, __float_as_uint(hr ? enr : none))
+                                            : make_uint2(r.x, __float_as_uint(hl ? enl : none)));
+                else atomicOr(err, ERR_BAD_INDEX);
+                cur = left_first ? r.x : r.y;
+                in = left_first ? hl : hr;
+                continue;
+            }
+            if (ml | mr) {
+                cur = ml ? r.x : r.y;
+                in = ml ? hl : hr;
+                continue;
+            }
+        }
+        bool found = false;
+        while (sp > 0) {
+            const uint2 e = st.get(--sp);
+            const bool take = __uint_as_float(e.y) < t_max;
+            if (__any_sync(FULL, take)) {
+                cur = e.x;
+                in = take;
+                found = true;
+                break;
+            }
+        }
+        if (!found) break;
+    }
+    return slot;
 }
 
 }  // namespace srk

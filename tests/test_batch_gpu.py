@@ -82,6 +82,7 @@ def test_every_schedule_gives_the_same_frames(engine, scene, tiling):
     t = engine.tuning(3)
     t.tile_w, t.tile_h, t.chunk_tiles, t.refill_lanes, t.leaf_coop, t.leaf_batch = tw, th, chunk, refill, coop, leaf_batch
     t.home_pct = home
+    t.packet = 0  # the per-ray kernels' schedules
     engine.set_tuning(3, t)
     try:
         obs, us, cams = _observers(13, 4, int(scene.info.n_nodes), scale=4)
@@ -105,6 +106,7 @@ def test_shared_memory_stack_gives_the_same_frames_and_visits(engine, scene, sta
     t = engine.tuning(3)
     t.tile_w, t.tile_h, t.chunk_tiles, t.refill_lanes, t.leaf_coop, t.leaf_batch, t.home_pct = 4, 8, 1, 32, 0, 1, 0
     t.block_threads, t.blocks_per_sm, t.stack_smem = threads, blocks, stack
+    t.packet = 0
     engine.set_tuning(3, t)
     try:
         obs, us, cams = _observers(14, 4, int(scene.info.n_nodes), scale=4)
@@ -135,7 +137,11 @@ def test_invalid_tuning_rejected(engine, scene):
     with pytest.raises(sr.SrError):
         engine.set_tuning(3, t)
     t = engine.tuning(3)
-    t.reserved = 1
+    t.packet = 2
+    with pytest.raises(sr.SrError):
+        engine.set_tuning(3, t)
+    t = engine.tuning(3)
+    t.packet, t.stack_smem = 1, 12  # the packet form keeps its stack in local memory
     with pytest.raises(sr.SrError):
         engine.set_tuning(3, t)
 
@@ -225,7 +231,7 @@ def test_compact_layout_gives_the_same_frames_and_visits(engine, scene, stack):
     keep = engine.tuning(3)
     t = engine.tuning(3)
     t.tile_w, t.tile_h, t.chunk_tiles, t.refill_lanes, t.leaf_coop, t.leaf_batch, t.home_pct = 4, 8, 1, 32, 0, 1, 0
-    t.stack_smem, t.top_levels = stack, 0
+    t.stack_smem, t.top_levels, t.packet = stack, 0, 0
     cam = sr.camera((0.0, 0.0, 0.0, -10.0), 90.0, rapidity=(0.3, 0.1, -0.2))
     u = sr.uniforms(cam, 256, 160, 0, 0, 0, num_nodes=int(scene.info.n_nodes))
     engine.set_tuning(3, t)
@@ -257,6 +263,7 @@ def test_staged_top_levels_give_the_same_frames_and_visits(engine, scene, stack,
     t = engine.tuning(3)
     t.tile_w, t.tile_h, t.chunk_tiles, t.refill_lanes, t.leaf_coop, t.leaf_batch, t.home_pct = 4, 8, 1, 32, 0, 1, 0
     t.block_threads, t.blocks_per_sm, t.stack_smem, t.top_levels = 128, 8, stack, top
+    t.packet = 0
     engine.set_tuning(3, t)
     try:
         obs, us, cams = _observers(16, 4, int(scene.info.n_nodes), scale=4)

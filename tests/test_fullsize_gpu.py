@@ -36,7 +36,7 @@ def full(engine):
     del s32
     f32 = engine.render(20, u, path=sr.SR_PATH_FAST, aux=True)
     f64 = engine.render(20, u, path=sr.SR_PATH_FAST, aux=True, cam=sr.cam64((0.0, 0.0, 0.0, 0.0), rap))
-    return dict(rap=rap, cfg=cfg, base=base, near=near, f32=f32, f64=f64)
+    return dict(rap=rap, cfg=cfg, base=base, near=near, f32=f32, f64=f64, u=u, n_nodes=int(u.num_nodes))
 
 
 @pytest.fixture(scope="module")
@@ -83,3 +83,35 @@ def test_f32_camera_frame_against_fp64_oracle(full, fp64_ref):
     same, lam_rel, tau_rel, d, ok = _against_fp64(full["f32"], fp64_ref, full["near"], "f32 camera")
     assert same.mean() >= 0.9999
     assert d[ok].max() <= 1
+
+
+def test_packet_traversal_at_full_size(engine, full):
+    """The packet traversal (SrTuning.packet = 1) on the full-size scene: the workload's own frame
+    bit-identical to the f32 oracle, and the bench's other seven observers (FP64 cameras) identical
+    to the per-ray order in hit record, lambda and tau."""
+    from specrel_b200 import shard
+    keep = engine.tuning(20)
+
+    def with_packet(on, fn):
+        t = engine.tuning(20)
+        t.packet = on
+        engine.set_tuning(20, t)
+        return fn()
+
+    try:
+        fr = with_packet(1, lambda: engine.render(20, full["u"], path=sr.SR_PATH_FAST, aux=True))
+        rep = compare(fr, full["base"], full["near"])
+        print("7.9M tets 1280x800, packet traversal, f32 camera vs f32 oracle:", rep)
+        assert rep.hit_match == 1.0 and rep.lam_max_rel == 0.0 and rep.tau_max_rel == 0.0
+        assert rep.rgb_max_unmasked <= 1
+        for r in shard.observer_rapidities(1, 0, 8, full["rap"])[1:]:
+            u = sr.uniforms(sr.camera(rapidity=r), W, H, 0, 1, 0, num_nodes=full["n_nodes"])
+            c = sr.cam64((0.0, 0.0, 0.0, 0.0), r)
+            a = with_packet(1, lambda: engine.render(20, u, path=sr.SR_PATH_FAST, aux=True, cam=c))
+            b = with_packet(0, lambda: engine.render(20, u, path=sr.SR_PATH_FAST, aux=True, cam=c))
+            assert (a.hit_id == b.hit_id).all()
+            assert (a.lam.view(np.uint32) == b.lam.view(np.uint32)).all()
+            assert (a.tau.view(np.uint32) == b.tau.view(np.uint32)).all()
+            assert (a.rgb == b.rgb).all()
+    finally:
+        engine.set_tuning(20, keep)
