@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--no-parity", action="store_true", help="skip the FP64-oracle parity block")
     ap.add_argument("--no-extra", action="store_true", help="skip the config4 / config5 / fresh-observer legs")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch parameters")
+    ap.add_argument("--no-roof", action="store_true",
+                    help="skip the coherent-ray roof (24 extra batches; for profiler launch lists)")
     ap.add_argument("--bodies", type=int, default=64,
                     help="icospheres in the scene (64 is the workload; fewer only for small profiling captures)")
     ap.add_argument("--workload", choices=["config2", "config4", "config5", "tunings"], default="config2",
@@ -601,7 +603,7 @@ def run_engine(args, rank, world, local):
         tuning = eng.tuning(0)
         stats = eng.stats(0)
         roof = None
-        if scene.num_stars == 0:
+        if scene.num_stars == 0 and not args.no_roof:
             roof = coherent_roof(sr, eng, scene, ptr, B, args.seed, work, float(np.median(trace_ms)))
 
         if not args.no_extra:
@@ -657,7 +659,7 @@ def run_engine(args, rank, world, local):
         "roofline": {"bound": "issue", "kernel": "k_trace_lean",
                      **(roof if roof is not None else
                         {"achieved": None, "peak": None, "unit": "Mrays/s", "frac": None,
-                         "peak_kind": "not measured (scene with stars)"}),
+                         "peak_kind": "not measured (--no-roof, or a scene with stars)"}),
                      "hbm_achieved_gbs": achieved, "hbm_peak_gbs": peak, "hbm_frac": achieved / peak,
                      "hbm_peak_kind": peak_kind,
                      "note": "frac = the trace kernel's time on this batch's counted work at warp-coherent speed "
