@@ -673,7 +673,7 @@ __device__ __forceinline__ uint32_t next_tile(const TraceBatchArgs& a, uint32_t 
 // (min, max) boxes then their references. PKT: each warp walks its tile's primary rays as one
 // packet (closest_packet; built with SS == 0, no staging and no counting).
 template <bool COUNT, int SS, bool OCT, bool TOP, bool PKT>
-__global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
+__global__ void __launch_bounds__(512) k_trace_lean(const __grid_constant__ TraceBatchArgs a) {
     static_assert(!PKT || (!COUNT && SS == 0 && !TOP), "the packet form is built alone");
     const uint32_t lane = threadIdx.x & 31u;
     Work wp{0, 0, 0}, wsh{0, 0, 0};
@@ -725,35 +725,47 @@ __global__ void __launch_bounds__(512) k_trace_lean(TraceBatchArgs a) {
                                                      top);
             }
         }
-        if (!valid) continue;
-        const SrGpuUniforms& U = a.U[obs];
-        a.hits[pix] = make_float4(best.lambda, best.u, best.v, best.w);
-        a.slots[pix] = slot < 0 ? 0xFFFFFFFFu : (uint32_t)slot;
+        // The main light's shadow query of the pixel (compute_illumination's condition,
+        // renderer.rs:617-633): per lane, or, in the packet form, the warp's queries as one packet.
         uint8_t sh = 0;
-        if (slot >= 0 && U.mode == 0u && U.shadow_mode != 0u && U.num_flashes == 0u) {
-            // compute_illumination's shadow-ray condition (renderer.rs:617-633).
-            const float4* at = a.attrs + 12u * (uint32_t)slot;
-            const uint32_t mat = __float_as_uint(__ldg(at + 10).z);
-            if (__float_as_uint(__ldg(a.mats + 3u * mat + 2u).y) == 0u) {
-                const float4 ev = sub4(mul4(d, best.lambda), no);  // o + d * lambda
-                float4 tl;
-                float dist;
-                // The camera is read again here rather than kept in registers across the traversal.
-                light_ray(U, cam_of(a.cam, obs), ev, &tl, &dist);
-                if (fmaxf(rest_frame_cos(tl, __ldg(at + 8), __ldg(at + 9)), 0.0f) > 0.0f) {
-                    // Bvh4D::is_occluded(hit.event, to_light, 2e-3, dist - 2e-3) (renderer.rs:636-641).
-                    sh = 1;
-                    const float4 sinv = v4(safe_inv(tl.x), safe_inv(tl.y), safe_inv(tl.z), safe_inv(tl.w));
-                    const float s0 = 2e-3f, s1 = dist - 2e-3f;
-                    float en, ex;
-                    slab_interval(a.ws.root_min, a.ws.root_max, neg4(ev), sinv, s0, s1, &en, &ex);
-                    if (ex >= en && any_lean<COUNT, OCT, TOP>(a.ws, a.ws.root_ref, neg4(ev), tl, sinv, s0, s1, st, a.err,
-                                                              wsh, top))
-                        sh = 2;
+        bool shadow_in = false;
+        float4 sno = v4(0.0f, 0.0f, 0.0f, 0.0f), sd = v4(0.0f, 0.0f, 1.0f, 0.0f), sinv = v4(1.0f, 1.0f, 1.0f, 1.0f);
+        float s0 = 0.0f, s1 = 0.0f;
+        if (valid) {
+            const SrGpuUniforms& U = a.U[obs];
+            a.hits[pix] = make_float4(best.lambda, best.u, best.v, best.w);
+            a.slots[pix] = slot < 0 ? 0xFFFFFFFFu : (uint32_t)slot;
+            if (slot >= 0 && U.mode == 0u && U.shadow_mode != 0u && U.num_flashes == 0u) {
+                const float4* at = a.attrs + 12u * (uint32_t)slot;
+                const uint32_t mat = __float_as_uint(__ldg(at + 10).z);
+                if (__float_as_uint(__ldg(a.mats + 3u * mat + 2u).y) == 0u) {
+                    const float4 ev = sub4(mul4(d, best.lambda), no);  // o + d * lambda
+                    float4 tl;
+                    float dist;
+                    // The camera is read again here rather than kept in registers across the traversal.
+                    light_ray(U, cam_of(a.cam, obs), ev, &tl, &dist);
+                    if (fmaxf(rest_frame_cos(tl, __ldg(at + 8), __ldg(at + 9)), 0.0f) > 0.0f) {
+                        // Bvh4D::is_occluded(hit.event, to_light, 2e-3, dist - 2e-3) (renderer.rs:636-641).
+                        sh = 1;
+                        sno = neg4(ev);
+                        sd = tl;
+                        sinv = v4(safe_inv(tl.x), safe_inv(tl.y), safe_inv(tl.z), safe_inv(tl.w));
+                        s0 = 2e-3f;
+                        s1 = dist - 2e-3f;
+                        float en, ex;
+                        slab_interval(a.ws.root_min, a.ws.root_max, sno, sinv, s0, s1, &en, &ex);
+                        shadow_in = ex >= en;
+                    }
                 }
             }
         }
-        a.shadow[pix] = sh;
+        if constexpr (PKT) {
+            if (__any_sync(0xFFFFFFFFu, shadow_in) && any_packet<OCT>(a.ws, shadow_in, sno, sd, sinv, s0, s1, st, a.err))
+                sh = 2;
+        } else if (shadow_in && any_lean<COUNT, OCT, TOP>(a.ws, a.ws.root_ref, sno, sd, sinv, s0, s1, st, a.err, wsh, top)) {
+            sh = 2;
+        }
+        if (valid) a.shadow[pix] = sh;
     }
     if (COUNT) {
         add_work(a.work, wp);

@@ -617,22 +617,20 @@ __device__ __forceinline__ int closest_packet(const WideScene& s, bool in, float
                 break;
             }
             const uint2 r = __ldg(s.refs + cur);
-            bool hl = false, hr = false;
-            float enl = none, enr = none;
-            if (in) {
-                const float4* b = ob + 4ull * cur;
-                const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
-                float exl, exr;
-                if (OCT) {
-                    slab_octant(lnear, lfar, no, inv, t_min, t_below, &enl, &exl);
-                    slab_octant(rnear, rfar, no, inv, t_min, t_below, &enr, &exr);
-                } else {
-                    slab_interval(lnear, lfar, no, inv, t_min, t_below, &enl, &exl);
-                    slab_interval(rnear, rfar, no, inv, t_min, t_below, &enr, &exr);
-                }
-                hl = exl >= enl;  // and enl < t_max
-                hr = exr >= enr;
+            // Every lane computes (the warp runs the code once either way); lanes that take no part
+            // are masked out, so the step has no divergent branch.
+            const float4* b = ob + 4ull * cur;
+            const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
+            float enl, exl, enr, exr;
+            if (OCT) {
+                slab_octant(lnear, lfar, no, inv, t_min, t_below, &enl, &exl);
+                slab_octant(rnear, rfar, no, inv, t_min, t_below, &enr, &exr);
+            } else {
+                slab_interval(lnear, lfar, no, inv, t_min, t_below, &enl, &exl);
+                slab_interval(rnear, rfar, no, inv, t_min, t_below, &enr, &exr);
             }
+            const bool hl = in && exl >= enl;  // and enl < t_max
+            const bool hr = in && exr >= enr;
             const uint32_t ml = __ballot_sync(FULL, hl), mr = __ballot_sync(FULL, hr);
             if (ml && mr) {
                 const uint32_t nl = __popc(__ballot_sync(FULL, hl && (!hr || enl <= enr)));
@@ -665,6 +663,77 @@ __device__ __forceinline__ int closest_packet(const WideScene& s, bool in, float
         if (!found) break;
     }
     return slot;
+}
+
+// The packet form of any_lean for the whole warp (all 32 lanes call it together, converged): the
+// lanes' any-hit queries walked as one node sequence, left child first. A lane takes part in a
+// node or leaf its own ray enters, and stops once it has a hit; the walk ends when no lane still
+// searching takes part in anything left. Every lane tests records of leaves its ray enters until
+// one hits, so its answer is any_lean's (an any-hit answer does not depend on the order).
+// `in`: this lane has a query whose ray enters the scene's box.
+template <bool OCT, class Stack>
+__device__ __forceinline__ bool any_packet(const WideScene& s, bool in, float4 no, float4 d, float4 inv, float t_min,
+                                           float t_max, const Stack& st, uint32_t* err) {
+    constexpr uint32_t FULL = 0xFFFFFFFFu;
+    const float4* ob = OCT ? octant_boxes(s, inv) : s.boxes;
+    bool hit = false, part = in;
+    int sp = 0;
+    uint32_t visits = 0;
+    uint32_t cur = s.root_ref;
+    for (;;) {
+        if (cur & REF_LEAF) {
+            if (part && !hit) {
+                GeomHit gh;
+                hit = intersect_lean(s.geoms + 5u * (cur & REF_FIRST_MASK), no, d, t_min, t_max, &gh);
+            }
+            cur += REF_NEXT_PRIM;
+            if ((cur & REF_COUNT_MASK) && __any_sync(FULL, part && !hit)) continue;
+        } else {
+            if (++visits > MAX_VISITS_FAST) {
+                atomicOr(err, ERR_TRAVERSAL_LIMIT);
+                break;
+            }
+            const uint2 r = __ldg(s.refs + cur);
+            const float4* b = ob + 4ull * cur;
+            const float4 lnear = __ldg(b), lfar = __ldg(b + 1), rnear = __ldg(b + 2), rfar = __ldg(b + 3);
+            float enl, exl, enr, exr;
+            if (OCT) {
+                slab_octant(lnear, lfar, no, inv, t_min, t_max, &enl, &exl);
+                slab_octant(rnear, rfar, no, inv, t_min, t_max, &enr, &exr);
+            } else {
+                slab_interval(lnear, lfar, no, inv, t_min, t_max, &enl, &exl);
+                slab_interval(rnear, rfar, no, inv, t_min, t_max, &enr, &exr);
+            }
+            const bool live = part && !hit;
+            const bool hl = live && exl >= enl, hr = live && exr >= enr;
+            const uint32_t ml = __ballot_sync(FULL, hl), mr = __ballot_sync(FULL, hr);
+            if (ml && mr) {
+                if (sp < FAST_STACK) st.put(sp++, make_uint2(r.y, hr ? 1u : 0u));
+                else atomicOr(err, ERR_BAD_INDEX);
+                cur = r.x;
+                part = hl;
+                continue;
+            }
+            if (ml | mr) {
+                cur = ml ? r.x : r.y;
+                part = ml ? hl : hr;
+                continue;
+            }
+        }
+        bool found = false;
+        while (sp > 0) {
+            const uint2 e = st.get(--sp);
+            const bool take = e.y != 0u && !hit;
+            if (__any_sync(FULL, take)) {
+                cur = e.x;
+                part = take;
+                found = true;
+                break;
+            }
+        }
+        if (!found) break;
+    }
+    return hit;
 }
 
 }  // namespace srk

@@ -137,3 +137,21 @@ def test_equal_lambda_hits_resolve_in_the_reference_order(engine):
         assert seen_copy > 100 and seen_orig > 100
     finally:
         engine.set_tuning(TIES, keep)
+
+
+@pytest.mark.parametrize("threads,blocks", [(64, 16), (256, 4), (512, 2)])
+def test_packet_block_shapes_give_the_same_frames(engine, scene, threads, blocks):
+    """The packet kernels (primary rays and the main light's shadow rays) in other block shapes:
+    the per-ray frames and the plain path's hit records."""
+    keep = engine.tuning(IDX)
+    try:
+        us, cams = _observers(33, 4, int(scene.info.n_nodes), 2)
+        _tuning(engine, IDX, packet=0)
+        per_ray = _batch(engine, IDX, us, cams)
+        _tuning(engine, IDX, packet=1, block_threads=threads, blocks_per_sm=blocks)
+        assert (_batch(engine, IDX, us, cams) == per_ray).all()
+        u, c = us[0], cams[0]
+        _aux_equal(engine.render(IDX, u, path=sr.SR_PATH_FAST, aux=True, cam=c),
+                   engine.render(IDX, u, path=sr.SR_PATH_PLAIN, aux=True, cam=c))
+    finally:
+        engine.set_tuning(IDX, keep)
