@@ -527,11 +527,15 @@ typedef struct SrTuning {
     uint32_t top_levels;      /* levels of the wide tree staged in shared memory per block, 0..8
                                  (0: none); with stack_smem 0 or 12; the compact layout
                                  (sr_set_layout) stages none */
-    uint32_t packet;          /* 1: the warp walks its tile's primary rays as one packet (one node
-                                 sequence for its 32 rays, each lane with its own closest hit;
-                                 the same hits as the per-ray order); with stack_smem 0,
-                                 top_levels 0 and the single-tile schedule; 0: each ray walks the
-                                 tree in its own near-first order */
+    uint32_t packet;          /* 1 (the default): the warp walks its tile's primary rays as one
+                                 packet (one node sequence for its 32 rays, each lane with its
+                                 own closest hit), then its main-light shadow rays likewise; the
+                                 same hits as the per-ray order, equal-lambda ties included, as
+                                 long as every hit lies inside its leaf box's computed entry
+                                 parameter (the records' 1e-4 box padding keeps it there); with
+                                 stack_smem 0, top_levels 0 and the single-tile schedule.
+                                 0: each ray walks the tree in its own near-first order (work
+                                 counts, SR_FLAG_COUNT_WORK, always come from this order) */
 } SrTuning;
 sr_status sr_get_tuning(const sr_ctx* ctx, uint32_t scene_idx, SrTuning* out);
 sr_status sr_set_tuning(sr_ctx* ctx, uint32_t scene_idx, const SrTuning* t);
