@@ -531,8 +531,9 @@ typedef struct SrTuning {
                                  packet (one node sequence for its 32 rays, each lane with its
                                  own closest hit), then its main-light shadow rays likewise; the
                                  same hits as the per-ray order, equal-lambda ties included, as
-                                 long as every hit lies inside its leaf box's computed entry
-                                 parameter (the records' 1e-4 box padding keeps it there); with
+                                 long as every hit lies beyond its leaf box's computed entry
+                                 parameter (the records' 1e-4 box padding keeps a margin of
+                                 1e-4 / |d| in ray parameter against its rounding); with
                                  stack_smem 0, top_levels 0 and the single-tile schedule.
                                  0: each ray walks the tree in its own near-first order (work
                                  counts, SR_FLAG_COUNT_WORK, always come from this order) */

@@ -510,8 +510,11 @@ __device__ __forceinline__ bool any_lean(const WideScene& s, uint32_t cur, float
 // reference's final one, so no box the reference enters on the way to its hit is culled, and that
 // hit is tested; no nearer hit exists among the records tested; of hits at equal lambda the lane
 // keeps the one the reference's near-first order meets first (packet_precedes). This holds as long
-// as every hit lies inside the entry parameter of its leaf's box as computed (the build pads every
-// record's box by 1e-4, far above the rounding of the slab and hit arithmetic).
+// as every hit lies beyond the entry parameter of its leaf's box as computed. A hit's event passes
+// the barycentric test, so it lies inside the record's box, which the build pads by 1e-4: in ray
+// parameter a margin of 1e-4 / |d| on the entering axis, against a rounding of the computed entry
+// of order 1e-7 lambda; only hits far along a fast axis (lambda ~ 100 or more with |d| ~ 8) bring
+// the two within a factor of two.
 // ---------------------------------------------------------------------------------------------
 
 // Whether hot record a comes before hot record b in the reference's visiting order for this ray
