@@ -155,3 +155,48 @@ def test_packet_block_shapes_give_the_same_frames(engine, scene, threads, blocks
                    engine.render(IDX, u, path=sr.SR_PATH_PLAIN, aux=True, cam=c))
     finally:
         engine.set_tuning(IDX, keep)
+
+
+def test_packet_on_a_one_leaf_tree_and_tiny_frames(engine, scene):
+    """Edge cases of the packet walk against the per-ray and plain paths, hit records bit for bit:
+    a tree that is a single leaf (three records the cube scene's camera hits, so every ray tests
+    all of them in one leaf), and frames smaller than a tile or not a multiple of it (1x1, 3x5,
+    7x9, 33x17), where a warp's lanes outside the frame take no part."""
+    cam = sr.camera((0.0, 0.0, 0.0, 0.0), 90.0)
+    u = sr.uniforms(cam, 160, 100, 0, 1, 0, num_nodes=int(scene.info.n_nodes))
+    full = engine.render(IDX, u, path=sr.SR_PATH_PLAIN, aux=True)
+    ids = np.unique(full.hit_id[full.hit_id != 0xFFFFFFFF])
+    assert len(ids) >= 3
+    boxes, geoms, attrs, p = sr.synth_scene(1, 2).build_inputs()
+    pick = ids[np.linspace(0, len(ids) - 1, 3).astype(int)]
+    b = np.ascontiguousarray(boxes[pick], np.float32)
+    nodes = np.zeros(5, L.NODE_DTYPE)
+    order = np.zeros(3, np.uint32)
+    nn, med = C.c_uint32(), C.c_uint32()
+    assert L.lib().sr_bvh_build_host(b.ctypes.data, 3, 1, nodes.ctypes.data, len(nodes), order.ctypes.data,
+                                     C.byref(nn), C.byref(med)) == L.SR_OK
+    assert nn.value == 1 and nodes[0]["count"] == 3  # the root is the one leaf
+    tiny = sr.PackedScene(nodes[:1].copy(), geoms[pick][order], attrs[pick][order], p.materials, p.stars, 0,
+                          p.light_pos, order.copy())
+    engine.upload(TIES, tiny)
+    keep = engine.tuning(TIES)
+    try:
+        for packet in (0, 1):
+            _tuning(engine, TIES, packet=packet)
+            f = engine.render(TIES, sr.uniforms(cam, 160, 100, 0, 1, 0, num_nodes=1), path=sr.SR_PATH_FAST, aux=True)
+            _aux_equal(f, engine.render(TIES, sr.uniforms(cam, 160, 100, 0, 1, 0, num_nodes=1), path=sr.SR_PATH_PLAIN,
+                                        aux=True))
+            assert (f.hit_id != 0xFFFFFFFF).sum() > 0
+    finally:
+        engine.set_tuning(TIES, keep)
+    keep = engine.tuning(IDX)
+    try:
+        for w, h in ((1, 1), (3, 5), (7, 9), (33, 17)):
+            uw = sr.uniforms(sr.camera((0.0, 0.0, 0.0, -10.0), 40.0, rapidity=(0.2, 0.0, 0.1)), w, h, 0, 1, 0,
+                             num_nodes=int(scene.info.n_nodes))
+            ref = engine.render(IDX, uw, path=sr.SR_PATH_PLAIN, aux=True)
+            for packet in (0, 1):
+                _tuning(engine, IDX, packet=packet)
+                _aux_equal(engine.render(IDX, uw, path=sr.SR_PATH_FAST, aux=True), ref)
+    finally:
+        engine.set_tuning(IDX, keep)
