@@ -546,8 +546,11 @@ def run_engine(args, rank, world, local):
 
         # The compact node layout (one copy of the child boxes instead of 16 sign-octant copies) on
         # the same batches: what the octant copies cost in memory and buy in speed.
+        # Every rank takes the leg or none does (the automatic layout depends on each GPU's free
+        # memory, and the leg holds a collective).
         compact = None
-        if not args.no_extra and eng.stats(0).box_copies == 16:
+        all_octant = max_over_ranks(0.0 if eng.stats(0).box_copies == 16 else 1.0) == 0.0
+        if not args.no_extra and all_octant:
             eng.set_layout(0, sr._lib.SR_LAYOUT_COMPACT)
             compact_stats = eng.stats(0)
             for _ in range(max(1, args.warmup)):
