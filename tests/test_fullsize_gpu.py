@@ -33,10 +33,17 @@ def full(engine):
     cfg = O.make_config(W, H, 0, 1, 0)
     base, near = oracle_frames(s32, O.make_camera(rapidity=rap), cfg, threads=THREADS)
     u = sr.uniforms(sr.camera(rapidity=rap), W, H, 0, 1, 0, num_nodes=int(s32.info.n_nodes))
+    # The three bench observers with the largest rapidities (the fastest ray axes), rendered by the
+    # f32 oracle too.
+    from specrel_b200 import shard
+    raps = shard.observer_rapidities(1, 0, 8, rap)[1:]
+    fast = sorted(raps, key=lambda r: -float(np.dot(r, r)))[:3]
+    boosted = [(r,) + oracle_frames(s32, O.make_camera(rapidity=r), cfg, threads=THREADS) for r in fast]
     del s32
     f32 = engine.render(20, u, path=sr.SR_PATH_FAST, aux=True)
     f64 = engine.render(20, u, path=sr.SR_PATH_FAST, aux=True, cam=sr.cam64((0.0, 0.0, 0.0, 0.0), rap))
-    return dict(rap=rap, cfg=cfg, base=base, near=near, f32=f32, f64=f64, u=u, n_nodes=int(u.num_nodes))
+    return dict(rap=rap, cfg=cfg, base=base, near=near, f32=f32, f64=f64, u=u, n_nodes=int(u.num_nodes),
+                boosted=boosted)
 
 
 @pytest.fixture(scope="module")
@@ -115,3 +122,17 @@ def test_packet_traversal_at_full_size(engine, full):
             assert (a.rgb == b.rgb).all()
     finally:
         engine.set_tuning(20, keep)
+
+
+def test_boosted_observers_equal_f32_oracle(engine, full):
+    """The bench's three most boosted observers (|phi| up to 2: the rays' fastest axes, where the
+    packet walk's margin between a hit and its leaf box's entry is thinnest) on the default fast
+    path (the packet traversal) against the f32 oracle at full size: hit ids, lambda and tau bit for
+    bit, RGB8 within 1/255 outside the near-threshold mask."""
+    assert engine.tuning(20).packet == 1
+    for r, base, near in full["boosted"]:
+        u = sr.uniforms(sr.camera(rapidity=r), W, H, 0, 1, 0, num_nodes=full["n_nodes"])
+        rep = compare(engine.render(20, u, path=sr.SR_PATH_FAST, aux=True), base, near)
+        print(f"7.9M tets 1280x800, rapidity |phi| = {float(np.linalg.norm(r)):.2f}, packet vs f32 oracle:", rep)
+        assert rep.hit_match == 1.0 and rep.lam_max_rel == 0.0 and rep.tau_max_rel == 0.0
+        assert rep.rgb_max_unmasked <= 1
