@@ -23,6 +23,9 @@ pytestmark = pytest.mark.gpu
 
 W, H = 1280, 800
 THREADS = os.cpu_count() or 1
+# (rapidity, yaw in degrees, slice mode): 0 past light cone, 1 God's-eye, 2 future light cone.
+VIEWS = [((2.8, 0.0, 0.0), 0.0, 0), ((-2.9, 0.4, 0.5), 35.0, 0), ((0.0, -2.5, 1.0), 0.0, 1),
+         ((1.5, 1.5, 1.5), -20.0, 2)]
 
 
 @pytest.fixture(scope="module")
@@ -39,11 +42,17 @@ def full(engine):
     raps = shard.observer_rapidities(1, 0, 8, rap)[1:]
     fast = sorted(raps, key=lambda r: -float(np.dot(r, r)))[:3]
     boosted = [(r,) + oracle_frames(s32, O.make_camera(rapidity=r), cfg, threads=THREADS) for r in fast]
+    # Views beyond the bench's: rapidities up to |phi| = 3, the God's-eye and future-cone slices, a
+    # turned camera.
+    views = []
+    for r, yaw, slice_mode in VIEWS:
+        c = O.make_config(W, H, 0, 1 if slice_mode == 0 else 2, slice_mode)
+        views.append((r, yaw, slice_mode) + oracle_frames(s32, O.make_camera(rapidity=r, yaw=yaw), c, threads=THREADS))
     del s32
     f32 = engine.render(20, u, path=sr.SR_PATH_FAST, aux=True)
     f64 = engine.render(20, u, path=sr.SR_PATH_FAST, aux=True, cam=sr.cam64((0.0, 0.0, 0.0, 0.0), rap))
     return dict(rap=rap, cfg=cfg, base=base, near=near, f32=f32, f64=f64, u=u, n_nodes=int(u.num_nodes),
-                boosted=boosted)
+                boosted=boosted, views=views)
 
 
 @pytest.fixture(scope="module")
@@ -134,5 +143,18 @@ def test_boosted_observers_equal_f32_oracle(engine, full):
         u = sr.uniforms(sr.camera(rapidity=r), W, H, 0, 1, 0, num_nodes=full["n_nodes"])
         rep = compare(engine.render(20, u, path=sr.SR_PATH_FAST, aux=True), base, near)
         print(f"7.9M tets 1280x800, rapidity |phi| = {float(np.linalg.norm(r)):.2f}, packet vs f32 oracle:", rep)
+        assert rep.hit_match == 1.0 and rep.lam_max_rel == 0.0 and rep.tau_max_rel == 0.0
+        assert rep.rgb_max_unmasked <= 1
+
+
+def test_sweep_of_views_equals_f32_oracle(engine, full):
+    """Views beyond the bench's observers on the default fast path (the packet traversal) against
+    the f32 oracle at full size: rapidities up to |phi| = 3, the God's-eye and future-cone slices, a
+    turned camera. Hit ids, lambda and tau bit for bit, RGB8 within 1/255 outside the mask."""
+    for r, yaw, slice_mode, base, near in full["views"]:
+        u = sr.uniforms(sr.camera(rapidity=r, yaw=yaw), W, H, 0, 1 if slice_mode == 0 else 2, slice_mode,
+                        num_nodes=full["n_nodes"])
+        rep = compare(engine.render(20, u, path=sr.SR_PATH_FAST, aux=True), base, near)
+        print(f"7.9M tets 1280x800, rapidity {r}, yaw {yaw}, slice {slice_mode}, packet vs f32 oracle:", rep)
         assert rep.hit_match == 1.0 and rep.lam_max_rel == 0.0 and rep.tau_max_rel == 0.0
         assert rep.rgb_max_unmasked <= 1
