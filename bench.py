@@ -17,6 +17,7 @@ observers, no data-path collective). The same line carries:
                hit-id agreement (the metric's "hit-ID match % vs FP64"), lambda / tau / RGB errors;
   e2e          the same batches through the C ABI with host buffers;
   value_fresh  every step a new seeded set of observers, L2 flushed before each step;
+  traversal_per_ray  the same batches with each ray walking the tree alone (no warp packets);
   config4      64 observers of mixed resolution and slice mode over the 147k-tet cube scene in one
                batch, against looping the plain path;
   config5      the image-loss gradient of one 1280x800 observer over 100k stars;
@@ -566,6 +567,26 @@ def run_engine(args, rank, world, local):
             eng.set_layout(0, sr._lib.SR_LAYOUT_AUTO)
             compact = (compact_stats, compact_ms)
 
+        # The per-ray traversal (each ray walks the tree alone, SrTuning.packet = 0) on the same
+        # batches, at its best measured launch shape: what the packet walk buys.
+        per_ray_ms = None
+        if not args.no_extra:
+            keep = eng.tuning(0)
+            t = eng.tuning(0)
+            t.packet, t.block_threads, t.blocks_per_sm, t.stack_smem, t.top_levels = 0, 128, 11, 0, 0
+            eng.set_tuning(0, t)
+            for _ in range(max(1, args.warmup)):
+                batch_step()
+            torch.cuda.synchronize()
+            barrier()
+            e0.record(stream)
+            for _ in range(args.steps):
+                batch_step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            per_ray_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+            eng.set_tuning(0, keep)
+
         # Fresh observers every step (new seeded rapidities, never rendered before), with L2 flushed
         # (a 256 MiB write) before each step; only the batches are inside the events.
         if not args.no_extra:
@@ -688,6 +709,12 @@ def run_engine(args, rank, world, local):
                                   "scene_device_bytes": int(cs.device_bytes), "box_copies": int(cs.box_copies),
                                   "how": "the same batches with SR_LAYOUT_COMPACT: one copy of the child boxes, "
                                          "per-axis min / max in the traversal"}
+    if per_ray_ms is not None:
+        line["traversal_per_ray"] = {"value": total_rays / (per_ray_ms / 1e3) / 1e6, "unit": UNIT,
+                                     "ms_per_step": per_ray_ms,
+                                     "how": "the same batches with SrTuning.packet = 0 (each ray walks the tree "
+                                            "alone, 128 threads x 11 blocks per SM); the headline walks each "
+                                            "tile's rays as a warp packet"}
     if not args.no_extra:
         line["value_fresh"] = {"value": total_rays / (fresh_ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": fresh_ms,
                                "how": "a new seeded set of observers every step, L2 flushed (256 MiB write) before "
